@@ -1,0 +1,97 @@
+// C entry points of the BSDF shading batch (include/vlrb.h).
+#include "vlrb_internal.h"
+
+#include <cstdio>
+#include <exception>
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t bytes) { return cudaMalloc(&p, bytes > 0 ? bytes : 1); }
+};
+
+bool validBatch(const VLRBBsdfBatch* b) {
+    if (!b || b->count < 0)
+        return false;
+    if (b->count == 0)
+        return true;
+    return b->wo && b->material && b->roughness && b->ior && b->albedo && b->metallic && b->u &&
+           b->wavelengthU && b->value && b->pdf && b->wi && b->evalValue && b->evalPdf;
+}
+
+} // namespace
+
+extern "C" const char* vlrbVersion(void) {
+    return "vlr_b200 sm_100a";
+}
+
+extern "C" VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream) {
+    if (!validBatch(batch))
+        return VLRResult_InvalidArgument;
+    try {
+        cudaError_t e = vlrb::launchBsdfBatch(*batch, reinterpret_cast<cudaStream_t>(stream), nullptr);
+        return e == cudaSuccess ? VLRResult_NoError : VLRResult_InternalError;
+    }
+    catch (const std::exception &ex) {
+        std::fprintf(stderr, "vlrbBsdfBatch: %s\n", ex.what());
+        return VLRResult_InternalError;
+    }
+}
+
+extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs) {
+    if (!validBatch(batch))
+        return VLRResult_InvalidArgument;
+    if (batch->count == 0) {
+        if (kernelMs) *kernelMs = 0.0f;
+        return VLRResult_NoError;
+    }
+    try {
+        const size_t n = static_cast<size_t>(batch->count);
+        // Inputs: wo 3, material 1 (u32), roughness 2, ior 1, albedo 3,
+        // metallic 1, u 3, wavelengthU 2  -> 16 words per query.
+        // Outputs: value 4, pdf 1, wi 3, evalValue 4, evalPdf 1 -> 13 words.
+        DevBuf in, out;
+        if (in.alloc(n * 16 * 4) != cudaSuccess || out.alloc(n * 13 * 4) != cudaSuccess)
+            return VLRResult_InternalError;
+        char* ib = static_cast<char*>(in.p);
+        char* ob = static_cast<char*>(out.p);
+        VLRBBsdfBatch d = *batch;
+        size_t off = 0;
+        auto place = [&](const void* src, size_t words, const void** dst) {
+            *dst = ib + off;
+            cudaMemcpy(ib + off, src, n * words * 4, cudaMemcpyHostToDevice);
+            off += n * words * 4;
+        };
+        place(batch->wo, 3, reinterpret_cast<const void**>(&d.wo));
+        place(batch->material, 1, reinterpret_cast<const void**>(&d.material));
+        place(batch->roughness, 2, reinterpret_cast<const void**>(&d.roughness));
+        place(batch->ior, 1, reinterpret_cast<const void**>(&d.ior));
+        place(batch->albedo, 3, reinterpret_cast<const void**>(&d.albedo));
+        place(batch->metallic, 1, reinterpret_cast<const void**>(&d.metallic));
+        place(batch->u, 3, reinterpret_cast<const void**>(&d.u));
+        place(batch->wavelengthU, 2, reinterpret_cast<const void**>(&d.wavelengthU));
+        // value first so its float4 stores stay 16-byte aligned.
+        d.value = reinterpret_cast<float*>(ob);
+        d.evalValue = reinterpret_cast<float*>(ob + n * 16);
+        d.pdf = reinterpret_cast<float*>(ob + n * 32);
+        d.wi = reinterpret_cast<float*>(ob + n * 36);
+        d.evalPdf = reinterpret_cast<float*>(ob + n * 48);
+        float ms = 0.0f;
+        cudaError_t e = vlrb::launchBsdfBatch(d, nullptr, &ms);
+        if (e != cudaSuccess)
+            return VLRResult_InternalError;
+        cudaMemcpy(batch->value, d.value, n * 16, cudaMemcpyDeviceToHost);
+        cudaMemcpy(batch->evalValue, d.evalValue, n * 16, cudaMemcpyDeviceToHost);
+        cudaMemcpy(batch->pdf, d.pdf, n * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(batch->wi, d.wi, n * 12, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(batch->evalPdf, d.evalPdf, n * 4, cudaMemcpyDeviceToHost);
+        if (kernelMs) *kernelMs = ms;
+        return e == cudaSuccess ? VLRResult_NoError : VLRResult_InternalError;
+    }
+    catch (const std::exception &ex) {
+        std::fprintf(stderr, "vlrbBsdfBatchHost: %s\n", ex.what());
+        return VLRResult_InternalError;
+    }
+}
