@@ -56,6 +56,59 @@ VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream);
  * done.  kernelMs (may be NULL) receives the kernel's device time. */
 VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs);
 
+
+/* ------------------------------------------------------------------------
+ * Rendering extensions.
+ * ---------------------------------------------------------------------- */
+
+/* Render `samples` samples per pixel in as few launches as the path budget
+ * allows (vlrContextRender renders exactly one per call, as the reference
+ * does: libVLR/context.cpp:1423-1442).  Same film, accumulation and
+ * firstFrame semantics as vlrContextRender; limitNumAccumFrames caps the
+ * total. */
+VLRResult vlrbContextRenderSamples(VLRContext context, CUstream stream, VLRCameraConst camera, bool firstFrame,
+                                   uint32_t samples, uint32_t limitNumAccumFrames, uint32_t* numAccumFrames);
+
+typedef struct VLRBRenderOptions {
+    uint32_t maxPathLength;       /* hits after which a path stops scattering (reference: 25) */
+    uint32_t maxPathsInFlight;    /* path slots per launch (memory ~ 200 B each) */
+    uint32_t lightPathsPerFrame;  /* LVC-BPT light subpaths per frame, 0 = one per pixel */
+} VLRBRenderOptions;
+
+VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options);
+VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* options);
+
+typedef struct VLRBRenderStats {
+    uint64_t pathSegments;        /* extension rays traced (camera rays included) */
+    uint64_t shadowRays;
+    uint64_t frames;              /* samples per pixel rendered since context creation */
+    uint32_t lightVertexOverflow; /* LVC-BPT cache appends dropped for lack of capacity */
+    uint32_t numTriangles;
+} VLRBRenderStats;
+
+VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);
+
+/* Copies the FP64 spectral film (width * height * 16 doubles, strata of
+ * 29.375 nm over 360-830 nm, sum over accumulated samples) to host memory. */
+VLRResult vlrbContextReadFilm(VLRContext context, double* strata);
+
+/* Device address of the RGBA32F output image (width * height * 16 bytes). */
+VLRResult vlrbContextGetOutputDevicePointer(VLRContext context, void** devicePtr);
+
+/* ------------------------------------------------------------------------
+ * LBVH build over world-space triangles (replaces the OptiX acceleration
+ * structure builds of libVLR/scene.cpp:1318-1328).
+ * triVerts: n triangles x 3 vertices x xyz (host).  Outputs (host):
+ *   sortedCodes[n]  30-bit Morton codes in BVH order
+ *   sortedPrims[n]  primitive index of each sorted slot
+ *   children[2(n-1)] child references of each internal node (>= 0 internal,
+ *                   ~i leaf i in sorted order)
+ *   nodeBoxes[6(n-1)] box (min xyz, max xyz) of each internal node
+ * buildMs (may be NULL) receives the GPU build time.
+ * ---------------------------------------------------------------------- */
+VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
+                           int32_t* children, float* nodeBoxes, float* buildMs);
+
 #if defined(__cplusplus)
 }
 #endif

@@ -72,7 +72,7 @@ def build(force=False, verbose=True):
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     objs = [o for o, _ in results]
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-o", LIB] + objs + ["-lcuda"]
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-o", LIB] + objs
         subprocess.check_call(cmd)
     if verbose:
         print("built", LIB)

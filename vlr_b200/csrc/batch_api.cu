@@ -1,5 +1,6 @@
 // C entry points of the BSDF shading batch (include/vlrb.h).
 #include "vlrb_internal.h"
+#include "lbvh_build.h"
 
 #include <cstdio>
 #include <exception>
@@ -92,6 +93,51 @@ extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernel
     }
     catch (const std::exception &ex) {
         std::fprintf(stderr, "vlrbBsdfBatchHost: %s\n", ex.what());
+        return VLRResult_InternalError;
+    }
+}
+
+extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
+                                      int32_t* children, float* nodeBoxes, float* buildMs) {
+    if (!triVerts || !sortedCodes || !sortedPrims || (n > 1 && (!children || !nodeBoxes)))
+        return VLRResult_InvalidArgument;
+    if (n == 0) return VLRResult_NoError;
+    try {
+        const size_t N = n;
+        auto a256 = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const size_t sizes[7] = { N * 36, N * 4, N * 4, N * 8, N * 24, N * sizeof(vlrb::BvhNode), N * sizeof(vlrb::BvhTri) };
+        size_t off[7], total = 0;
+        for (int i = 0; i < 7; ++i) { off[i] = total; total += a256(sizes[i]); }
+        DevBuf out, scratch;
+        if (out.alloc(total) != cudaSuccess || scratch.alloc(vlrb::lbvhScratchBytes(n)) != cudaSuccess)
+            return VLRResult_InternalError;
+        char* b = static_cast<char*>(out.p);
+        cudaMemcpy(b + off[0], triVerts, N * 36, cudaMemcpyHostToDevice);
+        vlrb::LbvhOutput lo{ reinterpret_cast<uint32_t*>(b + off[1]), reinterpret_cast<uint32_t*>(b + off[2]),
+                             reinterpret_cast<int32_t*>(b + off[3]), reinterpret_cast<float*>(b + off[4]),
+                             reinterpret_cast<vlrb::BvhNode*>(b + off[5]), reinterpret_cast<vlrb::BvhTri*>(b + off[6]) };
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, nullptr);
+        vlrb::lbvhBuild(reinterpret_cast<const float*>(b + off[0]), n, scratch.p, &lo, nullptr);
+        cudaEventRecord(e1, nullptr);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (buildMs) *buildMs = ms;
+        cudaMemcpy(sortedCodes, lo.sortedCodes, N * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(sortedPrims, lo.sortedPrims, N * 4, cudaMemcpyDeviceToHost);
+        if (n > 1) {
+            cudaMemcpy(children, lo.children, (N - 1) * 8, cudaMemcpyDeviceToHost);
+            cudaMemcpy(nodeBoxes, lo.nodeBoxes, (N - 1) * 24, cudaMemcpyDeviceToHost);
+        }
+        return cudaGetLastError() == cudaSuccess ? VLRResult_NoError : VLRResult_InternalError;
+    }
+    catch (const std::exception &ex) {
+        std::fprintf(stderr, "vlrbBvhBuildHost: %s\n", ex.what());
         return VLRResult_InternalError;
     }
 }

@@ -1,0 +1,663 @@
+// Rendering context: scene flattening and upload, light tables, environment
+// importance map, camera setup, render orchestration and film readout.
+//
+// Scene build (replaces Scene::setup, libVLR/scene.cpp:1149-1402, and the
+// OptiX GAS/IAS builds at :1318-1328): the node graph is walked from the
+// scene root, every (transform chain, triangle mesh) pair becomes one
+// instance whose vertices are transformed to world space, and a single LBVH
+// is built over all world-space triangles on the GPU.  Light tables keep the
+// reference's probabilities: emitting instances (environment first) and
+// emitting material groups are chosen uniformly, triangles by area.
+#include "context.cuh"
+#include "lbvh_build.h"
+#include "tables.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <random>
+#include <string>
+
+namespace vlrb {
+
+// envmap.cu
+void buildEnvDistribution(const float* hostLuminance, uint32_t w, uint32_t h, double* rowCdf, double* margCdf,
+                          float* rowPdf, float* margPdf, void* scratch, cudaStream_t stream);
+size_t envScratchBytes(uint32_t w, uint32_t h);
+// bpt.cu
+size_t bptBufferBytes(uint32_t numPaths, uint32_t cacheCapacity);
+void carveBptBuffers(void* base, uint32_t numPaths, uint32_t cacheCapacity, PathBuffers* lightPaths,
+                     BptBuffers* bb);
+void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const PathBuffers &lightPaths,
+                     const BptBuffers &bb, const Film &film, const FrameParams &fp, uint32_t numLightPaths,
+                     const WLS &commonWls, float wlPdf, int numSMs, cudaStream_t stream);
+
+namespace api {
+
+namespace {
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Column-major 4x4 helpers.
+void matMul(const float a[16], const float b[16], float out[16]) {
+    float r[16];
+    for (int c = 0; c < 4; ++c)
+        for (int rr = 0; rr < 4; ++rr) {
+            float s = 0;
+            for (int k = 0; k < 4; ++k) s += a[k * 4 + rr] * b[c * 4 + k];
+            r[c * 4 + rr] = s;
+        }
+    std::memcpy(out, r, sizeof(r));
+}
+void matIdentity(float m[16]) {
+    for (int i = 0; i < 16; ++i) m[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+}
+V3 xfPoint(const float m[16], const V3 &p) {
+    return V3(m[0] * p.x + m[4] * p.y + m[8] * p.z + m[12],
+              m[1] * p.x + m[5] * p.y + m[9] * p.z + m[13],
+              m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14]);
+}
+V3 xfVector(const float m[16], const V3 &v) {
+    return V3(m[0] * v.x + m[4] * v.y + m[8] * v.z, m[1] * v.x + m[5] * v.y + m[9] * v.z,
+              m[2] * v.x + m[6] * v.y + m[10] * v.z);
+}
+// Normals transform by the inverse transpose (shared/shared.h:316-321).
+V3 xfNormal(const float inv[16], const V3 &n) {
+    return V3(inv[0] * n.x + inv[1] * n.y + inv[2] * n.z, inv[4] * n.x + inv[5] * n.y + inv[6] * n.z,
+              inv[8] * n.x + inv[9] * n.y + inv[10] * n.z);
+}
+
+ColorSp parseColorSpace(const std::string &s) {
+    std::string l = lower(s);
+    if (l == "rec709(d65) srgb gamma") return ColorSp::sRGB;
+    if (l == "xyz") return ColorSp::XYZ;
+    if (l == "xyy") return ColorSp::xyY;
+    return ColorSp::Rec709;
+}
+
+UpSpec upsampleImm(const ImmSpectrum &s, SpType t) {
+    return mengUpsample(hostMengTables(), hostColorMatrices(), t, parseColorSpace(s.colorSpace), s.e[0], s.e[1], s.e[2]);
+}
+
+// Reference-style discrete distribution: PMF = w / sum, CDF prefix / sum with
+// a compensated (Kahan) running sum, CDF[n] = 1 (context.cpp:1796-1819).
+struct HostDist {
+    std::vector<float> pmf, cdf;
+    float integral = 0;
+};
+HostDist makeDist(const std::vector<float> &w) {
+    HostDist d;
+    const size_t n = w.size();
+    d.pmf = w;
+    d.cdf.assign(n + 1, 0.0f);
+    float sum = 0, comp = 0;
+    for (size_t i = 0; i < n; ++i) {
+        d.cdf[i] = sum;
+        float y = w[i] - comp;
+        float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    d.integral = sum;
+    for (size_t i = 0; i < n; ++i) { d.pmf[i] /= d.integral; d.cdf[i] /= d.integral; }
+    d.cdf[n] = 1.0f;
+    return d;
+}
+
+} // namespace
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void DeviceBuffer::resize(size_t b) {
+    if (b <= bytes && ptr) return;
+    release();
+    ck(cudaMalloc(&ptr, b > 0 ? b : 1), "cudaMalloc");
+    bytes = b;
+}
+
+Context::Context(CUcontext cu, bool log) : Object(Kind::Context), cuContext(cu), logging(log) {
+    typeName = "Context";
+    ctx = this;
+    ck(cudaGetDevice(&device), "cudaGetDevice");
+    ck(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device), "SM count");
+    ck(cudaMallocHost(reinterpret_cast<void**>(&hostCounters), (kMaxBounces + 1) * kCountersPerBounce * 4),
+       "pinned counters");
+}
+
+Context::~Context() {
+    for (Object* o : objects) delete o;
+    objects.clear();
+    if (outArray) cudaFreeArray(reinterpret_cast<cudaArray_t>(outArray));
+    if (hostCounters) cudaFreeHost(hostCounters);
+}
+
+void Context::destroy(Object* o) {
+    if (!owns(o)) return;
+    objects.erase(o);
+    if (o == scene) scene = nullptr;
+    delete o;
+    markDirty();
+}
+
+template <typename T>
+T* Context::upload(const std::vector<T> &v, cudaStream_t stream) {
+    auto buf = std::make_unique<DeviceBuffer>();
+    buf->resize(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (!v.empty())
+        ck(cudaMemcpyAsync(buf->ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
+    T* p = buf->as<T>();
+    sceneBufs.push_back(std::move(buf));
+    return p;
+}
+
+void Context::bindOutput(uint32_t w, uint32_t h) {
+    width = w;
+    height = h;
+    film.resize(size_t(w) * h * kNumStrata * 8);
+    output.resize(size_t(w) * h * 16);
+    ck(cudaMemset(film.ptr, 0, size_t(w) * h * kNumStrata * 8), "film clear");
+    ck(cudaMemset(output.ptr, 0, size_t(w) * h * 16), "output clear");
+    if (outArray) { cudaFreeArray(reinterpret_cast<cudaArray_t>(outArray)); outArray = nullptr; }
+    pathCapacity = 0;
+    numAccumFrames = 0;
+}
+
+CUarray Context::outputArray() {
+    // A CUDA array of RGBA32F texels refreshed from the output image; runtime
+    // API only so the library needs no link-time dependency on the driver.
+    if (!outArray && width > 0) {
+        cudaChannelFormatDesc desc = cudaCreateChannelDesc<float4>();
+        cudaArray_t a = nullptr;
+        ck(cudaMallocArray(&a, &desc, width, height), "cudaMallocArray");
+        outArray = reinterpret_cast<CUarray>(a);
+    }
+    if (outArray)
+        ck(cudaMemcpy2DToArray(reinterpret_cast<cudaArray_t>(outArray), 0, 0, output.ptr, size_t(width) * 16,
+                               size_t(width) * 16, height, cudaMemcpyDeviceToDevice), "output array copy");
+    return outArray;
+}
+
+void Context::readOutput(float* host) {
+    ck(cudaMemcpy(host, output.ptr, size_t(width) * height * 16, cudaMemcpyDeviceToHost), "read output");
+}
+
+void Context::readFilm(double* host) {
+    ck(cudaMemcpy(host, film.ptr, size_t(width) * height * kNumStrata * 8, cudaMemcpyDeviceToHost), "read film");
+}
+
+namespace {
+
+// Material descriptor from the material's parameters, following each
+// material's setupMaterialDescriptor / setupBSDF pair in the reference
+// (libVLR/materials.cpp and GPU_kernels/materials.cu).
+MatDesc describeMaterial(const SurfaceMaterial* m) {
+    MatDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.bsdfKind = kNullBSDF;
+    d.emitScale = 1.0f;
+    const std::string t = lower(m->typeName);
+    auto spec = [&](const char* name) { return m->spectra.at(lower(name)); };
+    auto roughAniso = [&](float* out) {
+        float r = m->getFloat("roughness", 0.1f), a = m->getFloat("anisotropy", 0.0f), rot = m->getFloat("rotation", 0.0f);
+        float alpha = r * r;
+        float aspect = std::sqrt(1.0f - 0.9f * a);
+        out[0] = std::fmax(0.001f, alpha / aspect);
+        out[1] = std::fmax(0.001f, alpha * aspect);
+        out[2] = 2 * kPi * rot;
+    };
+    if (t == "matte") {
+        d.bsdfKind = kMatte;
+        d.sp[0] = upsampleImm(spec("albedo"), SpType::Reflectance);
+    }
+    else if (t == "specularreflection") {
+        d.bsdfKind = kSpecularBRDF;
+        d.sp[0] = upsampleImm(spec("coeff"), SpType::Reflectance);
+        d.sp[1] = upsampleImm(spec("eta"), SpType::IOR);
+        d.sp[2] = upsampleImm(spec("k"), SpType::IOR);
+    }
+    else if (t == "specularscattering") {
+        d.bsdfKind = kSpecularBSDF;
+        d.sp[0] = upsampleImm(spec("coeff"), SpType::Reflectance);
+        d.sp[1] = upsampleImm(spec("eta ext"), SpType::IOR);
+        d.sp[2] = upsampleImm(spec("eta int"), SpType::IOR);
+    }
+    else if (t == "microfacetreflection") {
+        d.bsdfKind = kMicrofacetBRDF;
+        d.sp[1] = upsampleImm(spec("eta"), SpType::IOR);
+        d.sp[2] = upsampleImm(spec("k"), SpType::IOR);
+        roughAniso(d.f);
+    }
+    else if (t == "microfacetscattering") {
+        d.bsdfKind = kMicrofacetBSDF;
+        d.sp[0] = upsampleImm(spec("coeff"), SpType::Reflectance);
+        d.sp[1] = upsampleImm(spec("eta ext"), SpType::IOR);
+        d.sp[2] = upsampleImm(spec("eta int"), SpType::IOR);
+        roughAniso(d.f);
+    }
+    else if (t == "lambertianscattering") {
+        d.bsdfKind = kLambertianBSDF;
+        d.sp[0] = upsampleImm(spec("coeff"), SpType::Reflectance);
+        d.f[0] = m->getFloat("f0", 0.04f);
+    }
+    else if (t == "ue4") {
+        d.bsdfKind = kUE4;
+        d.sp[0] = upsampleImm(spec("base color"), SpType::Reflectance);
+        d.f[0] = std::fmax(0.01f, m->getFloat("roughness", 0.1f));
+        d.f[1] = m->getFloat("metallic", 0.0f);
+    }
+    else if (t == "diffuseemitter") {
+        d.emitter = 1;
+        d.emit = upsampleImm(spec("emittance"), SpType::LightSource);
+        d.emitScale = m->getFloat("scale", 1.0f);
+    }
+    else if (t == "environmentemitter") {
+        d.emitter = 2;
+        d.emit = upsampleImm(spec("emittance"), SpType::LightSource);
+        d.emitScale = m->getFloat("scale", 1.0f);
+    }
+    return d;
+}
+
+struct FlatScene {
+    std::vector<float4> pos, nrm, tan;
+    std::vector<uint4> tri;
+    std::vector<uint32_t> triMaterial;
+    std::vector<float> triVerts;                 // 9 floats per triangle for the BVH build
+    std::vector<MatDesc> mats;
+    std::vector<const SurfaceMaterial*> matObjs;
+    // geometry instances (one per instance x material group)
+    std::vector<uint32_t> geomInstInstance;
+    std::vector<uint32_t> geomInstMaterial;
+    std::vector<std::vector<uint32_t>> geomInstTris;
+    std::vector<std::vector<float>> geomInstAreas;
+    uint32_t numInstances = 0;
+    V3 lo{ FLT_MAX, FLT_MAX, FLT_MAX }, hi{ -FLT_MAX, -FLT_MAX, -FLT_MAX };
+};
+
+uint32_t materialIndex(FlatScene &f, const SurfaceMaterial* m) {
+    for (size_t i = 0; i < f.matObjs.size(); ++i)
+        if (f.matObjs[i] == m) return static_cast<uint32_t>(i);
+    f.matObjs.push_back(m);
+    f.mats.push_back(describeMaterial(m));
+    return static_cast<uint32_t>(f.mats.size() - 1);
+}
+
+void flattenNode(FlatScene &f, const Node* n, const float world[16], const float worldInv[16]) {
+    if (n->kind == Kind::TriangleMeshSurfaceNode) {
+        const auto* mesh = static_cast<const TriangleMeshNode*>(n);
+        const uint32_t inst = f.numInstances++;
+        const uint32_t base = static_cast<uint32_t>(f.pos.size());
+        for (const VLRVertex &v : mesh->vertices) {
+            V3 p = xfPoint(world, V3(v.position.x, v.position.y, v.position.z));
+            V3 nn = xfNormal(worldInv, V3(v.normal.x, v.normal.y, v.normal.z));
+            V3 tt = xfVector(world, V3(v.tc0Direction.x, v.tc0Direction.y, v.tc0Direction.z));
+            f.pos.push_back(make_float4(p.x, p.y, p.z, 0.0f));
+            f.nrm.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
+            f.tan.push_back(make_float4(tt.x, tt.y, tt.z, 0.0f));
+            f.lo = vmin3(f.lo, p);
+            f.hi = vmax3(f.hi, p);
+        }
+        for (const MaterialGroup &g : mesh->groups) {
+            if (!g.material) continue;
+            const uint32_t gi = static_cast<uint32_t>(f.geomInstMaterial.size());
+            const uint32_t mi = materialIndex(f, g.material);
+            f.geomInstInstance.push_back(inst);
+            f.geomInstMaterial.push_back(mi);
+            f.geomInstTris.emplace_back();
+            f.geomInstAreas.emplace_back();
+            for (size_t k = 0; k + 2 < g.indices.size(); k += 3) {
+                uint32_t i0 = g.indices[k], i1 = g.indices[k + 1], i2 = g.indices[k + 2];
+                if (i0 >= mesh->vertices.size() || i1 >= mesh->vertices.size() || i2 >= mesh->vertices.size())
+                    throw std::runtime_error("triangle index out of range");
+                const uint32_t t = static_cast<uint32_t>(f.tri.size());
+                f.tri.push_back(make_uint4(base + i0, base + i1, base + i2, gi));
+                f.triMaterial.push_back(mi);
+                const float4 &a = f.pos[base + i0], &b = f.pos[base + i1], &c = f.pos[base + i2];
+                f.triVerts.insert(f.triVerts.end(), { a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z });
+                // Triangle area in the mesh's own space, as the reference computes it
+                // before instancing (scene.cpp:206-207).
+                const VLRVertex &va = mesh->vertices[i0], &vb = mesh->vertices[i1], &vc = mesh->vertices[i2];
+                V3 e1(vb.position.x - va.position.x, vb.position.y - va.position.y, vb.position.z - va.position.z);
+                V3 e2(vc.position.x - va.position.x, vc.position.y - va.position.y, vc.position.z - va.position.z);
+                f.geomInstTris.back().push_back(t);
+                f.geomInstAreas.back().push_back(0.5f * cross(e1, e2).length());
+            }
+        }
+        return;
+    }
+    if (n->kind == Kind::InternalNode || n->kind == Kind::Scene) {
+        const auto* p = static_cast<const ParentNode*>(n);
+        float w[16], wi[16];
+        if (p->transform) {
+            matMul(world, p->transform->m, w);
+            matMul(p->transform->inv, worldInv, wi);
+        }
+        else {
+            std::memcpy(w, world, sizeof(w));
+            std::memcpy(wi, worldInv, sizeof(wi));
+        }
+        for (const Node* c : p->children) flattenNode(f, c, w, wi);
+    }
+}
+
+} // namespace
+
+void Context::buildScene(cudaStream_t stream) {
+    sceneBufs.clear();
+    std::memset(&sg, 0, sizeof(sg));
+    sg.meng = deviceMengTables();
+    sg.envInst = -1;
+    FlatScene f;
+    if (scene) {
+        float id[16];
+        matIdentity(id);
+        flattenNode(f, scene, id, id);
+    }
+    const uint32_t numTris = static_cast<uint32_t>(f.tri.size());
+    // environment material
+    const SurfaceMaterial* envMat = scene ? scene->envMaterial : nullptr;
+    uint32_t envMatIndex = 0;
+    if (envMat) envMatIndex = materialIndex(f, envMat);
+    if (f.mats.empty()) f.mats.push_back(MatDesc{});
+
+    // ---- light tables (scene.cpp:1237-1402)
+    struct LightInst { std::vector<uint32_t> groups; };
+    std::vector<LightInst> lightInsts;
+    std::vector<uint32_t> geomInstGroup(f.geomInstMaterial.size(), 0xFFFFFFFFu);
+    std::vector<EmitGroup> groups;
+    std::vector<uint32_t> lightTris;
+    std::vector<HostDist> groupDists;
+    const bool envEmitting = envMat && envMat->isEmitting();
+    if (envEmitting) lightInsts.push_back(LightInst{ { 0xFFFFFFFEu } });
+    {
+        std::map<uint32_t, size_t> instToLight;
+        for (size_t g = 0; g < f.geomInstMaterial.size(); ++g) {
+            if (!f.mats[f.geomInstMaterial[g]].emitter) continue;
+            if (f.geomInstTris[g].empty()) continue;
+            uint32_t inst = f.geomInstInstance[g];
+            auto it = instToLight.find(inst);
+            if (it == instToLight.end()) {
+                it = instToLight.emplace(inst, lightInsts.size()).first;
+                lightInsts.emplace_back();
+            }
+            const uint32_t grp = static_cast<uint32_t>(groups.size());
+            lightInsts[it->second].groups.push_back(grp);
+            geomInstGroup[g] = grp;
+            EmitGroup eg{};
+            eg.firstTri = static_cast<uint32_t>(lightTris.size());
+            eg.numTris = static_cast<uint32_t>(f.geomInstTris[g].size());
+            eg.material = f.geomInstMaterial[g];
+            lightTris.insert(lightTris.end(), f.geomInstTris[g].begin(), f.geomInstTris[g].end());
+            groupDists.push_back(makeDist(f.geomInstAreas[g]));
+            groups.push_back(eg);
+        }
+    }
+    // Device distributions.
+    std::vector<Dist1D> instGroupDists;
+    std::vector<uint32_t> instFirstGroup;
+    std::vector<float> geomLightProb(f.geomInstMaterial.size() + 1, 0.0f);
+    const float numLightInsts = static_cast<float>(lightInsts.size());
+    HostDist instDist = makeDist(std::vector<float>(lightInsts.size(), 1.0f));
+    for (size_t i = 0; i < lightInsts.size(); ++i) {
+        const size_t G = lightInsts[i].groups.size();
+        HostDist gd = makeDist(std::vector<float>(G, 1.0f));
+        Dist1D d{ upload(gd.pmf, stream), upload(gd.cdf, stream), gd.integral, static_cast<uint32_t>(G) };
+        instGroupDists.push_back(d);
+        const bool isEnv = envEmitting && i == 0;
+        instFirstGroup.push_back(isEnv ? 0u : lightInsts[i].groups[0]);
+        // Selection probabilities as the reference's MIS uses them
+        // (path_tracing.cu:168-170): instProb = groups(inst) / sum of instance
+        // importances, geomInstProb = 1 / groups(inst).
+        const float instProb = static_cast<float>(G) / numLightInsts;
+        const float geomInstProb = 1.0f / static_cast<float>(G);
+        if (isEnv) { sg.envInst = 0; sg.envLightProb = instProb * geomInstProb; }
+        else
+            for (size_t g = 0; g < f.geomInstMaterial.size(); ++g)
+                if (geomInstGroup[g] != 0xFFFFFFFFu &&
+                    std::find(lightInsts[i].groups.begin(), lightInsts[i].groups.end(), geomInstGroup[g]) !=
+                        lightInsts[i].groups.end())
+                    geomLightProb[g] = instProb * geomInstProb;
+    }
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const HostDist &hd = groupDists[g];
+        groups[g].prims = Dist1D{ upload(hd.pmf, stream), upload(hd.cdf, stream), hd.integral, groups[g].numTris };
+    }
+    sg.lightInsts = Dist1D{ upload(instDist.pmf, stream), upload(instDist.cdf, stream), instDist.integral,
+                            static_cast<uint32_t>(lightInsts.size()) };
+    sg.instGroups = upload(instGroupDists, stream);
+    sg.instFirstGroup = upload(instFirstGroup, stream);
+    sg.groups = upload(groups, stream);
+    sg.geomLightPdfArea = upload(geomLightProb, stream);
+    geomInstGroup.push_back(0xFFFFFFFFu);
+    sg.geomInstGroup = upload(geomInstGroup, stream);
+    sg.lightTris = upload(lightTris, stream);
+
+    // ---- geometry
+    sg.numTris = numTris;
+    sg.pos = upload(f.pos, stream);
+    sg.nrm = upload(f.nrm, stream);
+    sg.tan = upload(f.tan, stream);
+    sg.tri = upload(f.tri, stream);
+    sg.triMaterial = upload(f.triMaterial, stream);
+    sg.mats = upload(f.mats, stream);
+    if (f.pos.empty()) { f.lo = V3(0.0f); f.hi = V3(0.0f); }
+    sg.bounds.lo = f.lo;
+    sg.bounds.hi = f.hi;
+    sg.bounds.center = (f.lo + f.hi) * 0.5f;
+    sg.bounds.worldRadius = (f.hi - sg.bounds.center).length();
+    sg.bounds.worldDiscArea = kPi * sg.bounds.worldRadius * sg.bounds.worldRadius;
+
+    // ---- BVH
+    if (numTris > 0) {
+        const float* dVerts = upload(f.triVerts, stream);
+        auto out = std::make_unique<DeviceBuffer>();
+        const size_t n = numTris;
+        size_t off[6];
+        size_t total = 0;
+        const size_t sizes[6] = { n * 4, n * 4, n * 8, n * 24, n * sizeof(BvhNode), n * sizeof(BvhTri) };
+        for (int i = 0; i < 6; ++i) { off[i] = total; total += (sizes[i] + 255) & ~size_t(255); }
+        out->resize(total);
+        char* b = out->as<char>();
+        LbvhOutput lo{ reinterpret_cast<uint32_t*>(b + off[0]), reinterpret_cast<uint32_t*>(b + off[1]),
+                       reinterpret_cast<int32_t*>(b + off[2]), reinterpret_cast<float*>(b + off[3]),
+                       reinterpret_cast<BvhNode*>(b + off[4]), reinterpret_cast<BvhTri*>(b + off[5]) };
+        lbvhScratch.resize(lbvhScratchBytes(numTris));
+        lbvhBuild(dVerts, numTris, lbvhScratch.ptr, &lo, stream);
+        auto flag = std::make_unique<DeviceBuffer>();
+        flag->resize(256);
+        ck(cudaMemsetAsync(flag->ptr, 0, 4, stream), "bvh flag");
+        sg.bvh = Bvh{ lo.nodes, lo.tris, numTris, flag->as<uint32_t>() };
+        sceneBufs.push_back(std::move(flag));
+        sceneBufs.push_back(std::move(out));
+    }
+
+    // ---- environment (EnvironmentEmitter with an EnvironmentTexture node)
+    if (envMat) {
+        sg.envMaterial = envMatIndex;
+        sg.envRotation = scene->envRotation;
+        const Image2D* img = nullptr;
+        auto pit = envMat->plugs.find("emittance");
+        if (pit != envMat->plugs.end() && pit->second.nodeRef) {
+            const auto* node = reinterpret_cast<const ShaderNode*>(pit->second.nodeRef);
+            auto iit = node->objects.find("image");
+            if (iit != node->objects.end()) img = static_cast<const Image2D*>(iit->second);
+        }
+        uint32_t w = 1, h = 1;
+        std::vector<UpSpec> texels;
+        std::vector<float> lum;
+        if (img && img->width > 0) {
+            w = img->width;
+            h = img->height;
+            texels.resize(size_t(w) * h);
+            lum.resize(size_t(w) * h);
+            const ColorMatrices &M = hostColorMatrices();
+            for (size_t i = 0; i < texels.size(); ++i) {
+                float r = img->rgba[4 * i], g = img->rgba[4 * i + 1], bb2 = img->rgba[4 * i + 2];
+                texels[i] = mengUpsample(hostMengTables(), M, SpType::LightSource, ColorSp::Rec709, r, g, bb2);
+                float rgb[3] = { r, g, bb2 }, xyz[3];
+                mulColMajor(M.rec709D65ToXYZ, rgb, xyz);
+                lum[i] = std::fmax(xyz[1], 0.0f);
+            }
+        }
+        else {
+            // Constant environment: the immediate emittance everywhere.
+            texels.push_back(f.mats[envMatIndex].emit);
+            f.mats[envMatIndex].emitScale = f.mats[envMatIndex].emitScale;
+            lum.push_back(1.0f);
+        }
+        // The texel radiance already carries the immediate emittance for the
+        // textured case; the descriptor's scale multiplies both.
+        sg.envTexels = upload(texels, stream);
+        auto dist = std::make_unique<DeviceBuffer>();
+        const size_t bRow = (size_t(h) * (w + 1) * 8 + 255) & ~size_t(255);
+        const size_t bMarg = ((h + 1) * 8 + 255) & ~size_t(255);
+        const size_t bRowPdf = (size_t(h) * w * 4 + 255) & ~size_t(255);
+        const size_t bMargPdf = (h * 4 + 255) & ~size_t(255);
+        dist->resize(bRow + bMarg + bRowPdf + bMargPdf);
+        char* d = dist->as<char>();
+        sg.env.rowCdf = reinterpret_cast<double*>(d);
+        sg.env.margCdf = reinterpret_cast<double*>(d + bRow);
+        sg.env.rowPdf = reinterpret_cast<float*>(d + bRow + bMarg);
+        sg.env.margPdf = reinterpret_cast<float*>(d + bRow + bMarg + bRowPdf);
+        sg.env.w = w;
+        sg.env.h = h;
+        DeviceBuffer scratch;
+        scratch.resize(envScratchBytes(w, h));
+        buildEnvDistribution(lum.data(), w, h, const_cast<double*>(sg.env.rowCdf), const_cast<double*>(sg.env.margCdf),
+                             const_cast<float*>(sg.env.rowPdf), const_cast<float*>(sg.env.margPdf), scratch.ptr, stream);
+        ck(cudaStreamSynchronize(stream), "env build");
+        sceneBufs.push_back(std::move(dist));
+    }
+    ck(cudaStreamSynchronize(stream), "scene build");
+    builtGeneration = generation;
+}
+
+void Context::setupCamera(const Camera* cam) {
+    // PerspectiveCamera::setImagePlaneArea (shared/shared.h:895-900) and the
+    // quaternion-to-matrix conversion (include/vlr/basic_types.h:1386-1393).
+    auto f3 = [&](const char* n, std::vector<float> def) {
+        auto it = cam->floats.find(n);
+        return it != cam->floats.end() ? it->second : def;
+    };
+    std::vector<float> pos = f3("position", { 0, 0, 0 });
+    std::vector<float> q = f3("orientation", { 0, 0, 0, 1 });
+    const float aspect = cam->getFloat("aspect", 1.0f);
+    const float fovY = cam->getFloat("fovy", 45 * kPi / 180);
+    const float lensRadius = cam->getFloat("lens radius", 1.0f);
+    const float sensitivity = cam->getFloat("sensitivity", 1.0f);
+    const float objPlaneDistance = cam->getFloat("op distance", 1.0f);
+    vlrb::Camera &C = sg.cam;
+    C.position = V3(pos[0], pos[1], pos[2]);
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, zx = z * x, xw = x * w, yw = y * w, zw = z * w;
+    C.right = V3(1 - 2 * (yy + zz), 2 * (xy + zw), 2 * (zx - yw));
+    C.up = V3(2 * (xy - zw), 1 - 2 * (xx + zz), 2 * (yz + xw));
+    C.forward = V3(2 * (zx + yw), 2 * (yz - xw), 1 - 2 * (xx + yy));
+    C.sensitivity = sensitivity;
+    C.lensRadius = lensRadius;
+    C.objPlaneDistance = objPlaneDistance;
+    C.opHeight = 2.0f * objPlaneDistance * std::tan(fovY * 0.5f);
+    C.opWidth = C.opHeight * aspect;
+    C.imgPlaneDistance = 1.0f;
+    C.imgPlaneArea = C.opWidth * C.opHeight * sq(C.imgPlaneDistance / objPlaneDistance);
+}
+
+void Context::ensurePathBuffers(uint32_t paths) {
+    if (paths <= pathCapacity) return;
+    pathMem.resize(pathBufferBytes(paths));
+    carvePathBuffers(pathMem.ptr, paths, &pb);
+    std::vector<uint64_t> seeds(paths);
+    // Per-slot PCG32 states from std::mt19937_64, slot order = pixel order for
+    // the first sample of each pixel (context.cpp:1176-1190).
+    seedPathRngs(seeds.data(), paths, 591842031321323413ull);
+    ck(cudaMemcpy(pb.rng, seeds.data(), size_t(paths) * 8, cudaMemcpyHostToDevice), "seed rngs");
+    ck(cudaMemset(pb.totals, 0, 16), "totals");
+    pathCapacity = paths;
+}
+
+void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
+                     uint32_t samples, uint32_t* numAccumFramesOut) {
+    if (width == 0 || height == 0) throw std::runtime_error("no output buffer bound");
+    if (builtGeneration != generation) buildScene(stream);
+    if (firstFrame) {
+        setupCamera(cam);
+        numAccumFrames = 0;
+        filmClear(Film{ film.as<double>(), width, height }, stream);
+    }
+    const uint32_t pixels = width * height;
+    if (numAccumFrames + samples > limitFrames)
+        samples = limitFrames > numAccumFrames ? limitFrames - numAccumFrames : 0;
+    Film fl{ film.as<double>(), width, height };
+    if (samples > 0) {
+        uint32_t perLaunch = std::max<uint32_t>(1, std::min<uint32_t>(samples, options.maxPathsInFlight / pixels));
+        ensurePathBuffers(pixels * perLaunch);
+        uint32_t done = 0;
+        while (done < samples) {
+            const uint32_t k = std::min(perLaunch, samples - done);
+            FrameParams fp{};
+            fp.width = width;
+            fp.height = height;
+            fp.sppPerLaunch = k;
+            fp.numPaths = pixels * k;
+            fp.maxPathLength = options.maxPathLength;
+            if (renderer == VLRRenderer_BPT) {
+                const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame : pixels;
+                if (bptCapacityPaths < lightPaths * k) {
+                    bptCapacityPaths = lightPaths * k;
+                    bptCapacityVerts = lightPaths * k;
+                    bptMem.resize(bptBufferBytes(bptCapacityPaths, bptCapacityVerts));
+                    carveBptBuffers(bptMem.ptr, bptCapacityPaths, bptCapacityVerts, &lightPb, &bb);
+                    std::vector<uint64_t> seeds(bptCapacityPaths);
+                    seedPathRngs(seeds.data(), bptCapacityPaths, 459182033132123413ull);
+                    ck(cudaMemcpy(lightPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
+                    ck(cudaMemset(lightPb.totals, 0, 16), "totals");
+                }
+                // One common wavelength set per launch from a host generator
+                // (context.cpp:1462-1470).
+                std::uniform_real_distribution<float> u01(0.0f, 1.0f);
+                float wlPdf;
+                WLS wls = WLS::equalOffsets(u01(bptRng), u01(bptRng), &wlPdf);
+                bptRenderLaunch(sg, pb, lightPb, bb, fl, fp, lightPaths * k, wls, wlPdf, numSMs, stream);
+            }
+            else {
+                ptRenderLaunch(sg, pb, fl, fp, numSMs, stream);
+            }
+            done += k;
+        }
+        numAccumFrames += samples;
+        stats.frames += samples;
+    }
+    filmToRGBA(fl, numAccumFrames, output.as<float4>(), stream);
+    if (numAccumFramesOut) *numAccumFramesOut = numAccumFrames;
+}
+
+void Context::readStats(RenderStats* out) {
+    unsigned long long t[2] = { 0, 0 };
+    if (pathCapacity > 0) ck(cudaMemcpy(t, pb.totals, 16, cudaMemcpyDeviceToHost), "stats");
+    unsigned long long tl[2] = { 0, 0 };
+    if (bptCapacityPaths > 0) ck(cudaMemcpy(tl, lightPb.totals, 16, cudaMemcpyDeviceToHost), "light stats");
+    *out = stats;
+    if (sg.bvh.errorFlag) {
+        uint32_t e = 0;
+        ck(cudaMemcpy(&e, sg.bvh.errorFlag, 4, cudaMemcpyDeviceToHost), "bvh flag");
+        if (e) throw std::runtime_error("BVH traversal met an out-of-range node reference");
+    }
+    out->segments = t[0] + tl[0];
+    out->shadowRays = t[1] + tl[1];
+    if (bptCapacityPaths > 0) {
+        uint32_t c[2];
+        ck(cudaMemcpy(c, bb.counters, 8, cudaMemcpyDeviceToHost), "overflow");
+        out->lightVertexOverflow = c[1];
+    }
+}
+
+} // namespace api
+} // namespace vlrb

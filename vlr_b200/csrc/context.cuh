@@ -1,0 +1,96 @@
+// Rendering context: owns the API objects, the flattened device scene, the
+// path buffers, the FP64 film and the output image.
+#pragma once
+
+#include "api_objects.h"
+#include "pt.cuh"
+#include "bpt.cuh"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <random>
+
+namespace vlrb {
+namespace api {
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void release();
+    void resize(size_t b);     // discards contents
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct RenderOptions {
+    uint32_t maxPathLength = 25;      // path_tracing.cu:78, lvc_bpt.cu:216,513
+    uint32_t maxPathsInFlight = 1u << 22;
+    uint32_t lightPathsPerFrame = 0;  // 0: width * height
+};
+
+struct RenderStats {
+    uint64_t segments = 0;            // extension rays traced
+    uint64_t shadowRays = 0;
+    uint64_t frames = 0;
+    uint32_t lightVertexOverflow = 0;
+};
+
+class Context : public Object {
+public:
+    explicit Context(CUcontext cu, bool logging);
+    ~Context() override;
+
+    // object registry (handle validation)
+    std::set<Object*> objects;
+    template <typename T> T* adopt(T* o) { o->ctx = this; objects.insert(o); return o; }
+    bool owns(const Object* o) const { return o && objects.count(const_cast<Object*>(o)) != 0; }
+    void destroy(Object* o);
+
+    void bindOutput(uint32_t w, uint32_t h);
+    void setScene(Scene* s) { scene = s; markDirty(); }
+    void markDirty() { ++generation; }
+    void render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
+                uint32_t samples, uint32_t* numAccumFrames);
+    void readOutput(float* host);
+    void readFilm(double* host);
+    void readStats(RenderStats* out);
+    CUarray outputArray();
+    void* outputDevicePtr() const { return output.ptr; }
+    uint32_t numTriangles() const { return sg.numTris; }
+
+    CUcontext cuContext;
+    bool logging;
+    int device = 0, numSMs = 148;
+    uint32_t width = 0, height = 0;
+    Scene* scene = nullptr;
+    VLRRenderer renderer = VLRRenderer_PathTracing;
+    RenderOptions options;
+    RenderStats stats;
+    uint32_t numAccumFrames = 0;
+    uint64_t generation = 1, builtGeneration = 0;
+
+private:
+    void buildScene(cudaStream_t stream);
+    void setupCamera(const Camera* cam);
+    void ensurePathBuffers(uint32_t paths);
+
+    SceneGPU sg{};
+    std::vector<std::unique_ptr<DeviceBuffer>> sceneBufs;
+    DeviceBuffer film, output, pathMem, lbvhScratch, bptMem;
+    PathBuffers pb{};
+    PathBuffers lightPb{};
+    std::mt19937_64 bptRng{ 459182033132123413ull };
+    BptBuffers bb{};
+    uint32_t pathCapacity = 0;
+    uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0;
+    CUarray outArray = nullptr;
+    uint32_t* hostCounters = nullptr;
+    std::vector<float> envPixelsCache;
+    template <typename T> T* upload(const std::vector<T> &v, cudaStream_t stream);
+};
+
+} // namespace api
+} // namespace vlrb

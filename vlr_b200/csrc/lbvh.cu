@@ -1,0 +1,338 @@
+// LBVH construction on the GPU:
+//   1. centroid bounds (block reduction + one ordered-int atomic per CTA);
+//   2. 30-bit Morton codes of the quantised centroids;
+//   3. stable LSD radix sort of (code, primitive) pairs, 4-bit digits;
+//   4. Karras (2012) hierarchy over the sorted codes, ties broken by position;
+//   5. bottom-up refit with one arrival counter per internal node;
+//   6. triangles re-packed in sorted order for traversal.
+// Every integer result (codes, order, topology) and every box (min/max of the
+// input floats) is deterministic, so a host build of the same algorithm
+// reproduces it bit for bit.  Compiled without FMA contraction so the float
+// quantisation step rounds like the host build.
+#include "lbvh_build.h"
+
+#include <cuda_runtime.h>
+#include <stdexcept>
+#include <string>
+
+namespace vlrb {
+
+namespace {
+
+__device__ __forceinline__ uint32_t floatToOrdered(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedToFloat(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+__device__ __forceinline__ V3 loadVertex(const float* v, uint32_t tri, int k) {
+    const float* p = v + 9 * static_cast<size_t>(tri) + 3 * k;
+    return V3(p[0], p[1], p[2]);
+}
+
+// Centroid of a triangle: (v0 + v1 + v2) * (1/3), summed left to right.
+__device__ __forceinline__ V3 centroidOf(const float* verts, uint32_t i) {
+    V3 a = loadVertex(verts, i, 0), b = loadVertex(verts, i, 1), c = loadVertex(verts, i, 2);
+    return (a + b + c) * (1.0f / 3.0f);
+}
+
+__global__ void centroidBoundsKernel(const float* verts, uint32_t n, uint32_t* ordBox /* 6 */) {
+    __shared__ uint32_t s[6];
+    if (threadIdx.x < 3) s[threadIdx.x] = 0xFFFFFFFFu;
+    else if (threadIdx.x < 6) s[threadIdx.x] = 0u;
+    __syncthreads();
+    uint32_t lo[3] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu }, hi[3] = { 0u, 0u, 0u };
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        V3 c = centroidOf(verts, i);
+        uint32_t o[3] = { floatToOrdered(c.x), floatToOrdered(c.y), floatToOrdered(c.z) };
+        for (int k = 0; k < 3; ++k) { lo[k] = min(lo[k], o[k]); hi[k] = max(hi[k], o[k]); }
+    }
+    for (int k = 0; k < 3; ++k) {
+        for (int off = 16; off > 0; off >>= 1) {
+            lo[k] = min(lo[k], __shfl_xor_sync(0xFFFFFFFFu, lo[k], off));
+            hi[k] = max(hi[k], __shfl_xor_sync(0xFFFFFFFFu, hi[k], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) { atomicMin(&s[k], lo[k]); atomicMax(&s[3 + k], hi[k]); }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&ordBox[threadIdx.x], s[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&ordBox[threadIdx.x], s[threadIdx.x]);
+}
+
+__device__ __forceinline__ uint32_t spreadBits10(uint32_t x) {
+    x &= 0x3FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+__global__ void mortonKernel(const float* verts, uint32_t n, const uint32_t* ordBox,
+                             uint32_t* codes, uint32_t* prims) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float lo[3], scale[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = orderedToFloat(ordBox[k]);
+        float ext = orderedToFloat(ordBox[3 + k]) - lo[k];
+        scale[k] = ext > 0.0f ? 1024.0f / ext : 0.0f;
+    }
+    V3 c = centroidOf(verts, i);
+    float cc[3] = { c.x, c.y, c.z };
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+        float f = (cc[k] - lo[k]) * scale[k];
+        int qi = static_cast<int>(f);
+        q[k] = static_cast<uint32_t>(qi < 0 ? 0 : (qi > 1023 ? 1023 : qi));
+    }
+    codes[i] = (spreadBits10(q[0]) << 2) | (spreadBits10(q[1]) << 1) | spreadBits10(q[2]);
+    prims[i] = i;
+}
+
+// ---- stable LSD radix sort, 4-bit digits, tile of 256 threads x 16 items
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kRadix = 16;
+
+__global__ void radixHistKernel(const uint32_t* keys, uint32_t n, int shift, uint32_t* hist /* [16][numTiles] */) {
+    __shared__ uint32_t s[kRadix];
+    if (threadIdx.x < kRadix) s[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kSortTile;
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t i = base + k * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&s[(keys[i] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kRadix) hist[threadIdx.x * gridDim.x + blockIdx.x] = s[threadIdx.x];
+}
+
+// Exclusive scan of the [digit][tile] histogram in one CTA of 1024 threads.
+__global__ void radixScanKernel(uint32_t* hist, uint32_t count) {
+    __shared__ uint32_t partial[1024];
+    const uint32_t per = (count + 1023) / 1024;
+    const uint32_t begin = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t i = begin; i < begin + per && i < count; ++i) sum += hist[i];
+    partial[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        uint32_t v = threadIdx.x >= off ? partial[threadIdx.x - off] : 0u;
+        __syncthreads();
+        partial[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = partial[threadIdx.x] - sum;
+    for (uint32_t i = begin; i < begin + per && i < count; ++i) {
+        uint32_t v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+__global__ void radixScatterKernel(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t n, int shift,
+                                   const uint32_t* offsets, uint32_t* keysOut, uint32_t* valsOut) {
+    __shared__ uint32_t cnt[kRadix][kSortThreads + 1];
+    const uint32_t base = blockIdx.x * kSortTile + threadIdx.x * kSortItems;
+    uint32_t local[kRadix];
+    for (int d = 0; d < kRadix; ++d) local[d] = 0;
+    uint32_t key[kSortItems];
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t i = base + k;
+        key[k] = i < n ? keysIn[i] : 0u;
+        if (i < n) local[(key[k] >> shift) & (kRadix - 1)]++;
+    }
+    for (int d = 0; d < kRadix; ++d) cnt[d][threadIdx.x] = local[d];
+    __syncthreads();
+    // 16 threads each scan one digit's column over the CTA's threads.
+    if (threadIdx.x < kRadix) {
+        uint32_t run = 0;
+        for (int t = 0; t < kSortThreads; ++t) {
+            uint32_t v = cnt[threadIdx.x][t];
+            cnt[threadIdx.x][t] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    uint32_t pos[kRadix];
+    for (int d = 0; d < kRadix; ++d)
+        pos[d] = offsets[d * gridDim.x + blockIdx.x] + cnt[d][threadIdx.x];
+    for (int k = 0; k < kSortItems; ++k) {
+        uint32_t i = base + k;
+        if (i < n) {
+            uint32_t d = (key[k] >> shift) & (kRadix - 1);
+            uint32_t p = pos[d]++;
+            keysOut[p] = key[k];
+            valsOut[p] = valsIn[i];
+        }
+    }
+}
+
+// ---- Karras hierarchy
+__device__ __forceinline__ int prefixDelta(const uint32_t* codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = codes[i], b = codes[j];
+    if (a == b) return 32 + __clz(static_cast<uint32_t>(i ^ j));
+    return __clz(a ^ b);
+}
+
+__global__ void karrasKernel(const uint32_t* codes, int n, int32_t* children /* [n-1][2] */,
+                             int32_t* parentOfNode /* n-1 */, int32_t* parentOfLeaf /* n */) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (prefixDelta(codes, n, i, i + 1) - prefixDelta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dMin = prefixDelta(codes, n, i, i - d);
+    int lMax = 2;
+    while (prefixDelta(codes, n, i, i + lMax * d) > dMin) lMax <<= 1;
+    int l = 0;
+    for (int t = lMax >> 1; t >= 1; t >>= 1)
+        if (prefixDelta(codes, n, i, i + (l + t) * d) > dMin) l += t;
+    int j = i + l * d;
+    int dNode = prefixDelta(codes, n, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (prefixDelta(codes, n, i, i + (s + t) * d) > dNode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + (d < 0 ? d : 0);
+    int lo = i < j ? i : j, hi = i < j ? j : i;
+    int left = (lo == gamma) ? ~gamma : gamma;
+    int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    children[2 * i + 0] = left;
+    children[2 * i + 1] = right;
+    if (left >= 0) parentOfNode[left] = i; else parentOfLeaf[~left] = i;
+    if (right >= 0) parentOfNode[right] = i; else parentOfLeaf[~right] = i;
+    if (i == 0) parentOfNode[0] = -1;
+}
+
+__device__ __forceinline__ void triBox(const float* verts, uint32_t prim, V3* lo, V3* hi) {
+    V3 a = loadVertex(verts, prim, 0), b = loadVertex(verts, prim, 1), c = loadVertex(verts, prim, 2);
+    *lo = vmin3(vmin3(a, b), c);
+    *hi = vmax3(vmax3(a, b), c);
+}
+
+// Bottom-up refit: the second thread to arrive at a node computes its two
+// child boxes (the first one exits), so every node is written exactly once.
+__global__ void refitKernel(const float* verts, const uint32_t* sortedPrims, int n, const int32_t* children,
+                            const int32_t* parentOfNode, const int32_t* parentOfLeaf, uint32_t* arrivals,
+                            float* nodeBox /* [n-1][6] */, BvhNode* nodes) {
+    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    int node = parentOfLeaf[leaf];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1u) == 0u) return;
+        __threadfence();
+        V3 lo[2], hi[2];
+        int c[2] = { children[2 * node + 0], children[2 * node + 1] };
+        for (int k = 0; k < 2; ++k) {
+            if (c[k] < 0) {
+                triBox(verts, sortedPrims[~c[k]], &lo[k], &hi[k]);
+            }
+            else {
+                const float* b = nodeBox + 6 * c[k];
+                lo[k] = V3(__ldcg(b + 0), __ldcg(b + 1), __ldcg(b + 2));
+                hi[k] = V3(__ldcg(b + 3), __ldcg(b + 4), __ldcg(b + 5));
+            }
+        }
+        V3 ulo = vmin3(lo[0], lo[1]), uhi = vmax3(hi[0], hi[1]);
+        float* ob = nodeBox + 6 * node;
+        __stcg(ob + 0, ulo.x); __stcg(ob + 1, ulo.y); __stcg(ob + 2, ulo.z);
+        __stcg(ob + 3, uhi.x); __stcg(ob + 4, uhi.y); __stcg(ob + 5, uhi.z);
+        BvhNode nd;
+        nd.lo0 = make_float4(lo[0].x, lo[0].y, lo[0].z, __int_as_float(c[0]));
+        nd.hi0 = make_float4(hi[0].x, hi[0].y, hi[0].z, 0.0f);
+        nd.lo1 = make_float4(lo[1].x, lo[1].y, lo[1].z, __int_as_float(c[1]));
+        nd.hi1 = make_float4(hi[1].x, hi[1].y, hi[1].z, 0.0f);
+        nodes[node] = nd;
+        node = parentOfNode[node];
+    }
+}
+
+__global__ void packTrisKernel(const float* verts, const uint32_t* sortedPrims, uint32_t n, BvhTri* tris) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t p = sortedPrims[i];
+    V3 a = loadVertex(verts, p, 0), b = loadVertex(verts, p, 1), c = loadVertex(verts, p, 2);
+    V3 e1 = b - a, e2 = c - a;
+    BvhTri t;
+    t.v0 = make_float4(a.x, a.y, a.z, __uint_as_float(p));
+    t.e1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
+    t.e2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+    tris[i] = t;
+}
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string("lbvh ") + what + ": " + cudaGetErrorString(e));
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+} // namespace
+
+size_t lbvhScratchBytes(uint32_t n) {
+    const size_t numTiles = (n + kSortTile - 1) / kSortTile;
+    size_t b = 0;
+    b += align256(6 * 4);                       // ordered centroid box
+    b += 4 * align256(size_t(n) * 4);           // codes/prims ping-pong
+    b += align256(size_t(kRadix) * numTiles * 4); // histogram
+    b += align256(size_t(n) * 4);               // parentOfLeaf
+    b += align256(size_t(n) * 4);               // parentOfNode
+    b += align256(size_t(n) * 4);               // arrivals
+    b += align256(size_t(n) * 24);              // node boxes
+    return b;
+}
+
+void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, cudaStream_t stream) {
+    if (n == 0) return;
+    char* s = static_cast<char*>(scratch);
+    auto take = [&](size_t bytes) { char* p = s; s += align256(bytes); return p; };
+    const uint32_t numTiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* ordBox = reinterpret_cast<uint32_t*>(take(6 * 4));
+    uint32_t* keysA = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    uint32_t* valsA = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    uint32_t* keysB = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    uint32_t* valsB = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    uint32_t* hist = reinterpret_cast<uint32_t*>(take(size_t(kRadix) * numTiles * 4));
+    int32_t* parentOfLeaf = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    int32_t* parentOfNode = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    uint32_t* arrivals = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    float* nodeBox = reinterpret_cast<float*>(take(size_t(n) * 24));
+
+    const uint32_t init[6] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u };
+    ck(cudaMemcpyAsync(ordBox, init, sizeof(init), cudaMemcpyHostToDevice, stream), "init box");
+    const uint32_t tb = 256;
+    const uint32_t blocks = (n + tb - 1) / tb;
+    const uint32_t redBlocks = blocks < 1184 ? blocks : 1184;
+    centroidBoundsKernel<<<redBlocks, tb, 0, stream>>>(verts, n, ordBox);
+    mortonKernel<<<blocks, tb, 0, stream>>>(verts, n, ordBox, keysA, valsA);
+    uint32_t* kin = keysA; uint32_t* vin = valsA; uint32_t* kout = keysB; uint32_t* vout = valsB;
+    for (int shift = 0; shift < 30; shift += 4) {
+        radixHistKernel<<<numTiles, kSortThreads, 0, stream>>>(kin, n, shift, hist);
+        radixScanKernel<<<1, 1024, 0, stream>>>(hist, kRadix * numTiles);
+        radixScatterKernel<<<numTiles, kSortThreads, 0, stream>>>(kin, vin, n, shift, hist, kout, vout);
+        uint32_t* t = kin; kin = kout; kout = t;
+        t = vin; vin = vout; vout = t;
+    }
+    ck(cudaMemcpyAsync(out->sortedCodes, kin, size_t(n) * 4, cudaMemcpyDeviceToDevice, stream), "codes");
+    ck(cudaMemcpyAsync(out->sortedPrims, vin, size_t(n) * 4, cudaMemcpyDeviceToDevice, stream), "prims");
+    if (n > 1) {
+        ck(cudaMemsetAsync(arrivals, 0, size_t(n) * 4, stream), "arrivals");
+        karrasKernel<<<(n - 1 + tb - 1) / tb, tb, 0, stream>>>(out->sortedCodes, static_cast<int>(n),
+                                                                out->children, parentOfNode, parentOfLeaf);
+        refitKernel<<<blocks, tb, 0, stream>>>(verts, out->sortedPrims, static_cast<int>(n), out->children,
+                                               parentOfNode, parentOfLeaf, arrivals, nodeBox, out->nodes);
+        ck(cudaMemcpyAsync(out->nodeBoxes, nodeBox, size_t(n - 1) * 24, cudaMemcpyDeviceToDevice, stream), "boxes");
+    }
+    packTrisKernel<<<blocks, tb, 0, stream>>>(verts, out->sortedPrims, n, out->tris);
+    ck(cudaGetLastError(), "launch");
+}
+
+} // namespace vlrb

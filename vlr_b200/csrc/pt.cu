@@ -1,0 +1,487 @@
+// Wavefront spectral path tracer with MIS next-event estimation.
+//
+// Per launch (one or more samples per pixel):
+//   cameraKernel      camera rays for every path slot (path_tracing.cu:30-77)
+//   per bounce b:
+//     traceKernel     closest hit of the active rays, then the path index is
+//                     appended to the queue of the hit material's BSDF kind
+//                     (or the miss queue): material-sorted shading
+//     shadeKernel     walks the sorted queues; implicit emission with MIS,
+//                     Russian roulette, NEE light sample, BSDF sample
+//                     (path_tracing.cu:133-259, miss :266-337)
+//     shadowKernel    any-hit visibility of the NEE rays; adds their
+//                     contribution when unoccluded
+//   filmKernel        bins each path's 4-wavelength contribution into 16 FP64
+//                     strata of its pixel (spectrum_types.h:674-684)
+// Queue lengths live in device counters, so a launch never synchronises with
+// the host and its fixed kernel sequence can be captured in a CUDA graph.
+#include "pt.cuh"
+#include "tables.cuh"
+
+#include <random>
+#include <stdexcept>
+#include <string>
+
+namespace vlrb {
+
+namespace {
+
+__device__ __forceinline__ uint32_t* bounceCounters(const PathBuffers &pb, uint32_t b) {
+    return pb.counters + b * kCountersPerBounce;
+}
+
+// Warp-aggregated append: lanes with the same queue share one atomic.
+__device__ __forceinline__ uint32_t appendSlot(uint32_t* counter, uint32_t key) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (static_cast<int>(lane) == leader)
+        base = atomicAdd(counter, static_cast<uint32_t>(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ WLS loadWls(const PathBuffers &pb, uint32_t p) {
+    float4 l = pb.lambda[p];
+    uint32_t f = pb.flags[p];
+    WLS w;
+    w.lambda[0] = l.x; w.lambda[1] = l.y; w.lambda[2] = l.z; w.lambda[3] = l.w;
+    w.selected = f & 0xFu;
+    w.single = (f >> 4) & 1u;
+    return w;
+}
+
+__device__ __forceinline__ S4 toS4(const float4 &v) { S4 s; s[0] = v.x; s[1] = v.y; s[2] = v.z; s[3] = v.w; return s; }
+__device__ __forceinline__ float4 toF4(const S4 &s) { return make_float4(s[0], s[1], s[2], s[3]); }
+
+__global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
+    const uint32_t P = fp.numPaths;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const uint32_t pixel = p % (fp.width * fp.height);
+        const uint32_t px = pixel % fp.width, py = pixel / fp.width;
+        PCG32 rng{ pb.rng[p] };
+        float jx = rng.uniform(), jy = rng.uniform();
+        float fx = px + jx, fy = py + jy;
+        float selectWLPDF;
+        float wo = rng.uniform(), ws = rng.uniform();
+        WLS wls = WLS::equalOffsets(wo, ws, &selectWLPDF);
+        // PerspectiveCamera_sample (cameras.cu:42-74)
+        const Camera &C = S.cam;
+        float lx, ly;
+        float l0 = rng.uniform(), l1 = rng.uniform();
+        concentricDisk(l0, l1, &lx, &ly);
+        V3 orgLocal(C.lensRadius * lx, C.lensRadius * ly, 0.0f);
+        V3 gn = normalize(C.forward);
+        Frame camFrame;
+        camFrame.z = gn;
+        camFrame.x = normalize(C.right);
+        camFrame.y = cross(camFrame.z, camFrame.x);
+        V3 lensPos = C.right * orgLocal.x + C.up * orgLocal.y + C.forward * orgLocal.z + C.position;
+        float areaPDF = C.lensRadius > 0.0f ? 1.0f / (kPi * C.lensRadius * C.lensRadius) : 1.0f;
+        // PerspectiveCameraIDF::sampleInternal (cameras.cu:142-155)
+        float u0 = fx / fp.width, u1 = fy / fp.height;
+        V3 pFocus(C.opWidth * (0.5f - u0), C.opHeight * (0.5f - u1), C.objPlaneDistance);
+        V3 dirLocal = normalize(pFocus - V3(C.lensRadius * lx, C.lensRadius * ly, 0.0f));
+        float dirPDF = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
+        dirPDF *= static_cast<float>(fp.width * fp.height);
+        V3 rayDir = camFrame.fromLocal(dirLocal);
+        S4 We0(C.sensitivity);
+        S4 alpha = (We0 * S4::one()) * (absDot(rayDir, gn) / (areaPDF * dirPDF * selectWLPDF));
+        pb.rng[p] = rng.state;
+        pb.lambda[p] = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
+        pb.flags[p] = wls.selected;
+        pb.alpha[p] = toF4(alpha);
+        pb.contrib[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pb.initImportance[p] = alpha.importance(wls.selected);
+        pb.prevDirPDF[p] = dirPDF;
+        pb.prevType[p] = dir::Acquisition | dir::LowFreq;
+        pb.rayOrg[p] = make_float4(lensPos.x, lensPos.y, lensPos.z, FLT_MAX);
+        pb.rayDir[p] = make_float4(rayDir.x, rayDir.y, rayDir.z, 0.0f);
+        pb.active[0][p] = p;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) bounceCounters(pb, 0)[kCntActive] = P;
+}
+
+__global__ void __launch_bounds__(256) traceKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
+    uint32_t* ctr = bounceCounters(pb, fp.bounce);
+    const uint32_t n = ctr[kCntActive];
+    const uint32_t* queue = pb.active[fp.bounce & 1];
+    const uint32_t P = fp.numPaths;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = queue[i];
+        float4 o = pb.rayOrg[p], d = pb.rayDir[p];
+        Hit h = traceBvh<false>(S.bvh, V3(o.x, o.y, o.z), V3(d.x, d.y, d.z), o.w);
+        pb.hit[p] = make_float4(h.t, h.b1, h.b2, __uint_as_float(h.prim));
+        uint32_t key = kNumBsdfKinds;
+        if (h.prim != 0xFFFFFFFFu)
+            key = S.mats[__ldg(S.triMaterial + h.prim)].bsdfKind;
+        uint32_t slot = appendSlot(ctr + kCntBucket0 + key, key);
+        pb.buckets[key * P + slot] = p;
+    }
+}
+
+// Environment contribution for a ray that left the scene
+// (path_tracing.cu:266-337).
+__device__ __forceinline__ void shadeMiss(const SceneGPU &S, const PathBuffers &pb, uint32_t p, const WLS &wls,
+                                          uint32_t pathLength, S4 &contrib) {
+    if (S.envInst < 0) return;
+    float4 d4 = pb.rayDir[p];
+    V3 direction(d4.x, d4.y, d4.z);
+    float phi, theta;
+    toPolarYUp(direction, &theta, &phi);
+    float posPhi = phi;
+    phi += S.envRotation;
+    phi = phi - floorf(phi / (2 * kPi)) * 2 * kPi;
+    float tu = phi / (2 * kPi), tv = theta / kPi;
+    float uvPDF = envPdfUV(S.env, tu, tv);
+    float hypAreaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
+    const MatDesc &m = S.mats[S.envMaterial];
+    // EnvironmentEDF: emittance pi*E, directional factor 1/pi for the
+    // direction facing the scene (materials.cu:2830-2893).
+    S4 E = envRadiance(S, tu, tv, wls) * m.emitScale;
+    S4 spEmittance = kPi * E;
+    (void)posPhi;
+    if (!spEmittance.hasNonZero()) return;
+    S4 Le = spEmittance * (1.0f / kPi);
+    float MIS = 1.0f;
+    uint32_t prevType = pb.prevType[p];
+    if (!dir::isDelta(prevType) && pathLength > 1) {
+        float bsdfPDF = pb.prevDirPDF[p];
+        float lightPDF = S.envLightProb * hypAreaPDF * 1.0f / 1.0f;
+        MIS = (bsdfPDF * bsdfPDF) / (lightPDF * lightPDF + bsdfPDF * bsdfPDF);
+    }
+    contrib += toS4(pb.alpha[p]) * Le * MIS;
+}
+
+__global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
+    uint32_t* ctr = bounceCounters(pb, fp.bounce);
+    uint32_t* next = bounceCounters(pb, fp.bounce + 1);
+    __shared__ uint32_t sOff[kNumShadeBuckets + 1];
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < kNumShadeBuckets; ++k) { sOff[k] = run; run += ctr[kCntBucket0 + k]; }
+        sOff[kNumShadeBuckets] = run;
+    }
+    __syncthreads();
+    const uint32_t total = sOff[kNumShadeBuckets];
+    const uint32_t P = fp.numPaths;
+    uint32_t* nextQueue = pb.active[(fp.bounce + 1) & 1];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        uint32_t k = 0;
+        while (j >= sOff[k + 1]) ++k;
+        const uint32_t p = pb.buckets[k * P + (j - sOff[k])];
+        WLS wls = loadWls(pb, p);
+        uint32_t flags = pb.flags[p];
+        uint32_t pathLength = ((flags >> 8) & 0xFFFFu) + 1;
+        bool maxLengthTerminate = pathLength >= fp.maxPathLength;
+        flags = (flags & 0x1Fu) | (pathLength << 8) | (maxLengthTerminate ? 0x20u : 0u);
+        S4 contrib = toS4(pb.contrib[p]);
+        if (k == kNumBsdfKinds) {
+            shadeMiss(S, pb, p, wls, pathLength, contrib);
+            pb.contrib[p] = toF4(contrib);
+            pb.flags[p] = flags;
+            continue;
+        }
+        float4 h = pb.hit[p];
+        const uint32_t prim = __float_as_uint(h.w);
+        SurfPt sp;
+        float hypAreaPDF;
+        decodeHit(S, prim, h.y, h.z, &sp, &hypAreaPDF);
+        const MatDesc &mat = S.mats[__ldg(S.triMaterial + prim)];
+        Bsdf bsdf = buildBsdf(S.meng, mat, wls);
+        float4 o4 = pb.rayOrg[p], d4 = pb.rayDir[p];
+        V3 rayOrg(o4.x, o4.y, o4.z), rayDir(d4.x, d4.y, d4.z);
+        V3 dirOutLocal = sp.frame.toLocal(-rayDir);
+        S4 alpha = toS4(pb.alpha[p]);
+        // implicit light sampling
+        S4 spEmittance = emittance(S.meng, mat, wls);
+        if (spEmittance.hasNonZero()) {
+            S4 Le = spEmittance * diffuseEdfEval(dirOutLocal);
+            float MIS = 1.0f;
+            if (!dir::isDelta(pb.prevType[p]) && pathLength > 1) {
+                float bsdfPDF = pb.prevDirPDF[p];
+                float dist2 = (sp.position - rayOrg).sqLength();
+                float lightPDF = __ldg(S.geomLightPdfArea + sp.geomInst) * hypAreaPDF * dist2 /
+                                 fabsf(dirOutLocal.z);
+                MIS = (bsdfPDF * bsdfPDF) / (lightPDF * lightPDF + bsdfPDF * bsdfPDF);
+            }
+            contrib += alpha * Le * MIS;
+        }
+        pb.contrib[p] = toF4(contrib);
+        pb.flags[p] = flags;
+        if (maxLengthTerminate) continue;
+        PCG32 rng{ pb.rng[p] };
+        // Russian roulette on the hero-weighted throughput
+        float continueProb = fminf(alpha.importance(wls.selected) / pb.initImportance[p], 1.0f);
+        if (rng.uniform() >= continueProb) { pb.rng[p] = rng.state; continue; }
+        alpha /= continueProb;
+        V3 gnLocal = sp.frame.toLocal(sp.gn);
+        BsdfQuery q;
+        q.dirLocal = dirOutLocal;
+        q.wlHint = wls.selected;
+        q.filter = dir::All;
+        q.importanceMode = 0;
+        // next-event estimation
+        if (bsdfHasNonDelta(bsdf) && S.lightInsts.n > 0) {
+            float uLight = rng.uniform();
+            float instProb, uInst;
+            uint32_t li = S.lightInsts.sample(uLight, &instProb, &uInst);
+            float ue0 = rng.uniform(), ue1 = rng.uniform();
+            LightSample ls;
+            float lightProb;
+            S4 M;
+            bool ok = true;
+            if (static_cast<int32_t>(li) == S.envInst) {
+                // sampleInfiniteSphere (infinite_sphere.cu:60-114)
+                float groupProb, uPrim;
+                S.instGroups[li].sample(uInst, &groupProb, &uPrim);
+                lightProb = instProb * groupProb;
+                float uu, vv, uvPDF;
+                envSampleUV(S.env, ue0, ue1, &uu, &vv, &uvPDF);
+                float phi = 2 * kPi * uu, theta = kPi * vv;
+                float posPhi = phi - S.envRotation;
+                posPhi = posPhi - floorf(posPhi / (2 * kPi)) * 2 * kPi;
+                V3 dirE = dirFromPolarYUp(posPhi, theta);
+                ls.sp.position = dirE;
+                ls.sp.gn = -dirE;
+                ls.sp.frame.z = -dirE;
+                ls.sp.atInfinity = true;
+                ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
+                ls.delta = false;
+                ls.material = S.envMaterial;
+                M = kPi * envRadiance(S, uu, vv, wls) * S.mats[S.envMaterial].emitScale;
+                ok = uvPDF > 0.0f;
+            }
+            else {
+                float groupProb, uPrim;
+                uint32_t g = S.instGroups[li].sample(uInst, &groupProb, &uPrim);
+                lightProb = instProb * groupProb;
+                uint32_t grp = __ldg(S.instFirstGroup + li) + g;
+                sampleTriangleGroup(S, grp, uPrim, ue0, ue1, &ls);
+                M = emittance(S.meng, S.mats[ls.material], wls);
+            }
+            if (ok && M.hasNonZero()) {
+                // testVisibility (light_transport_common.h:147-177)
+                V3 shadowDir;
+                float dist2;
+                if (ls.sp.atInfinity) { shadowDir = normalize(ls.sp.position); dist2 = 1.0f; }
+                else {
+                    V3 dv = ls.sp.position - sp.position;
+                    dist2 = dv.sqLength();
+                    shadowDir = dv / sqrtf(dist2);
+                }
+                bool front = dot(sp.gn, shadowDir) > 0;
+                V3 sOrg = offsetRayOrigin(sp.position, front ? sp.gn : -sp.gn);
+                float tmax = FLT_MAX;
+                if (!ls.sp.atInfinity) {
+                    bool lfront = -dot(ls.sp.gn, shadowDir) > 0;
+                    V3 lPt = offsetRayOrigin(ls.sp.position, lfront ? ls.sp.gn : -ls.sp.gn);
+                    tmax = (lPt - sOrg).length() * 0.9999f;
+                }
+                float recSqDist = 1.0f / dist2;
+                V3 dirL = ls.sp.atInfinity ? V3(0.0f, 0.0f, 1.0f) : ls.sp.frame.toLocal(-shadowDir);
+                V3 dirSn = sp.frame.toLocal(shadowDir);
+                S4 Le = M * diffuseEdfEval(dirL);
+                float lightPDF = lightProb * ls.areaPDF;
+                S4 fs = bsdfEval(bsdf, q, gnLocal, dirSn, nullptr);
+                float cosLight = ls.sp.atInfinity ? absDot(-shadowDir, ls.sp.gn) : absDot(-shadowDir, ls.sp.gn);
+                float bsdfPdfV = bsdfPDF(bsdf, q, dirSn, nullptr) * cosLight * recSqDist;
+                float MIS = 1.0f;
+                if (!ls.delta && !isinf(lightPDF))
+                    MIS = (lightPDF * lightPDF) / (lightPDF * lightPDF + bsdfPdfV * bsdfPdfV);
+                float G = absDot(dirSn, gnLocal) * cosLight * recSqDist;
+                float scalar = G * MIS / lightPDF;
+                S4 c = alpha * Le * fs * scalar;
+                if (c.hasNonZero()) {
+                    uint32_t slot = appendSlot(ctr + kCntShadow, 0u);
+                    ShadowRay sr;
+                    sr.org = make_float4(sOrg.x, sOrg.y, sOrg.z, tmax);
+                    sr.dir = make_float4(shadowDir.x, shadowDir.y, shadowDir.z, __uint_as_float(p));
+                    sr.contrib = toF4(c);
+                    pb.shadow[slot] = sr;
+                }
+            }
+        }
+        // BSDF sampling
+        float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
+        pb.rng[p] = rng.state;
+        BsdfSample bs;
+        S4 fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
+        if (fs.isZero() || bs.dirPDF == 0.0f) continue;
+        if (dir::isDispersive(bs.sampledType) && !wls.single) {
+            bs.dirPDF /= kNumLambdas;
+            flags |= 0x10u;
+            pb.flags[p] = flags;
+        }
+        float cosFactor = dot(bs.dirLocal, gnLocal);
+        alpha *= fs * (fabsf(cosFactor) / bs.dirPDF);
+        V3 dirIn = sp.frame.fromLocal(bs.dirLocal);
+        V3 org = offsetRayOrigin(sp.position, cosFactor > 0.0f ? sp.gn : -sp.gn);
+        pb.alpha[p] = toF4(alpha);
+        pb.prevDirPDF[p] = bs.dirPDF;
+        pb.prevType[p] = bs.sampledType;
+        pb.rayOrg[p] = make_float4(org.x, org.y, org.z, FLT_MAX);
+        pb.rayDir[p] = make_float4(dirIn.x, dirIn.y, dirIn.z, 0.0f);
+        uint32_t slot = appendSlot(next + kCntActive, 0u);
+        nextQueue[slot] = p;
+    }
+}
+
+__global__ void __launch_bounds__(256) shadowKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
+    const uint32_t n = bounceCounters(pb, fp.bounce)[kCntShadow];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        ShadowRay sr = pb.shadow[i];
+        Hit h = traceBvh<true>(S.bvh, V3(sr.org.x, sr.org.y, sr.org.z), V3(sr.dir.x, sr.dir.y, sr.dir.z), sr.org.w);
+        if (h.prim == 0xFFFFFFFFu) {
+            uint32_t p = __float_as_uint(sr.dir.w);
+            float4 c = pb.contrib[p];
+            c.x += sr.contrib.x; c.y += sr.contrib.y; c.z += sr.contrib.z; c.w += sr.contrib.w;
+            pb.contrib[p] = c;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) filmKernel(PathBuffers pb, Film film, FrameParams fp) {
+    const uint32_t P = fp.numPaths;
+    const float recBinWidth = kNumStrata / (kWavelengthHigh - kWavelengthLow);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        S4 c = toS4(pb.contrib[p]);
+        if (!c.allFinite()) continue;
+        float4 l = pb.lambda[p];
+        float lam[4] = { l.x, l.y, l.z, l.w };
+        const uint32_t pixel = p % (fp.width * fp.height);
+        double* dst = film.strata + static_cast<size_t>(pixel) * kNumStrata;
+        for (int i = 0; i < 4; ++i) {
+            uint32_t bin = vmin<uint32_t>(static_cast<uint32_t>((lam[i] - kWavelengthLow) /
+                                          (kWavelengthHigh - kWavelengthLow) * kNumStrata), kNumStrata - 1);
+            float v = c[i] * recBinWidth;
+            if (v != 0.0f) atomicAdd(dst + bin, static_cast<double>(v));
+        }
+    }
+}
+
+struct FilmConst {
+    float xbar[kNumStrata], ybar[kNumStrata], zbar[kNumStrata];
+    float integralCMF;
+    float xyzToRgb[9];
+};
+
+__global__ void filmToRGBAKernel(Film film, uint32_t frames, FilmConst fc, float4* out) {
+    const uint32_t n = film.width * film.height;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double* s = film.strata + static_cast<size_t>(i) * kNumStrata;
+        double X = 0, Y = 0, Z = 0;
+        for (uint32_t k = 0; k < kNumStrata; ++k) {
+            double v = s[k];
+            X += fc.xbar[k] * v;
+            Y += fc.ybar[k] * v;
+            Z += fc.zbar[k] * v;
+        }
+        double scale = static_cast<double>(n) / (static_cast<double>(fc.integralCMF) * frames);
+        float xyz[3] = { static_cast<float>(X * scale), static_cast<float>(Y * scale), static_cast<float>(Z * scale) };
+        float rgb[3];
+        mulColMajor(fc.xyzToRgb, xyz, rgb);
+        out[i] = make_float4(rgb[0], rgb[1], rgb[2], 1.0f);
+    }
+}
+
+// Adds this launch's per-bounce queue lengths to the running totals.
+__global__ void statsKernel(PathBuffers pb, uint32_t bounces) {
+    unsigned long long seg = 0, sh = 0;
+    for (uint32_t b = threadIdx.x; b < bounces; b += 32) {
+        seg += bounceCounters(pb, b)[kCntActive];
+        sh += bounceCounters(pb, b)[kCntShadow];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        seg += __shfl_xor_sync(0xFFFFFFFFu, seg, off);
+        sh += __shfl_xor_sync(0xFFFFFFFFu, sh, off);
+    }
+    if (threadIdx.x == 0) { pb.totals[0] += seg; pb.totals[1] += sh; }
+}
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string("pt ") + what + ": " + cudaGetErrorString(e));
+}
+
+inline size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
+
+} // namespace
+
+size_t pathBufferBytes(uint32_t P) {
+    size_t b = 0;
+    b += a256(size_t(P) * 8);                 // rng
+    b += a256(size_t(P) * 16) * 2;            // lambda, alpha
+    b += a256(size_t(P) * 4) * 4;             // flags, initImportance, prevDirPDF, prevType
+    b += a256(size_t(P) * 16) * 4;            // contrib, rayOrg, rayDir, hit
+    b += a256(size_t(P) * 4) * 2;             // active queues
+    b += a256(size_t(P) * 4 * kNumShadeBuckets);
+    b += a256(size_t(P) * sizeof(ShadowRay));
+    b += a256(size_t(kMaxBounces + 1) * kCountersPerBounce * 4);
+    b += a256(16);
+    return b;
+}
+
+void carvePathBuffers(void* base, uint32_t P, PathBuffers* pb) {
+    char* s = static_cast<char*>(base);
+    auto take = [&](size_t bytes) { char* r = s; s += a256(bytes); return r; };
+    pb->rng = reinterpret_cast<uint64_t*>(take(size_t(P) * 8));
+    pb->lambda = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->alpha = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->flags = reinterpret_cast<uint32_t*>(take(size_t(P) * 4));
+    pb->initImportance = reinterpret_cast<float*>(take(size_t(P) * 4));
+    pb->prevDirPDF = reinterpret_cast<float*>(take(size_t(P) * 4));
+    pb->prevType = reinterpret_cast<uint32_t*>(take(size_t(P) * 4));
+    pb->contrib = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->rayOrg = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->rayDir = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->hit = reinterpret_cast<float4*>(take(size_t(P) * 16));
+    pb->active[0] = reinterpret_cast<uint32_t*>(take(size_t(P) * 4));
+    pb->active[1] = reinterpret_cast<uint32_t*>(take(size_t(P) * 4));
+    pb->buckets = reinterpret_cast<uint32_t*>(take(size_t(P) * 4 * kNumShadeBuckets));
+    pb->shadow = reinterpret_cast<ShadowRay*>(take(size_t(P) * sizeof(ShadowRay)));
+    pb->counters = reinterpret_cast<uint32_t*>(take(size_t(kMaxBounces + 1) * kCountersPerBounce * 4));
+    pb->totals = reinterpret_cast<unsigned long long*>(take(16));
+}
+
+void seedPathRngs(uint64_t* states, uint32_t n, uint64_t seed) {
+    std::mt19937_64 gen(seed);
+    for (uint32_t i = 0; i < n; ++i) states[i] = gen();
+}
+
+void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fpIn,
+                    int numSMs, cudaStream_t stream) {
+    FrameParams fp = fpIn;
+    if (fp.maxPathLength == 0 || fp.maxPathLength > kMaxBounces)
+        throw std::runtime_error("maxPathLength out of range");
+    ck(cudaMemsetAsync(pb.counters, 0, size_t(kMaxBounces + 1) * kCountersPerBounce * 4, stream), "counters");
+    const int grid = numSMs * 8;
+    cameraKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+    for (uint32_t b = 0; b < fp.maxPathLength; ++b) {
+        fp.bounce = b;
+        traceKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        shadeKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        shadowKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+    }
+    filmKernel<<<grid, 256, 0, stream>>>(pb, film, fp);
+    statsKernel<<<1, 32, 0, stream>>>(pb, fp.maxPathLength);
+    ck(cudaGetLastError(), "launch");
+}
+
+void filmClear(const Film &film, cudaStream_t stream) {
+    ck(cudaMemsetAsync(film.strata, 0, size_t(film.width) * film.height * kNumStrata * 8, stream), "film clear");
+}
+
+void filmToRGBA(const Film &film, uint32_t frames, float4* out, cudaStream_t stream) {
+    FilmConst fc;
+    const CmfStrata &cs = hostCmfStrata();
+    for (uint32_t k = 0; k < kNumStrata; ++k) { fc.xbar[k] = cs.xbar[k]; fc.ybar[k] = cs.ybar[k]; fc.zbar[k] = cs.zbar[k]; }
+    fc.integralCMF = cs.integralCMF;
+    for (int k = 0; k < 9; ++k) fc.xyzToRgb[k] = hostColorMatrices().xyzToRec709D65[k];
+    const uint32_t n = film.width * film.height;
+    filmToRGBAKernel<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, stream>>>(film, frames ? frames : 1, fc, out);
+    ck(cudaGetLastError(), "film convert");
+}
+
+} // namespace vlrb

@@ -1,0 +1,83 @@
+// Wavefront path tracer: device buffers and host launch interface.
+#pragma once
+
+#include "scene_gpu.cuh"
+#include <cuda_runtime.h>
+
+namespace vlrb {
+
+constexpr uint32_t kNumShadeBuckets = kNumBsdfKinds + 1;  // + miss
+constexpr uint32_t kCountersPerBounce = 16;
+constexpr uint32_t kMaxBounces = 64;
+
+// Counter slots within one bounce's block of kCountersPerBounce words.
+enum : uint32_t {
+    kCntActive = 0,          // rays to trace this bounce
+    kCntShadow = 1,          // shadow rays emitted by this bounce's shading
+    kCntBucket0 = 2,         // material-sorted hit queues (kNumShadeBuckets)
+};
+
+struct ShadowRay {
+    float4 org;      // xyz, w = tmax
+    float4 dir;      // xyz, w = path index (bits)
+    float4 contrib;  // contribution if unoccluded
+};
+
+// Per-path state, structure of arrays (P = number of path slots).
+struct PathBuffers {
+    uint64_t* rng;
+    float4* lambda;
+    uint32_t* flags;          // bits 0-3 hero index, 4 single, 5 max-length, 8-23 path length
+    float4* alpha;
+    float4* contrib;
+    float* initImportance;
+    float* prevDirPDF;
+    uint32_t* prevType;
+    float4* rayOrg;
+    float4* rayDir;
+    float4* hit;              // t, b1, b2, prim bits
+    uint32_t* active[2];
+    uint32_t* buckets;        // [kNumShadeBuckets][P]
+    ShadowRay* shadow;        // [P]
+    uint32_t* counters;       // [kMaxBounces + 1][kCountersPerBounce]
+    unsigned long long* totals;  // [0] extension rays traced, [1] shadow rays (never reset)
+};
+
+struct FrameParams {
+    uint32_t width, height;
+    uint32_t sppPerLaunch;    // paths per pixel in this launch
+    uint32_t numPaths;        // width * height * sppPerLaunch
+    uint32_t maxPathLength;   // hits after which a path stops scattering
+    uint32_t bounce;          // current bounce (0-based)
+};
+
+// Film: 16 FP64 strata per pixel, [pixel][16].
+struct Film {
+    double* strata;
+    uint32_t width, height;
+};
+
+size_t pathBufferBytes(uint32_t numPaths);
+void carvePathBuffers(void* base, uint32_t numPaths, PathBuffers* pb);
+
+// Seeds every path slot's PCG32 state from std::mt19937_64 in slot order, the
+// reference's per-pixel seeding (context.cpp:1176-1190) for one slot per pixel.
+void seedPathRngs(uint64_t* hostStates, uint32_t numSlots, uint64_t seed);
+
+struct PTStats {
+    uint64_t segments;        // extension rays traced
+    uint64_t shadowRays;
+};
+
+// Render one launch of sppPerLaunch samples per pixel and accumulate the film.
+// counterHost (pinned, optional) receives the per-bounce counters after the
+// launch for statistics.
+void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fp,
+                    int numSMs, cudaStream_t stream);
+
+// Convert the FP64 film to RGBA32F: XYZ / frames * (W*H) -> Rec.709 D65
+// (post_process.cu:93-163).
+void filmToRGBA(const Film &film, uint32_t numAccumFrames, float4* out, cudaStream_t stream);
+void filmClear(const Film &film, cudaStream_t stream);
+
+} // namespace vlrb

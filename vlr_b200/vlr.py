@@ -1,0 +1,334 @@
+"""Python mirror of the reference's vlrcpp.h wrapper over the C API.
+
+Names follow libVLR/include/vlr/vlrcpp.h (Context::create, createScene,
+createTriangleMeshSurfaceNode, createSurfaceMaterial, createCamera, render);
+errors raise VLRError the way vlrcpp's errorCheck throws
+(vlrcpp.h:697-701).  Every call goes through libvlr_b200.so's C ABI.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import lib, check, VLRError
+
+c_void_p = ctypes.c_void_p
+
+
+class VLRVertex(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("normal", ctypes.c_float * 3),
+                ("tc0Direction", ctypes.c_float * 3), ("texCoord", ctypes.c_float * 2)]
+
+
+class VLRImmediateSpectrum(ctypes.Structure):
+    _fields_ = [("colorSpace", ctypes.c_char_p), ("e0", ctypes.c_float), ("e1", ctypes.c_float),
+                ("e2", ctypes.c_float)]
+
+
+class VLRShaderNodePlug(ctypes.Structure):
+    _fields_ = [("nodeRef", ctypes.c_size_t), ("info", ctypes.c_uint32)]
+
+
+class VLRBRenderOptions(ctypes.Structure):
+    _fields_ = [("maxPathLength", ctypes.c_uint32), ("maxPathsInFlight", ctypes.c_uint32),
+                ("lightPathsPerFrame", ctypes.c_uint32)]
+
+
+class VLRBRenderStats(ctypes.Structure):
+    _fields_ = [("pathSegments", ctypes.c_uint64), ("shadowRays", ctypes.c_uint64), ("frames", ctypes.c_uint64),
+                ("lightVertexOverflow", ctypes.c_uint32), ("numTriangles", ctypes.c_uint32)]
+
+
+RENDERER_PATH_TRACING = 0
+RENDERER_BPT = 2
+PLUG_SPECTRUM = 7
+
+
+def _api():
+    L = lib()
+    if getattr(L, "_vlr_sigs", False):
+        return L
+    v = c_void_p
+    sigs = {
+        "vlrCreateContext": [v, ctypes.c_bool, ctypes.c_uint32, ctypes.POINTER(v)],
+        "vlrDestroyContext": [v],
+        "vlrContextBindOutputBuffer": [v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
+        "vlrContextGetOutputBufferSize": [v, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)],
+        "vlrContextReadOutputBuffer": [v, v],
+        "vlrContextSetScene": [v, v],
+        "vlrContextSetRenderer": [v, ctypes.c_int],
+        "vlrContextRender": [v, v, v, ctypes.c_bool, ctypes.c_uint32, ctypes.c_bool, ctypes.c_uint32,
+                             ctypes.POINTER(ctypes.c_uint32)],
+        "vlrSurfaceMaterialCreate": [v, ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrShaderNodeCreate": [v, ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrShaderNodeGetPlug": [v, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(VLRShaderNodePlug)],
+        "vlrQueryableSetImmediateSpectrum": [v, ctypes.c_char_p, ctypes.POINTER(VLRImmediateSpectrum)],
+        "vlrQueryableSetFloat": [v, ctypes.c_char_p, ctypes.c_float],
+        "vlrQueryableSetFloatTuple": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float), ctypes.c_uint32],
+        "vlrQueryableSetPoint3D": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 3)],
+        "vlrQueryableSetQuaternion": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 4)],
+        "vlrQueryableSetImage2D": [v, ctypes.c_char_p, v],
+        "vlrQueryableSetShaderNodePlug": [v, ctypes.c_char_p, VLRShaderNodePlug],
+        "vlrQueryableGetFloat": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)],
+        "vlrQueryableGetNumParameters": [v, ctypes.POINTER(ctypes.c_uint32)],
+        "vlrLinearImage2DCreate": [v, v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p,
+                                   ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrStaticTransformCreate": [v, ctypes.POINTER(ctypes.c_float * 16), ctypes.POINTER(v)],
+        "vlrTriangleMeshSurfaceNodeCreate": [v, ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrTriangleMeshSurfaceNodeSetVertices": [v, v, ctypes.c_uint32],
+        "vlrTriangleMeshSurfaceNodeAddMaterialGroup": [v, v, ctypes.c_uint32, v, VLRShaderNodePlug,
+                                                       VLRShaderNodePlug, VLRShaderNodePlug],
+        "vlrInternalNodeCreate": [v, ctypes.c_char_p, v, ctypes.POINTER(v)],
+        "vlrParentNodeAddChild": [v, v],
+        "vlrSceneCreate": [v, v, ctypes.POINTER(v)],
+        "vlrSceneSetEnvironment": [v, v],
+        "vlrSceneSetEnvironmentRotation": [v, ctypes.c_float],
+        "vlrCameraCreate": [v, ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrbContextRenderSamples": [v, v, v, ctypes.c_bool, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.POINTER(ctypes.c_uint32)],
+        "vlrbContextSetRenderOptions": [v, ctypes.POINTER(VLRBRenderOptions)],
+        "vlrbContextGetRenderOptions": [v, ctypes.POINTER(VLRBRenderOptions)],
+        "vlrbContextGetStats": [v, ctypes.POINTER(VLRBRenderStats)],
+        "vlrbContextReadFilm": [v, v],
+        "vlrbContextGetOutputDevicePointer": [v, ctypes.POINTER(v)],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    L._vlr_sigs = True
+    return L
+
+
+NULL_PLUG = VLRShaderNodePlug(0, 0)
+
+
+class Queryable:
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+
+    def set(self, name, value):
+        L = _api()
+        n = name.encode()
+        if isinstance(value, Spectrum):
+            check(L.vlrQueryableSetImmediateSpectrum(self.h, n, ctypes.byref(value.c())), f"set {name}")
+        elif isinstance(value, Plug):
+            check(L.vlrQueryableSetShaderNodePlug(self.h, n, value.plug), f"set {name}")
+        elif isinstance(value, Image):
+            check(L.vlrQueryableSetImage2D(self.h, n, value.h), f"set {name}")
+        elif isinstance(value, (int, float)):
+            check(L.vlrQueryableSetFloat(self.h, n, float(value)), f"set {name}")
+        else:
+            raise TypeError(value)
+
+    def set_point(self, name, p):
+        check(_api().vlrQueryableSetPoint3D(self.h, name.encode(), ctypes.byref((ctypes.c_float * 3)(*p))), name)
+
+    def set_quaternion(self, name, q):
+        check(_api().vlrQueryableSetQuaternion(self.h, name.encode(), ctypes.byref((ctypes.c_float * 4)(*q))), name)
+
+    def get_float(self, name):
+        v = ctypes.c_float()
+        check(_api().vlrQueryableGetFloat(self.h, name.encode(), ctypes.byref(v)), name)
+        return v.value
+
+
+class Spectrum:
+    def __init__(self, color_space, e0, e1, e2):
+        self.cs = color_space.encode()
+        self.e = (e0, e1, e2)
+
+    def c(self):
+        return VLRImmediateSpectrum(self.cs, *self.e)
+
+
+def rgb(r, g, b):
+    return Spectrum("Rec709(D65)", r, g, b)
+
+
+class Plug:
+    def __init__(self, plug):
+        self.plug = plug
+
+
+class Image:
+    def __init__(self, handle, keep):
+        self.h = handle
+        self._keep = keep
+
+
+class ShaderNode(Queryable):
+    def plug(self, plug_type=PLUG_SPECTRUM, option=0):
+        p = VLRShaderNodePlug()
+        check(_api().vlrShaderNodeGetPlug(self.h, plug_type, option, ctypes.byref(p)), "getPlug")
+        return Plug(p)
+
+
+class TriangleMesh:
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+
+    def set_vertices(self, verts):
+        """verts: float32 array (n, 11): position, normal, tc0Direction, texCoord."""
+        a = np.ascontiguousarray(verts, dtype=np.float32)
+        assert a.ndim == 2 and a.shape[1] == 11
+        self._verts = a
+        check(_api().vlrTriangleMeshSurfaceNodeSetVertices(self.h, a.ctypes.data_as(c_void_p), a.shape[0]),
+              "setVertices")
+
+    def add_material_group(self, indices, material):
+        idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        check(_api().vlrTriangleMeshSurfaceNodeAddMaterialGroup(
+            self.h, idx.ctypes.data_as(c_void_p), idx.size, material.h, NULL_PLUG, NULL_PLUG, NULL_PLUG),
+            "addMaterialGroup")
+
+
+class ParentNode:
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+        self.children = []
+
+    def add_child(self, node):
+        self.children.append(node)
+        check(_api().vlrParentNodeAddChild(self.h, node.h), "addChild")
+
+
+class SceneNode(ParentNode):
+    def set_environment(self, material, rotation=0.0):
+        self.env = material
+        check(_api().vlrSceneSetEnvironment(self.h, material.h), "setEnvironment")
+        check(_api().vlrSceneSetEnvironmentRotation(self.h, rotation), "setEnvironmentRotation")
+
+
+class Context:
+    """vlr::Context (vlrcpp.h:652-835)."""
+
+    def __init__(self, logging=False):
+        import torch  # initialises the CUDA primary context used by the library
+        torch.cuda.init()
+        L = _api()
+        h = c_void_p()
+        check(L.vlrCreateContext(None, logging, 8, ctypes.byref(h)), "vlrCreateContext")
+        self.h = h
+        self._objects = []
+        self.width = self.height = 0
+
+    @classmethod
+    def create(cls, logging=False):
+        return cls(logging)
+
+    def close(self):
+        if self.h:
+            _api().vlrDestroyContext(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _new(self, fn, *args):
+        h = c_void_p()
+        check(getattr(_api(), fn)(self.h, *args, ctypes.byref(h)), fn)
+        return h
+
+    def identity(self):
+        m = (ctypes.c_float * 16)(*[1.0 if i % 5 == 0 else 0.0 for i in range(16)])
+        return self._new("vlrStaticTransformCreate", ctypes.byref(m))
+
+    def transform(self, mat4_colmajor):
+        m = (ctypes.c_float * 16)(*[float(x) for x in mat4_colmajor])
+        return self._new("vlrStaticTransformCreate", ctypes.byref(m))
+
+    def createScene(self):
+        return SceneNode(self, self._new("vlrSceneCreate", self.identity()))
+
+    def createInternalNode(self, name, transform=None):
+        t = transform if transform is not None else self.identity()
+        return ParentNode(self, self._new("vlrInternalNodeCreate", name.encode(), t))
+
+    def createTriangleMeshSurfaceNode(self, name):
+        return TriangleMesh(self, self._new("vlrTriangleMeshSurfaceNodeCreate", name.encode()))
+
+    def createSurfaceMaterial(self, type_name):
+        return Queryable(self, self._new("vlrSurfaceMaterialCreate", type_name.encode()))
+
+    def createShaderNode(self, type_name):
+        return ShaderNode(self, self._new("vlrShaderNodeCreate", type_name.encode()))
+
+    def createLinearImage2D(self, rgba_f32, spectrum_type="Light Source", color_space="Rec709(D65)"):
+        a = np.ascontiguousarray(rgba_f32, dtype=np.float32)
+        h, w = a.shape[:2]
+        handle = self._new("vlrLinearImage2DCreate", a.ctypes.data_as(c_void_p), w, h, b"RGBA32Fx4",
+                           spectrum_type.encode(), color_space.encode())
+        return Image(handle, a)
+
+    def createCamera(self, type_name="Perspective"):
+        return Queryable(self, self._new("vlrCameraCreate", type_name.encode()))
+
+    def bindOutputBuffer(self, width, height):
+        check(_api().vlrContextBindOutputBuffer(self.h, width, height, 0), "bindOutputBuffer")
+        self.width, self.height = width, height
+
+    def setScene(self, scene):
+        self.scene = scene
+        check(_api().vlrContextSetScene(self.h, scene.h), "setScene")
+
+    def setRenderer(self, renderer):
+        check(_api().vlrContextSetRenderer(self.h, renderer), "setRenderer")
+
+    def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None):
+        o = VLRBRenderOptions()
+        check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
+        if max_path_length is not None:
+            o.maxPathLength = max_path_length
+        if max_paths_in_flight is not None:
+            o.maxPathsInFlight = max_paths_in_flight
+        if light_paths_per_frame is not None:
+            o.lightPathsPerFrame = light_paths_per_frame
+        check(_api().vlrbContextSetRenderOptions(self.h, ctypes.byref(o)), "setOptions")
+
+    def render(self, camera, first_frame, limit=1 << 30, stream=0):
+        """One sample per pixel, exactly like vlrContextRender."""
+        n = ctypes.c_uint32()
+        check(_api().vlrContextRender(self.h, c_void_p(stream), camera.h, False, 1, first_frame, limit,
+                                      ctypes.byref(n)), "vlrContextRender")
+        return n.value
+
+    def render_samples(self, camera, first_frame, samples, limit=1 << 30, stream=0):
+        n = ctypes.c_uint32()
+        check(_api().vlrbContextRenderSamples(self.h, c_void_p(stream), camera.h, first_frame, samples, limit,
+                                              ctypes.byref(n)), "vlrbContextRenderSamples")
+        return n.value
+
+    def read_output(self, out=None):
+        if out is None:
+            out = np.empty((self.height, self.width, 4), np.float32)
+        check(_api().vlrContextReadOutputBuffer(self.h, out.ctypes.data_as(c_void_p)), "readOutputBuffer")
+        return out
+
+    def read_film(self):
+        f = np.empty((self.height, self.width, 16), np.float64)
+        check(_api().vlrbContextReadFilm(self.h, f.ctypes.data_as(c_void_p)), "readFilm")
+        return f
+
+    def output_device_ptr(self):
+        p = c_void_p()
+        check(_api().vlrbContextGetOutputDevicePointer(self.h, ctypes.byref(p)), "outputPtr")
+        return p.value
+
+    def stats(self):
+        s = VLRBRenderStats()
+        check(_api().vlrbContextGetStats(self.h, ctypes.byref(s)), "getStats")
+        return {k: getattr(s, k) for k, _ in VLRBRenderStats._fields_}
+
+
+def quat_rotate_y(angle):
+    return (0.0, math.sin(angle / 2), 0.0, math.cos(angle / 2))
+
+
+__all__ = ["Context", "rgb", "Spectrum", "VLRError", "quat_rotate_y", "RENDERER_PATH_TRACING", "RENDERER_BPT"]
