@@ -226,12 +226,15 @@ __global__ void refitKernel(const float* verts, const uint32_t* sortedPrims, int
     int leaf = blockIdx.x * blockDim.x + threadIdx.x;
     if (leaf >= n) return;
     int node = parentOfLeaf[leaf];
-    while (node >= 0) {
+    // Parent links start at -1; every index is range-checked so a malformed
+    // hierarchy ends the walk instead of reaching outside the arrays.
+    while (node >= 0 && node < n - 1) {
         __threadfence();
         if (atomicAdd(&arrivals[node], 1u) == 0u) return;
         __threadfence();
         V3 lo[2], hi[2];
         int c[2] = { children[2 * node + 0], children[2 * node + 1] };
+        if (c[0] >= n - 1 || c[1] >= n - 1 || ~c[0] >= n || ~c[1] >= n) return;
         for (int k = 0; k < 2; ++k) {
             if (c[k] < 0) {
                 triBox(verts, sortedPrims[~c[k]], &lo[k], &hi[k]);
@@ -325,6 +328,8 @@ void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, c
     ck(cudaMemcpyAsync(out->sortedPrims, vin, size_t(n) * 4, cudaMemcpyDeviceToDevice, stream), "prims");
     if (n > 1) {
         ck(cudaMemsetAsync(arrivals, 0, size_t(n) * 4, stream), "arrivals");
+        ck(cudaMemsetAsync(parentOfLeaf, 0xFF, size_t(n) * 4, stream), "leaf parents");
+        ck(cudaMemsetAsync(parentOfNode, 0xFF, size_t(n) * 4, stream), "node parents");
         karrasKernel<<<(n - 1 + tb - 1) / tb, tb, 0, stream>>>(out->sortedCodes, static_cast<int>(n),
                                                                 out->children, parentOfNode, parentOfLeaf);
         refitKernel<<<blocks, tb, 0, stream>>>(verts, out->sortedPrims, static_cast<int>(n), out->children,
