@@ -1,0 +1,340 @@
+"""Benchmark: spectral path tracing of the Cornell box workload on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (one "step"): a full 512x512 frame of 256 samples per pixel, 4 hero
+wavelengths, maximum path length 8, MIS next-event estimation, FP64 film, on
+the seeded procedural Cornell box (vlr_b200.scenes.cornell_box_desc).  Metric:
+path segments per second (extension rays traced, camera rays included, each
+with its shading and NEE shadow ray), reported in G segments/s.
+
+  value   device-timed throughput of the render call with the scene, film and
+          path state resident in HBM (CUDA events, max over ranks);
+  e2e     the same metric through the public C API with the step's result
+          read back to host memory every step (vlrbContextRenderSamples +
+          vlrContextReadOutputBuffer into pinned memory);
+  roofline   dominant wavefront stage against the measured HBM bandwidth;
+  cpu_baseline  the CPU restatement of the reference path tracer over the
+          reference's own BSDF/spectral code, all host threads, bounded sample.
+
+With --gpus N > 1 (under torchrun) every rank renders its own 256 spp of the
+same frame (weak scaling) and the FP64 films are summed with one NCCL
+all-reduce per step.  --impl reference times the reference's CPU
+implementation of the path on the host cores instead.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1% RMSE vs FP64 ref, guided vs plain PT on 1 B200; G path segments/s"
+UNIT = "G path segments/s"
+W = H = 512
+SPP_PER_STEP = 256
+MAX_PATH_LENGTH = 8
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[4 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(seconds_target=12.0):
+    """The reference CPU path: CPU restatement of path_tracing.cu over the
+    reference's own BSDF/spectral code (oracle/_ref), all host threads."""
+    from oracle import ref
+    from vlr_b200 import scenes
+    if not ref.available():
+        return None
+    desc = scenes.cornell_box_desc(W, H)
+    flat = scenes.flatten_desc(desc)
+    threads = os.cpu_count() or 1
+    spp = 1
+    t0 = time.time()
+    _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, threads=threads)
+    dt = time.time() - t0
+    spp = max(1, min(64, int(seconds_target / max(dt, 1e-3))))
+    t0 = time.time()
+    _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, threads=threads)
+    dt = time.time() - t0
+    return {"value": seg / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{W}x{H} Cornell box, {spp} spp, max path length {MAX_PATH_LENGTH} "
+                      f"({seg} segments, {dt:.1f} s): CPU restatement of path_tracing.cu over the reference's "
+                      f"own BSDF/spectral code, brute-force intersection"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference host build oracle/_ref is missing"}))
+        return 0
+    from vlr_b200 import scenes
+    desc = scenes.cornell_box_desc(W, H)
+    flat = scenes.flatten_desc(desc)
+    threads = os.cpu_count() or 1
+    spp_step = 2
+    for _ in range(args.warmup):
+        ref.pt_render(flat, desc["camera"], W, H, 1, MAX_PATH_LENGTH, threads=threads)
+    total_seg = 0
+    t0 = time.time()
+    for _ in range(args.steps):
+        _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp_step, MAX_PATH_LENGTH, threads=threads)
+        total_seg += seg
+    dt = time.time() - t0
+    v = total_seg / dt / 1e9
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"Cornell box PT {W}x{H}, {spp_step} spp per step (bounded CPU sample of the "
+                                   f"256 spp frame), max path length {MAX_PATH_LENGTH}, 4 hero wavelengths"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{spp_step} spp of {W}x{H} per step: CPU restatement of path_tracing.cu "
+                                       f"over the reference's own BSDF/spectral code"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# Algorithmic bytes per unit of work of each wavefront stage (SoA path state,
+# counted once per read or write; BVH traffic excluded):
+#   trace: queue index 4 + ray 32 + hit 16 + bucket append 4          = 56 B / ray
+#   shade: bucket index 4 + flags 4 + wavelengths 16 + hit 16 + ray 32
+#          + throughput 16x2 + contribution 16x2 + rng 8x2 + pdf/type 8x2
+#          + triangle gather 3x48 (pos/nrm/tan) + index 16 + next ray 32
+#          + next-queue append 4 + shadow ray 48                      = 412 B / hit
+#   shadow: shadow ray 48 + contribution read-modify-write 32        = 80 B / shadow ray
+STAGE_BYTES = {"trace": 56, "shade": 412, "shadow": 80}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vlr_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from vlr_b200 import vlr as V, scenes
+
+    ctx = V.Context()
+    ctx.bindOutputBuffer(W, H)
+    desc = scenes.cornell_box_desc(W, H)
+    scene, cam, keep = scenes.build(ctx, desc)
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 22)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    film_t = None
+    if world > 1:
+        class _Film:
+            pass
+        # Wrap the library's FP64 film (W*H*16 doubles) for the all-reduce.
+        f = _Film()
+        f.__cuda_array_interface__ = {"shape": (H * W * 16,), "typestr": "<f8", "version": 3,
+                                      "data": (ctx.film_device_ptr(), False)}
+        film_t = torch.as_tensor(f, device="cuda")
+
+    def step():
+        ctx.render_samples(cam, True, SPP_PER_STEP, stream=stream)
+        if film_t is not None:
+            dist.all_reduce(film_t)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    seg0 = ctx.stats()["pathSegments"]
+    ctx.kernel_times(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    seg = ctx.stats()["pathSegments"] - seg0
+    _, launches = ctx.kernel_times()
+    param_bytes = ctx.launch_param_bytes()
+    t = torch.tensor([ms, float(seg)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, seg_total = mx[0].item(), sm[1].item()
+    else:
+        ms_max, seg_total = ms, float(seg)
+    value = seg_total / (ms_max * 1e-3) / 1e9
+
+    # ---- end to end through the C API, result read back to pinned host memory
+    out_host = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    out_np = out_host.numpy()
+    seg1 = ctx.stats()["pathSegments"]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+        ctx.read_output(out_np)
+    t_e2e = time.perf_counter() - t0
+    seg_e2e = ctx.stats()["pathSegments"] - seg1
+    te = torch.tensor([t_e2e, float(seg_e2e)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        mx = te.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = te.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        t_e2e, seg_e2e = mx[0].item(), sm[1].item()
+    e2e = seg_e2e / t_e2e / 1e9
+
+    # ---- per-stage device times (separate profiled pass; events add syncs)
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    q0 = ctx.stats()
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    stages, _ = ctx.kernel_times(reset=True)
+    q1 = ctx.stats()
+    ctx.set_profiling(False)
+    rays = q1["pathSegments"] - q0["pathSegments"]
+    shadow = q1["shadowRays"] - q0["shadowRays"]
+    units = {"trace": rays, "shade": rays, "shadow": shadow}
+    hbm_peak, peak_kind = measured_peaks()
+    dominant = max(("trace", "shade", "shadow"), key=lambda k: stages[k]["ms"])
+    st = stages[dominant]
+    per_launch_ms = st["ms"] / max(st["launches"], 1)
+    bytes_per_launch = STAGE_BYTES[dominant] * units[dominant] / max(st["launches"], 1)
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant + "Kernel", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": peak_kind,
+                "stage_ms_per_step": {k: v["ms"] / 2 for k, v in stages.items()}}
+    prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(prof):
+        try:
+            tr = json.load(open(prof)).get(dominant)
+            if tr:
+                roofline["traffic"] = tr["bytes_per_unit"] * units[dominant] / max(st["launches"], 1)
+        except Exception:
+            pass
+
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                base = cpu_baseline()
+            except Exception as ex:  # reported, never fatal for the GPU line
+                base = {"error": str(ex)}
+        launches_per_step = launches / args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"Cornell box PT {W}x{H}, {SPP_PER_STEP} spp per step, max path length "
+                                   f"{MAX_PATH_LENGTH}, 4 hero wavelengths, MIS NEE, FP64 film",
+                       "scene_triangles": ctx.stats()["numTriangles"],
+                       "l2": "working set > L2: 4M path slots x ~200 B of SoA path state per launch",
+                       "parallelism": f"replica render per GPU + NCCL film all-reduce" if world > 1 else "1 GPU"},
+            "segments_per_step": seg_total / args.steps,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(param_bytes / args.steps),
+                    "d2h_bytes_per_step": W * H * 16},
+            "roofline": roofline,
+            "cpu_baseline": base,
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": launches_per_step,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -109,6 +109,46 @@ VLRResult vlrbContextGetOutputDevicePointer(VLRContext context, void** devicePtr
 VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
                            int32_t* children, float* nodeBoxes, float* buildMs);
 
+/* ------------------------------------------------------------------------
+ * Spectral utilities (host-side, no GPU needed).
+ * ---------------------------------------------------------------------- */
+
+/* Meng-Simon RGB -> spectrum upsampling (the reference's UpsampledSpectrum
+ * constructor, libVLR/shared/spectrum_types.cpp:162-228).
+ * spectrumType: 0 Reflectance, 1 Light Source, 2 IndexOfRefraction, 3 NA.
+ * colorSpace: 0 Rec709(D65) sRGB Gamma, 1 Rec709(D65), 2 XYZ, 3 xyY.
+ * packed receives the 12-byte representation {adjacent indices, s, t, scale}. */
+VLRResult vlrbUpsampleSpectrum(uint32_t spectrumType, uint32_t colorSpace, float e0, float e1, float e2,
+                               uint32_t packed[3]);
+
+/* Evaluate an upsampled spectrum at four wavelengths (nm)
+ * (spectrum_types.cpp:273-322). */
+VLRResult vlrbEvaluateSpectrum(const uint32_t packed[3], const float lambdas[4], float values[4]);
+
+/* The CIE 1931 colour-matching functions integrated over the 16 film strata
+ * (xyz[0..15] = xbar, [16..31] = ybar, [32..47] = zbar) and the Y integral
+ * (spectrum_types.cpp:634-680). */
+VLRResult vlrbCmfStrata(float xyz[48], float* integralCMF);
+
+/* ------------------------------------------------------------------------
+ * Kernel timing.  With profiling on, every wavefront stage is bracketed by
+ * CUDA events on the render stream (adds a host synchronisation per render
+ * call); times accumulate until reset.  Stages: 0 camera, 1 trace
+ * (closest hit + material sort), 2 shade, 3 shadow rays, 4 film.
+ * launchCount counts every kernel this library launched for rendering,
+ * profiling on or off.
+ * ---------------------------------------------------------------------- */
+VLRResult vlrbContextSetProfiling(VLRContext context, bool enabled);
+VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[5], uint64_t stageLaunches[5],
+                                    uint64_t* launchCount);
+VLRResult vlrbContextResetKernelTimes(VLRContext context);
+/* Bytes of kernel parameters passed host-to-device with the counted launches
+ * (the per-launch inputs: scene, path-buffer and frame descriptors). */
+VLRResult vlrbContextGetLaunchParamBytes(VLRContext context, uint64_t* bytes);
+
+/* Device address of the FP64 film (width * height * 16 doubles). */
+VLRResult vlrbContextGetFilmDevicePointer(VLRContext context, void** devicePtr);
+
 #if defined(__cplusplus)
 }
 #endif

@@ -52,7 +52,7 @@ FLAGS=(-std=c++20 -O2 -fPIC -fopenmp -DVLR_USE_SPECTRAL_RENDERING -mlzcnt -mpopc
 
 "$CXX" "${FLAGS[@]}" -c "$MIR/shared/spectrum_base.cpp" -o "$OUT/obj/spectrum_base.o"
 "$CXX" "${FLAGS[@]}" -c "$MIR/shared/spectrum_types.cpp" -o "$OUT/obj/spectrum_types.o"
-"$CXX" "${FLAGS[@]}" -x c++ -c "$HERE/ref_shim.cpp" -o "$OUT/obj/ref_shim.o"
+"$CXX" "${FLAGS[@]}" -I "$HERE" -x c++ -c "$HERE/ref_shim.cpp" -o "$OUT/obj/ref_shim.o"
 "$CXX" -shared -fopenmp -o "$OUT/libvlrref.so" \
     "$OUT/obj/ref_shim.o" "$OUT/obj/spectrum_base.o" "$OUT/obj/spectrum_types.o"
 echo "built $OUT/libvlrref.so"

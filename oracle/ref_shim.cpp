@@ -219,3 +219,5 @@ void vlrref_tables(const void** grid, const void** points, const float** cmf16, 
 }
 
 }
+
+#include "ref_pt.inc"

@@ -628,7 +628,7 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 bptRenderLaunch(sg, pb, lightPb, bb, fl, fp, lightPaths * k, wls, wlPdf, numSMs, stream);
             }
             else {
-                ptRenderLaunch(sg, pb, fl, fp, numSMs, stream);
+                ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer);
             }
             done += k;
         }
@@ -636,6 +636,8 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
         stats.frames += samples;
     }
     filmToRGBA(fl, numAccumFrames, output.as<float4>(), stream);
+    ++timer.totalLaunches;
+    timer.paramBytes += sizeof(Film) + 4 + 40 + sizeof(void*);
     if (numAccumFramesOut) *numAccumFramesOut = numAccumFrames;
 }
 

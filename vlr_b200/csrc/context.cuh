@@ -59,6 +59,7 @@ public:
     void readStats(RenderStats* out);
     CUarray outputArray();
     void* outputDevicePtr() const { return output.ptr; }
+    void* filmDevicePtr() const { return film.ptr; }
     uint32_t numTriangles() const { return sg.numTris; }
 
     CUcontext cuContext;
@@ -69,6 +70,7 @@ public:
     VLRRenderer renderer = VLRRenderer_PathTracing;
     RenderOptions options;
     RenderStats stats;
+    StageTimer timer;
     uint32_t numAccumFrames = 0;
     uint64_t generation = 1, builtGeneration = 0;
 

@@ -395,6 +395,10 @@ VLRB_HD UpSpec mengUpsample(const MengTables &T, const ColorMatrices &M,
 // evaluate (spectrum_types.cpp:273-322).
 VLRB_HD S4 mengEvaluate(const MengTables &T, const UpSpec &sp, const WLS &wls) {
     uint32_t a[4] = { sp.adj & 0xFF, (sp.adj >> 8) & 0xFF, (sp.adj >> 16) & 0xFF, (sp.adj >> 24) & 0xFF };
+    // No containing cell or triangle was found (chromaticity outside the
+    // tabulated gamut): the reference leaves the spectrum undefined; here it
+    // evaluates to zero instead of indexing past the table.
+    if (a[0] == 0xFF) return S4(0.0f);
     float sf = static_cast<float>(sp.s) / (65535 - 1);
     float tf = static_cast<float>(sp.t) / (65535 - 1);
     int n;

@@ -450,23 +450,67 @@ void seedPathRngs(uint64_t* states, uint32_t n, uint64_t seed) {
     for (uint32_t i = 0; i < n; ++i) states[i] = gen();
 }
 
+void StageTimer::begin(uint32_t stage, cudaStream_t s, size_t params) {
+    ++totalLaunches;
+    paramBytes += params;
+    if (!enabled) return;
+    if (used == 0)
+        for (auto &e : ev) if (!e) cudaEventCreate(&e);
+    stageOf[used] = stage;
+    cudaEventRecord(ev[2 * used], s);
+}
+
+void StageTimer::end(cudaStream_t s) {
+    if (!enabled) return;
+    cudaEventRecord(ev[2 * used + 1], s);
+    ++used;
+}
+
+void StageTimer::collect() {
+    if (!enabled) return;
+    for (uint32_t i = 0; i < used; ++i) {
+        float t = 0.0f;
+        cudaEventSynchronize(ev[2 * i + 1]);
+        cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+        ms[stageOf[i]] += t;
+        launches[stageOf[i]] += 1;
+    }
+    used = 0;
+}
+
 void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fpIn,
-                    int numSMs, cudaStream_t stream) {
+                    int numSMs, cudaStream_t stream, StageTimer* timer) {
     FrameParams fp = fpIn;
     if (fp.maxPathLength == 0 || fp.maxPathLength > kMaxBounces)
         throw std::runtime_error("maxPathLength out of range");
+    StageTimer dummy;
+    StageTimer &T = timer ? *timer : dummy;
     ck(cudaMemsetAsync(pb.counters, 0, size_t(kMaxBounces + 1) * kCountersPerBounce * 4, stream), "counters");
     const int grid = numSMs * 8;
+    const size_t pMain = sizeof(SceneGPU) + sizeof(PathBuffers) + sizeof(FrameParams);
+    T.begin(kStageCamera, stream, pMain);
     cameraKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+    T.end(stream);
     for (uint32_t b = 0; b < fp.maxPathLength; ++b) {
         fp.bounce = b;
+        T.begin(kStageTrace, stream, pMain);
         traceKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        T.end(stream);
+        T.begin(kStageShade, stream, pMain);
         shadeKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        T.end(stream);
+        T.begin(kStageShadow, stream, pMain);
         shadowKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        T.end(stream);
     }
+    T.begin(kStageFilm, stream, sizeof(PathBuffers) + sizeof(Film) + sizeof(FrameParams));
     filmKernel<<<grid, 256, 0, stream>>>(pb, film, fp);
+    T.end(stream);
+    T.begin(kStageFilm, stream, sizeof(PathBuffers) + 4);
     statsKernel<<<1, 32, 0, stream>>>(pb, fp.maxPathLength);
+    T.end(stream);
     ck(cudaGetLastError(), "launch");
+    T.collect();
 }
 
 void filmClear(const Film &film, cudaStream_t stream) {

@@ -72,8 +72,24 @@ struct PTStats {
 // Render one launch of sppPerLaunch samples per pixel and accumulate the film.
 // counterHost (pinned, optional) receives the per-bounce counters after the
 // launch for statistics.
+// Optional per-stage timing with CUDA events on the launching stream.
+enum PtStage : uint32_t { kStageCamera = 0, kStageTrace, kStageShade, kStageShadow, kStageFilm, kNumPtStages };
+struct StageTimer {
+    bool enabled = false;
+    cudaEvent_t ev[2 * (3 * kMaxBounces + 4)];
+    uint32_t stageOf[3 * kMaxBounces + 4];
+    uint32_t used = 0;
+    double ms[kNumPtStages] = {};
+    uint64_t launches[kNumPtStages] = {};
+    uint64_t totalLaunches = 0;
+    uint64_t paramBytes = 0;   // kernel parameter bytes sent with the launches
+    void begin(uint32_t stage, cudaStream_t s, size_t params = 0);
+    void end(cudaStream_t s);
+    void collect();   // synchronises on the recorded events and accumulates
+};
+
 void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fp,
-                    int numSMs, cudaStream_t stream);
+                    int numSMs, cudaStream_t stream, StageTimer* timer = nullptr);
 
 // Convert the FP64 film to RGBA32F: XYZ / frames * (W*H) -> Rec.709 D65
 // (post_process.cu:93-163).

@@ -1204,4 +1204,41 @@ VLRResult vlrbContextGetOutputDevicePointer(VLRContext context, void** devicePtr
     return VLRResult_NoError;
 }
 
+VLRResult vlrbContextSetProfiling(VLRContext context, bool enabled) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    c->timer.enabled = enabled;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[5], uint64_t stageLaunches[5],
+                                    uint64_t* launchCount) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!stageMs || !stageLaunches || !launchCount) return VLRResult_InvalidArgument;
+    for (int i = 0; i < 5; ++i) { stageMs[i] = c->timer.ms[i]; stageLaunches[i] = c->timer.launches[i]; }
+    *launchCount = c->timer.totalLaunches;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextResetKernelTimes(VLRContext context) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    for (int i = 0; i < 5; ++i) { c->timer.ms[i] = 0; c->timer.launches[i] = 0; }
+    c->timer.totalLaunches = 0;
+    c->timer.paramBytes = 0;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextGetLaunchParamBytes(VLRContext context, uint64_t* bytes) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!bytes) return VLRResult_InvalidArgument;
+    *bytes = c->timer.paramBytes;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextGetFilmDevicePointer(VLRContext context, void** devicePtr) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!devicePtr || c->width == 0) return VLRResult_InvalidArgument;
+    *devicePtr = c->filmDevicePtr();
+    return VLRResult_NoError;
+}
+
 } // extern "C"

@@ -73,9 +73,35 @@ def uv_sphere(center, radius, n_lat, n_lon):
     return np.array(verts, np.float32), np.array(idx, np.uint32)
 
 
-def cornell_box(ctx, width=512, height=512, glass="box", light_scale=1.0, emittance=15.0):
-    scene = ctx.createScene()
-    walls = ctx.createTriangleMeshSurfaceNode("CornellBox")
+MAT_TYPES = {"Matte": 0, "SpecularReflection": 1, "MicrofacetReflection": 2, "MicrofacetScattering": 3,
+             "LambertianScattering": 4, "UE4": 5, "SpecularScattering": 6, "DiffuseEmitter": 7}
+COLOR_SPACES = {"Rec709(D65) sRGB Gamma": 0, "Rec709(D65)": 1, "XYZ": 2, "xyY": 3}
+# spectrum parameter of each slot, per material type
+SPEC_SLOTS = {"Matte": ("albedo",), "SpecularReflection": ("coeff", "eta", "k"),
+              "MicrofacetReflection": (None, "eta", "k"), "MicrofacetScattering": ("coeff", "eta ext", "eta int"),
+              "LambertianScattering": ("coeff",), "UE4": ("base color",),
+              "SpecularScattering": ("coeff", "eta ext", "eta int"), "DiffuseEmitter": ("emittance",)}
+FLOAT_SLOTS = {"MicrofacetReflection": ("roughness", "anisotropy", "rotation"),
+               "MicrofacetScattering": ("roughness", "anisotropy", "rotation"),
+               "LambertianScattering": ("f0",), "UE4": ("roughness", "metallic")}
+FLOAT_DEFAULTS = {"roughness": 0.1, "anisotropy": 0.0, "rotation": 0.0, "f0": 0.04, "metallic": 0.0}
+
+
+def cornell_box_desc(width=512, height=512, glass="box", light_scale=1.0, emittance=15.0):
+    """Plain description of the Cornell box workload (see module doc)."""
+    srgb = "Rec709(D65) sRGB Gamma"
+    lin = "Rec709(D65)"
+    mats = {
+        "white": ("Matte", {"albedo": (srgb, 0.75, 0.75, 0.75)}),
+        "red": ("Matte", {"albedo": (srgb, 0.75, 0.25, 0.25)}),
+        "green": ("Matte", {"albedo": (srgb, 0.25, 0.75, 0.25)}),
+        "light": ("DiffuseEmitter", {"emittance": (lin, emittance, emittance, emittance)}),
+        "metal": ("MicrofacetReflection", {"eta": (lin, 0.2, 0.4, 1.4), "k": (lin, 3.9, 2.4, 1.8),
+                                           "roughness": 0.3, "anisotropy": 0.8}),
+        "glass": ("MicrofacetScattering", {"coeff": (lin, 1.0, 1.0, 1.0), "eta ext": (lin, 1.0, 1.0, 1.0),
+                                          "eta int": (lin, 1.5, 1.5, 1.5),
+                                          "roughness": 0.02 if glass == "sphere" else 0.01}),
+    }
     v = []
     v += _quad((-1.5, 0, -1.5), (-1.5, 0, 1.5), (1.5, 0, 1.5), (1.5, 0, -1.5), (0, 1, 0), (1, 0, 0))      # floor
     v += _quad((-1.5, 0, -1.5), (1.5, 0, -1.5), (1.5, 3, -1.5), (-1.5, 3, -1.5), (0, 0, 1), (1, 0, 0))    # back
@@ -84,54 +110,99 @@ def cornell_box(ctx, width=512, height=512, glass="box", light_scale=1.0, emitta
     v += _quad((1.5, 0, -1.5), (1.5, 0, 1.5), (1.5, 3, 1.5), (1.5, 3, -1.5), (-1, 0, 0), (0, 0, 1))       # right
     hl = 0.5 * math.sqrt(light_scale)
     v += _quad((-hl, 2.9, -hl), (hl, 2.9, -hl), (hl, 2.9, hl), (-hl, 2.9, hl), (0, -1, 0), (1, 0, 0))     # light
-    walls.set_vertices(np.array(v, np.float32))
-    white = ctx.createSurfaceMaterial("Matte")
-    white.set("albedo", V.Spectrum("Rec709(D65) sRGB Gamma", 0.75, 0.75, 0.75))
-    red = ctx.createSurfaceMaterial("Matte")
-    red.set("albedo", V.Spectrum("Rec709(D65) sRGB Gamma", 0.75, 0.25, 0.25))
-    green = ctx.createSurfaceMaterial("Matte")
-    green.set("albedo", V.Spectrum("Rec709(D65) sRGB Gamma", 0.25, 0.75, 0.25))
-    light = ctx.createSurfaceMaterial("DiffuseEmitter")
-    light.set("emittance", V.Spectrum("Rec709(D65)", emittance, emittance, emittance))
-    walls.add_material_group([0, 1, 2, 0, 2, 3, 4, 5, 6, 4, 6, 7, 8, 9, 10, 8, 10, 11], white)
-    walls.add_material_group([12, 13, 14, 12, 14, 15], red)
-    walls.add_material_group([16, 17, 18, 16, 18, 19], green)
-    walls.add_material_group([20, 21, 22, 20, 22, 23], light)
-    scene.add_child(walls)
-
-    metal = ctx.createSurfaceMaterial("MicrofacetReflection")
-    metal.set("eta", V.Spectrum("Rec709(D65)", 0.2, 0.4, 1.4))
-    metal.set("k", V.Spectrum("Rec709(D65)", 3.9, 2.4, 1.8))
-    metal.set("roughness", 0.3)
-    metal.set("anisotropy", 0.8)
-    box_v, box_i = _box((-0.6, 0.0, -0.5), 0.6, math.radians(20))
-    mbox = ctx.createTriangleMeshSurfaceNode("MetalBox")
-    mbox.set_vertices(box_v)
-    mbox.add_material_group(box_i, metal)
-    scene.add_child(mbox)
-
-    glass_mat = ctx.createSurfaceMaterial("MicrofacetScattering")
-    glass_mat.set("coeff", V.Spectrum("Rec709(D65)", 1.0, 1.0, 1.0))
-    glass_mat.set("eta ext", V.Spectrum("Rec709(D65)", 1.0, 1.0, 1.0))
-    glass_mat.set("eta int", V.Spectrum("Rec709(D65)", 1.5, 1.5, 1.5))
-    gnode = ctx.createTriangleMeshSurfaceNode("Glass")
+    meshes = [{"name": "CornellBox", "verts": np.array(v, np.float32), "groups": [
+        (np.array([0, 1, 2, 0, 2, 3, 4, 5, 6, 4, 6, 7, 8, 9, 10, 8, 10, 11], np.uint32), "white"),
+        (np.array([12, 13, 14, 12, 14, 15], np.uint32), "red"),
+        (np.array([16, 17, 18, 16, 18, 19], np.uint32), "green"),
+        (np.array([20, 21, 22, 20, 22, 23], np.uint32), "light")]}]
+    bv, bi = _box((-0.6, 0.0, -0.5), 0.6, math.radians(20))
+    meshes.append({"name": "MetalBox", "verts": bv, "groups": [(bi, "metal")]})
     if glass == "sphere":
-        glass_mat.set("roughness", 0.02)
         gv, gi = uv_sphere((0.5, 0.55, 0.4), 0.55, 71, 142)   # 20,022 triangles
     else:
-        glass_mat.set("roughness", 0.01)
         gv, gi = _box((0.6, 0.0, 0.5), 0.3, math.radians(-15))
-    gnode.set_vertices(gv)
-    gnode.add_material_group(gi, glass_mat)
-    scene.add_child(gnode)
+    meshes.append({"name": "Glass", "verts": gv, "groups": [(gi, "glass")]})
+    camera = {"position": (0.0, 1.5, 6.0), "orientation": V.quat_rotate_y(math.pi), "aspect": width / height,
+              "sensitivity": 1.0, "fovy": 40 * math.pi / 180, "lens radius": 0.0, "op distance": 1.0}
+    return {"materials": mats, "meshes": meshes, "camera": camera, "width": width, "height": height}
 
+
+def build(ctx, desc):
+    """Create the described scene through the C API. Returns (scene, camera, keepalive)."""
+    scene = ctx.createScene()
+    keep = []
+    mats = {}
+    for name, (typ, params) in desc["materials"].items():
+        m = ctx.createSurfaceMaterial(typ)
+        for k, val in params.items():
+            m.set(k, V.Spectrum(*val) if isinstance(val, tuple) else float(val))
+        mats[name] = m
+        keep.append(m)
+    for mesh in desc["meshes"]:
+        node = ctx.createTriangleMeshSurfaceNode(mesh["name"])
+        node.set_vertices(mesh["verts"])
+        for idx, mname in mesh["groups"]:
+            node.add_material_group(idx, mats[mname])
+        scene.add_child(node)
+        keep.append(node)
+    c = desc["camera"]
     cam = ctx.createCamera("Perspective")
-    cam.set_point("position", (0.0, 1.5, 6.0))
-    cam.set_quaternion("orientation", V.quat_rotate_y(math.pi))
-    cam.set("aspect", width / height)
-    cam.set("sensitivity", 1.0)
-    cam.set("fovy", 40 * math.pi / 180)
-    cam.set("lens radius", 0.0)
-    cam.set("op distance", 1.0)
-    keep = [walls, mbox, gnode, white, red, green, light, metal, glass_mat]
+    cam.set_point("position", c["position"])
+    cam.set_quaternion("orientation", c["orientation"])
+    for k in ("aspect", "sensitivity", "fovy", "lens radius", "op distance"):
+        cam.set(k, c[k])
     return scene, cam, keep
+
+
+def cornell_box(ctx, width=512, height=512, glass="box", light_scale=1.0, emittance=15.0):
+    return build(ctx, cornell_box_desc(width, height, glass, light_scale, emittance))
+
+
+MAT_DTYPE = np.dtype([("type", "<i4"), ("colorSpace", "<i4", 3), ("spectra", "<f4", (3, 3)),
+                      ("params", "<f4", 4), ("emitScale", "<f4")])
+
+
+def flatten_desc(desc):
+    """World-space arrays of a description with identity transforms, in the
+    layout of the oracle's path tracer: positions, normals, tangents,
+    triangles (i0, i1, i2, group), group material, group light instance
+    (each emitting mesh is one light instance), material records."""
+    names = list(desc["materials"].keys())
+    recs = np.zeros(len(names), MAT_DTYPE)
+    for i, name in enumerate(names):
+        typ, params = desc["materials"][name]
+        recs[i]["type"] = MAT_TYPES[typ]
+        recs[i]["emitScale"] = float(params.get("scale", 1.0))
+        for k, slot in enumerate(SPEC_SLOTS[typ]):
+            if slot is None:
+                recs[i]["colorSpace"][k] = 1
+                continue
+            cs, e0, e1, e2 = params[slot]
+            recs[i]["colorSpace"][k] = COLOR_SPACES[cs]
+            recs[i]["spectra"][k] = (e0, e1, e2)
+        for k, slot in enumerate(FLOAT_SLOTS.get(typ, ())):
+            recs[i]["params"][k] = float(params.get(slot, FLOAT_DEFAULTS[slot]))
+    pos, nrm, tan, tris, gmat, glight = [], [], [], [], [], []
+    base = 0
+    n_light_inst = 0
+    for mesh in desc["meshes"]:
+        vv = mesh["verts"]
+        pos.append(vv[:, 0:3]); nrm.append(vv[:, 3:6]); tan.append(vv[:, 6:9])
+        emitting = False
+        for idx, mname in mesh["groups"]:
+            g = len(gmat)
+            gmat.append(names.index(mname))
+            is_emit = desc["materials"][mname][0] == "DiffuseEmitter"
+            glight.append(n_light_inst if is_emit else -1)
+            emitting = emitting or is_emit
+            t = idx.reshape(-1, 3).astype(np.uint32) + base
+            tris.append(np.concatenate([t, np.full((len(t), 1), g, np.uint32)], axis=1))
+        if emitting:
+            n_light_inst += 1
+        base += len(vv)
+    return {"pos": np.ascontiguousarray(np.concatenate(pos), np.float32),
+            "nrm": np.ascontiguousarray(np.concatenate(nrm), np.float32),
+            "tan": np.ascontiguousarray(np.concatenate(tan), np.float32),
+            "tris": np.ascontiguousarray(np.concatenate(tris), np.uint32),
+            "groupMaterial": np.array(gmat, np.int32), "groupLightInst": np.array(glight, np.int32),
+            "mats": recs}

@@ -91,6 +91,12 @@ def _api():
         "vlrbContextGetStats": [v, ctypes.POINTER(VLRBRenderStats)],
         "vlrbContextReadFilm": [v, v],
         "vlrbContextGetOutputDevicePointer": [v, ctypes.POINTER(v)],
+        "vlrbContextSetProfiling": [v, ctypes.c_bool],
+        "vlrbContextGetKernelTimes": [v, ctypes.POINTER(ctypes.c_double * 5), ctypes.POINTER(ctypes.c_uint64 * 5),
+                                      ctypes.POINTER(ctypes.c_uint64)],
+        "vlrbContextResetKernelTimes": [v],
+        "vlrbContextGetLaunchParamBytes": [v, ctypes.POINTER(ctypes.c_uint64)],
+        "vlrbContextGetFilmDevicePointer": [v, ctypes.POINTER(v)],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -319,6 +325,30 @@ class Context:
     def output_device_ptr(self):
         p = c_void_p()
         check(_api().vlrbContextGetOutputDevicePointer(self.h, ctypes.byref(p)), "outputPtr")
+        return p.value
+
+    def set_profiling(self, on):
+        check(_api().vlrbContextSetProfiling(self.h, bool(on)), "setProfiling")
+
+    def kernel_times(self, reset=False):
+        ms = (ctypes.c_double * 5)()
+        ln = (ctypes.c_uint64 * 5)()
+        total = ctypes.c_uint64()
+        check(_api().vlrbContextGetKernelTimes(self.h, ctypes.byref(ms), ctypes.byref(ln), ctypes.byref(total)),
+              "getKernelTimes")
+        if reset:
+            check(_api().vlrbContextResetKernelTimes(self.h), "resetKernelTimes")
+        names = ("camera", "trace", "shade", "shadow", "film")
+        return {n: {"ms": ms[i], "launches": ln[i]} for i, n in enumerate(names)}, total.value
+
+    def launch_param_bytes(self):
+        b = ctypes.c_uint64()
+        check(_api().vlrbContextGetLaunchParamBytes(self.h, ctypes.byref(b)), "launchParamBytes")
+        return b.value
+
+    def film_device_ptr(self):
+        p = c_void_p()
+        check(_api().vlrbContextGetFilmDevicePointer(self.h, ctypes.byref(p)), "filmPtr")
         return p.value
 
     def stats(self):
