@@ -99,9 +99,38 @@ __device__ __forceinline__ Bsdf buildBatchBsdf(const BsdfBatchArgs &a, int64_t i
     return B;
 }
 
-__global__ void __launch_bounds__(256) bsdfBatchKernel(BsdfBatchArgs a) {
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+// Queries arrive in random material order; shading them in that order makes
+// every warp execute all six BSDFs.  Each CTA therefore takes a tile of 256
+// queries, counting-sorts the tile's indices by material in shared memory,
+// and lets thread t shade the t-th query of the sorted tile, so warps run one
+// material each except at the few material boundaries.  Inputs and outputs
+// stay in their original slots.
+constexpr int kBatchTile = 256;
+
+__global__ void __launch_bounds__(kBatchTile) bsdfBatchKernel(BsdfBatchArgs a) {
+    __shared__ uint32_t sCount[8];
+    __shared__ uint32_t sOffset[8];
+    __shared__ uint16_t sOrder[kBatchTile];
+    const int64_t numTiles = (a.n + kBatchTile - 1) / kBatchTile;
+    for (int64_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x) {
+        const int64_t base = tile * kBatchTile;
+        if (threadIdx.x < 8) sCount[threadIdx.x] = 0;
+        __syncthreads();
+        const int64_t mine = base + threadIdx.x;
+        uint32_t key = 7;   // slots past the end of the batch sort last
+        if (mine < a.n) key = min(__ldg(a.mat + mine), 6u);
+        const uint32_t rank = atomicAdd(&sCount[key], 1u);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (int k = 0; k < 8; ++k) { sOffset[k] = run; run += sCount[k]; }
+        }
+        __syncthreads();
+        sOrder[sOffset[key] + rank] = static_cast<uint16_t>(threadIdx.x);
+        __syncthreads();
+        const int64_t i = base + sOrder[threadIdx.x];
+        __syncthreads();
+        if (i >= a.n) continue;
         float wlPdf;
         WLS wls = WLS::equalOffsets(__ldg(a.wl + 2 * i + 0), __ldg(a.wl + 2 * i + 1), &wlPdf);
         Bsdf B = buildBatchBsdf(a, i, wls);

@@ -11,6 +11,7 @@
 #include "context.cuh"
 #include "lbvh_build.h"
 #include "tables.cuh"
+#include "bpt.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -26,14 +27,6 @@ namespace vlrb {
 void buildEnvDistribution(const float* hostLuminance, uint32_t w, uint32_t h, double* rowCdf, double* margCdf,
                           float* rowPdf, float* margPdf, void* scratch, cudaStream_t stream);
 size_t envScratchBytes(uint32_t w, uint32_t h);
-// bpt.cu
-size_t bptBufferBytes(uint32_t numPaths, uint32_t cacheCapacity);
-void carveBptBuffers(void* base, uint32_t numPaths, uint32_t cacheCapacity, PathBuffers* lightPaths,
-                     BptBuffers* bb);
-void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const PathBuffers &lightPaths,
-                     const BptBuffers &bb, const Film &film, const FrameParams &fp, uint32_t numLightPaths,
-                     const WLS &commonWls, float wlPdf, int numSMs, cudaStream_t stream);
-
 namespace api {
 
 namespace {
@@ -601,7 +594,7 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
         ensurePathBuffers(pixels * perLaunch);
         uint32_t done = 0;
         while (done < samples) {
-            const uint32_t k = std::min(perLaunch, samples - done);
+            uint32_t k = std::min(perLaunch, samples - done);
             FrameParams fp{};
             fp.width = width;
             fp.height = height;
@@ -609,23 +602,36 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
             fp.numPaths = pixels * k;
             fp.maxPathLength = options.maxPathLength;
             if (renderer == VLRRenderer_BPT) {
-                const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame : pixels;
-                if (bptCapacityPaths < lightPaths * k) {
-                    bptCapacityPaths = lightPaths * k;
-                    bptCapacityVerts = lightPaths * k;
-                    bptMem.resize(bptBufferBytes(bptCapacityPaths, bptCapacityVerts));
-                    carveBptBuffers(bptMem.ptr, bptCapacityPaths, bptCapacityVerts, &lightPb, &bb);
-                    std::vector<uint64_t> seeds(bptCapacityPaths);
-                    seedPathRngs(seeds.data(), bptCapacityPaths, 459182033132123413ull);
+                // One frame per launch: all paths of a frame share its
+                // wavelength samples.  Light subpaths per frame default to a
+                // quarter of the pixel count and the cache holds one vertex
+                // per pixel (overflow is counted, see vlrbContextGetStats).
+                const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame
+                                                                       : std::max<uint32_t>(1, pixels / 4);
+                const uint32_t capacity = std::max<uint32_t>(pixels, lightPaths);
+                if (bptCapacityPaths < lightPaths || bptCapacityVerts < capacity || bptEyeCapacity < pixels) {
+                    bptCapacityPaths = lightPaths;
+                    bptCapacityVerts = capacity;
+                    bptEyeCapacity = pixels;
+                    bptMem.resize(bptBufferBytes(lightPaths, pixels, capacity));
+                    carveBptBuffers(bptMem.ptr, lightPaths, pixels, capacity, &lightPb, &bb);
+                    std::vector<uint64_t> seeds(lightPaths);
+                    // The reference seeds its light-path RNGs from this generator (context.cpp:618-626).
+                    seedPathRngs(seeds.data(), lightPaths, 459182033132123413ull);
                     ck(cudaMemcpy(lightPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
                     ck(cudaMemset(lightPb.totals, 0, 16), "totals");
                 }
-                // One common wavelength set per launch from a host generator
+                // One common wavelength set per frame from a host generator
                 // (context.cpp:1462-1470).
                 std::uniform_real_distribution<float> u01(0.0f, 1.0f);
                 float wlPdf;
-                WLS wls = WLS::equalOffsets(u01(bptRng), u01(bptRng), &wlPdf);
-                bptRenderLaunch(sg, pb, lightPb, bb, fl, fp, lightPaths * k, wls, wlPdf, numSMs, stream);
+                float o = u01(bptRng), sel = u01(bptRng);
+                WLS wls = WLS::equalOffsets(o, sel, &wlPdf);
+                FrameParams bf = fp;
+                bf.sppPerLaunch = 1;
+                bf.numPaths = pixels;
+                bptRenderLaunch(sg, pb, lightPb, bb, fl, bf, lightPaths, wls, wlPdf, numSMs, stream, &timer);
+                k = 1;
             }
             else {
                 ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer);

@@ -87,7 +87,7 @@ private:
     std::mt19937_64 bptRng{ 459182033132123413ull };
     BptBuffers bb{};
     uint32_t pathCapacity = 0;
-    uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0;
+    uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0, bptEyeCapacity = 0;
     CUarray outArray = nullptr;
     uint32_t* hostCounters = nullptr;
     std::vector<float> envPixelsCache;

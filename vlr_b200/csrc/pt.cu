@@ -17,6 +17,7 @@
 // the host and its fixed kernel sequence can be captured in a CUDA graph.
 #include "pt.cuh"
 #include "tables.cuh"
+#include "wavefront.cuh"
 
 #include <random>
 #include <stdexcept>
@@ -25,23 +26,6 @@
 namespace vlrb {
 
 namespace {
-
-__device__ __forceinline__ uint32_t* bounceCounters(const PathBuffers &pb, uint32_t b) {
-    return pb.counters + b * kCountersPerBounce;
-}
-
-// Warp-aggregated append: lanes with the same queue share one atomic.
-__device__ __forceinline__ uint32_t appendSlot(uint32_t* counter, uint32_t key) {
-    const uint32_t active = __activemask();
-    const uint32_t peers = __match_any_sync(active, key);
-    const int leader = __ffs(peers) - 1;
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t base = 0;
-    if (static_cast<int>(lane) == leader)
-        base = atomicAdd(counter, static_cast<uint32_t>(__popc(peers)));
-    base = __shfl_sync(peers, base, leader);
-    return base + __popc(peers & ((1u << lane) - 1u));
-}
 
 __device__ __forceinline__ WLS loadWls(const PathBuffers &pb, uint32_t p) {
     float4 l = pb.lambda[p];
@@ -52,9 +36,6 @@ __device__ __forceinline__ WLS loadWls(const PathBuffers &pb, uint32_t p) {
     w.single = (f >> 4) & 1u;
     return w;
 }
-
-__device__ __forceinline__ S4 toS4(const float4 &v) { S4 s; s[0] = v.x; s[1] = v.y; s[2] = v.z; s[3] = v.w; return s; }
-__device__ __forceinline__ float4 toF4(const S4 &s) { return make_float4(s[0], s[1], s[2], s[3]); }
 
 __global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
     const uint32_t P = fp.numPaths;
@@ -511,6 +492,11 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
     T.end(stream);
     ck(cudaGetLastError(), "launch");
     T.collect();
+}
+
+void launchTraceSorted(const SceneGPU &scene, const PathBuffers &pb, const FrameParams &fp, int grid,
+                       cudaStream_t stream) {
+    traceKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
 }
 
 void filmClear(const Film &film, cudaStream_t stream) {

@@ -93,6 +93,11 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
 
 // Convert the FP64 film to RGBA32F: XYZ / frames * (W*H) -> Rec.709 D65
 // (post_process.cu:93-163).
+// Closest-hit trace of bounce fp.bounce's active queue with material-sorted
+// output queues (used by both integrators).
+void launchTraceSorted(const SceneGPU &scene, const PathBuffers &pb, const FrameParams &fp, int grid,
+                       cudaStream_t stream);
+
 void filmToRGBA(const Film &film, uint32_t numAccumFrames, float4* out, cudaStream_t stream);
 void filmClear(const Film &film, cudaStream_t stream);
 

@@ -206,3 +206,219 @@ def flatten_desc(desc):
             "tris": np.ascontiguousarray(np.concatenate(tris), np.uint32),
             "groupMaterial": np.array(gmat, np.int32), "groupLightInst": np.array(glight, np.int32),
             "mats": recs}
+
+
+def _fbm(n, seed, octaves=7):
+    """(n+1)x(n+1) fractional Brownian motion heights in [-1, 1] from bilinearly
+    interpolated value noise, seeded."""
+    rng = np.random.default_rng(seed)
+    h = np.zeros((n + 1, n + 1), np.float64)
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = 4 * (2 ** o)
+        g = rng.uniform(-1, 1, (cells + 1, cells + 1))
+        x = np.linspace(0, cells, n + 1)
+        i = np.minimum(x.astype(int), cells - 1)
+        t = x - i
+        t = t * t * (3 - 2 * t)
+        a = g[i][:, i] * (1 - t)[None, :] + g[i][:, i + 1] * t[None, :]
+        b = g[i + 1][:, i] * (1 - t)[None, :] + g[i + 1][:, i + 1] * t[None, :]
+        h += amp * (a * (1 - t)[:, None] + b * t[:, None])
+        total += amp
+        amp *= 0.5
+    return h / total
+
+
+def icosphere(level=2):
+    """Unit icosphere: 20 * 4**level triangles (320 at level 2)."""
+    t = (1 + 5 ** 0.5) / 2
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    v = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        cache = {}
+
+        def mid(a, b):
+            k = (min(a, b), max(a, b))
+            if k not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[k] = len(v) - 1
+            return cache[k]
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    P = np.array(v, np.float32)
+    tan = np.cross(np.array([0, 1, 0], np.float32), P)
+    bad = np.linalg.norm(tan, axis=1) < 1e-6
+    tan[bad] = (1, 0, 0)
+    tan /= np.linalg.norm(tan, axis=1, keepdims=True)
+    verts = np.concatenate([P, P, tan, np.zeros((len(P), 2), np.float32)], axis=1).astype(np.float32)
+    return verts, np.array(f, np.uint32).reshape(-1)
+
+
+def sky_image(width=2048, height=1024, sun_dir=(0.35, 0.6, -0.72), sun_radius_deg=0.5, sun_rel=1e4):
+    """Procedural RGB sky on an equirectangular grid (row 0 = zenith): a
+    horizon-to-zenith gradient, dark ground below the horizon, and a sun disc
+    of the given angular diameter whose radiance is sun_rel times the zenith
+    sky's."""
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = np.pi * v[:, None]
+    phi = 2 * np.pi * u[None, :]
+    # direction for (phi, theta) with y up, matching the renderer's mapping
+    d = np.stack([-np.sin(phi) * np.sin(theta), np.cos(theta) * np.ones_like(phi), np.cos(phi) * np.sin(theta)], -1)
+    up = d[..., 1]
+    zen = np.array([0.25, 0.45, 0.95])
+    hor = np.array([0.85, 0.9, 1.0])
+    t = np.clip(up, 0, 1)[..., None]
+    sky = hor * (1 - t) ** 3 + zen * (1 - (1 - t) ** 3)
+    ground = np.array([0.18, 0.16, 0.14])
+    img = np.where(up[..., None] > 0, sky, ground * np.clip(1 + up, 0, 1)[..., None])
+    s = np.array(sun_dir, np.float64)
+    s /= np.linalg.norm(s)
+    cosang = np.clip(d @ s, -1, 1)
+    half = np.radians(sun_radius_deg / 2)
+    sun = cosang >= np.cos(half)
+    img[sun] = zen.max() * sun_rel * np.array([1.0, 0.95, 0.85])
+    rgba = np.concatenate([img, np.ones(img.shape[:2] + (1,))], -1).astype(np.float32)
+    return rgba
+
+
+def terrain_scene_desc(width=1920, height=1080, cells=1024, n_spheres=4096, seed=7, sky=(2048, 1024)):
+    """Description of the LVC-BPT + environment workload (see module doc).
+    Terrain: cells x cells quads = 2 * cells**2 triangles; spheres: instanced
+    320-triangle icospheres with random scale in [0.5, 3] and random material."""
+    rng = np.random.default_rng(seed)
+    size = 1024.0
+    h = _fbm(cells, seed) * 60.0
+    xs = np.linspace(-size / 2, size / 2, cells + 1)
+    X, Z = np.meshgrid(xs, xs)
+    P = np.stack([X, h, Z], -1).astype(np.float32)
+    dx = np.gradient(h, xs, axis=1)
+    dz = np.gradient(h, xs, axis=0)
+    N = np.stack([-dx, np.ones_like(h), -dz], -1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    T = np.stack([np.ones_like(h), dx, np.zeros_like(h)], -1)
+    T /= np.linalg.norm(T, axis=-1, keepdims=True)
+    verts = np.concatenate([P.reshape(-1, 3), N.reshape(-1, 3), T.reshape(-1, 3),
+                            np.zeros(((cells + 1) ** 2, 2))], 1).astype(np.float32)
+    i = np.arange(cells)
+    r, c = np.meshgrid(i, i, indexing="ij")
+    v00 = (r * (cells + 1) + c).reshape(-1)
+    v01, v10, v11 = v00 + 1, v00 + cells + 1, v00 + cells + 2
+    quads = np.stack([v00, v10, v11, v00, v11, v01], 1).astype(np.uint32)
+    # materials: 8 terrain materials assigned per 64x64-cell patch
+    mats = {}
+    for k in range(8):
+        rough = float(rng.uniform(0.2, 0.9))
+        col = tuple(float(x) for x in rng.uniform(0.15, 0.6, 3))
+        if k % 2 == 0:
+            mats[f"terrain{k}"] = ("Matte", {"albedo": ("Rec709(D65)",) + col})
+        else:
+            mats[f"terrain{k}"] = ("UE4", {"base color": ("Rec709(D65)",) + col, "roughness": rough,
+                                           "metallic": float(rng.uniform(0, 0.3))})
+    patch = ((r // 64) * 7 + (c // 64) * 3).reshape(-1) % 8
+    groups = [(quads[patch == k].reshape(-1), f"terrain{k}") for k in range(8)]
+    meshes = [{"name": "Terrain", "verts": verts, "groups": groups}]
+    # sphere materials and instances
+    sv, si = icosphere(2)
+    sphere_mats = []
+    for k in range(8):
+        name = f"sphere{k}"
+        col = tuple(float(x) for x in rng.uniform(0.1, 0.9, 3))
+        kind = k % 4
+        if kind == 0:
+            mats[name] = ("Matte", {"albedo": ("Rec709(D65)",) + col})
+        elif kind == 1:
+            mats[name] = ("UE4", {"base color": ("Rec709(D65)",) + col, "roughness": float(rng.uniform(0.2, 0.9)),
+                                  "metallic": 1.0})
+        elif kind == 2:
+            mats[name] = ("MicrofacetReflection", {"eta": ("Rec709(D65)", 0.2, 0.4, 1.4),
+                                                   "k": ("Rec709(D65)", 3.9, 2.4, 1.8),
+                                                   "roughness": float(rng.uniform(0.2, 0.6))})
+        else:
+            mats[name] = ("LambertianScattering", {"coeff": ("Rec709(D65)",) + col})
+        sphere_mats.append(name)
+    instances = []
+    for s in range(n_spheres):
+        px, pz = rng.uniform(-size / 2 * 0.9, size / 2 * 0.9, 2)
+        ci = int(np.clip((px + size / 2) / size * cells, 0, cells))
+        ri = int(np.clip((pz + size / 2) / size * cells, 0, cells))
+        scale = float(rng.uniform(0.5, 3.0))
+        y = float(h[ri, ci]) + scale * 0.8
+        instances.append({"mesh": sphere_mats[int(rng.integers(0, 8))], "scale": scale, "translate": (px, y, pz)})
+    sphere_meshes = {name: {"name": "Ico_" + name, "verts": sv, "groups": [(si, name)]} for name in sphere_mats}
+    camera = {"position": (0.0, 160.0, 420.0), "orientation": _look_quat((0.0, -0.35, -1.0)),
+              "aspect": width / height, "sensitivity": 1.0, "fovy": 50 * math.pi / 180, "lens radius": 0.0,
+              "op distance": 1.0}
+    return {"materials": mats, "meshes": meshes, "instanced": sphere_meshes, "instances": instances,
+            "camera": camera, "width": width, "height": height,
+            "env": {"image": sky_image(*sky), "scale": 1.0}}
+
+
+def _look_quat(forward):
+    """Quaternion (x, y, z, w) rotating +z onto `forward` with +y kept up."""
+    f = np.array(forward, np.float64)
+    f /= np.linalg.norm(f)
+    r = np.cross(np.array([0.0, 1.0, 0.0]), f)
+    r /= np.linalg.norm(r)
+    u = np.cross(f, r)
+    m = np.stack([r, u, f], 1)   # columns: right, up, forward
+    tr = m[0, 0] + m[1, 1] + m[2, 2]
+    if tr > 0:
+        s = math.sqrt(tr + 1.0) * 2
+        return ((m[2, 1] - m[1, 2]) / s, (m[0, 2] - m[2, 0]) / s, (m[1, 0] - m[0, 1]) / s, 0.25 * s)
+    i = int(np.argmax([m[0, 0], m[1, 1], m[2, 2]]))
+    j, k = (i + 1) % 3, (i + 2) % 3
+    s = math.sqrt(1.0 + m[i, i] - m[j, j] - m[k, k]) * 2
+    q = [0.0, 0.0, 0.0, 0.0]
+    q[i] = 0.25 * s
+    q[j] = (m[j, i] + m[i, j]) / s
+    q[k] = (m[k, i] + m[i, k]) / s
+    q[3] = (m[k, j] - m[j, k]) / s
+    return tuple(q)
+
+
+def build_instanced(ctx, desc):
+    """build() plus instanced meshes under internal nodes and the environment."""
+    scene, cam, keep = build(ctx, desc)
+    mats = {}
+    for name, (typ, params) in desc["materials"].items():
+        if name in desc.get("instanced", {}):
+            pass
+    # material handles created by build(), in order
+    names = list(desc["materials"].keys())
+    mats = dict(zip(names, keep[:len(names)]))
+    meshes = {}
+    for name, mesh in desc.get("instanced", {}).items():
+        node = ctx.createTriangleMeshSurfaceNode(mesh["name"])
+        node.set_vertices(mesh["verts"])
+        for idx, mname in mesh["groups"]:
+            node.add_material_group(idx, mats[mname])
+        meshes[name] = node
+        keep.append(node)
+    for inst in desc.get("instances", []):
+        s = inst["scale"]
+        tx, ty, tz = inst["translate"]
+        m = [s, 0, 0, 0, 0, s, 0, 0, 0, 0, s, 0, tx, ty, tz, 1]
+        node = ctx.createInternalNode("inst", ctx.transform(m))
+        node.add_child(meshes[inst["mesh"]])
+        scene.add_child(node)
+        keep.append(node)
+    env = desc.get("env")
+    if env is not None:
+        img = ctx.createLinearImage2D(env["image"], "Light Source", "Rec709(D65)")
+        tex = ctx.createShaderNode("EnvironmentTexture")
+        tex.set("image", img)
+        em = ctx.createSurfaceMaterial("EnvironmentEmitter")
+        em.set("emittance", tex.plug())
+        em.set("scale", env.get("scale", 1.0))
+        scene.set_environment(em, env.get("rotation", 0.0))
+        keep += [img, tex, em]
+    return scene, cam, keep
