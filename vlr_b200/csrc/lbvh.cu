@@ -32,10 +32,15 @@ __device__ __forceinline__ V3 loadVertex(const float* v, uint32_t tri, int k) {
     return V3(p[0], p[1], p[2]);
 }
 
-// Centroid of a triangle: (v0 + v1 + v2) * (1/3), summed left to right.
+// Centroid of a triangle: (v0 + v1 + v2) * (1/3), summed left to right.  The
+// product is rounded on its own (__fmul_rn): left to the compiler it fuses
+// with the "- lo" of the quantisation into one FMA, which moves centroids that
+// sit on a cell boundary into the neighbouring cell.
 __device__ __forceinline__ V3 centroidOf(const float* verts, uint32_t i) {
     V3 a = loadVertex(verts, i, 0), b = loadVertex(verts, i, 1), c = loadVertex(verts, i, 2);
-    return (a + b + c) * (1.0f / 3.0f);
+    V3 s = a + b + c;
+    const float third = 1.0f / 3.0f;
+    return V3(__fmul_rn(s.x, third), __fmul_rn(s.y, third), __fmul_rn(s.z, third));
 }
 
 __global__ void centroidBoundsKernel(const float* verts, uint32_t n, uint32_t* ordBox /* 6 */) {

@@ -435,6 +435,7 @@ void StageTimer::begin(uint32_t stage, cudaStream_t s, size_t params) {
     ++totalLaunches;
     paramBytes += params;
     if (!enabled) return;
+    if (used == kSlots) collect();   // every slot recorded: drain before reuse
     if (used == 0)
         for (auto &e : ev) if (!e) cudaEventCreate(&e);
     stageOf[used] = stage;
@@ -445,6 +446,10 @@ void StageTimer::end(cudaStream_t s) {
     if (!enabled) return;
     cudaEventRecord(ev[2 * used + 1], s);
     ++used;
+}
+
+StageTimer::~StageTimer() {
+    for (auto &e : ev) if (e) cudaEventDestroy(e);
 }
 
 void StageTimer::collect() {

@@ -76,8 +76,9 @@ struct PTStats {
 enum PtStage : uint32_t { kStageCamera = 0, kStageTrace, kStageShade, kStageShadow, kStageFilm, kNumPtStages };
 struct StageTimer {
     bool enabled = false;
-    cudaEvent_t ev[2 * (3 * kMaxBounces + 4)];
-    uint32_t stageOf[3 * kMaxBounces + 4];
+    static constexpr uint32_t kSlots = 3 * kMaxBounces + 4;
+    cudaEvent_t ev[2 * kSlots] = {};
+    uint32_t stageOf[kSlots] = {};
     uint32_t used = 0;
     double ms[kNumPtStages] = {};
     uint64_t launches[kNumPtStages] = {};
@@ -86,6 +87,10 @@ struct StageTimer {
     void begin(uint32_t stage, cudaStream_t s, size_t params = 0);
     void end(cudaStream_t s);
     void collect();   // synchronises on the recorded events and accumulates
+    StageTimer() = default;
+    StageTimer(const StageTimer &) = delete;
+    StageTimer &operator=(const StageTimer &) = delete;
+    ~StageTimer();
 };
 
 void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fp,
