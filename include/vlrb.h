@@ -110,6 +110,23 @@ VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCo
                            int32_t* children, float* nodeBoxes, float* buildMs);
 
 /* ------------------------------------------------------------------------
+ * The same LBVH build with caller-owned DEVICE buffers that allocates no
+ * device memory (no counterpart in the reference, whose acceleration
+ * structures OptiX builds).  Its scratch is a static device array sized for
+ * VLRB_BVH_NO_ALLOC_MAX_TRIANGLES triangles; a larger n returns
+ * VLRResult_InvalidArgument.  The arrays are those of vlrbBvhBuildHost plus
+ *   nodes[(n-1) x 64 bytes]  traversal nodes,
+ *   tris[n x 48 bytes]       triangles in sorted order.
+ * Work is enqueued on `stream`.  One scratch per device: calls on the same
+ * device must not overlap (serialise them on one stream or synchronise
+ * between them).  The first call on a device does a one-time set-up; make it
+ * before any stream capture.  No scratch byte needs an initial value.
+ * ---------------------------------------------------------------------- */
+#define VLRB_BVH_NO_ALLOC_MAX_TRIANGLES 65536u
+VLRResult vlrbBvhBuildNoAlloc(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
+                              int32_t* children, float* nodeBoxes, void* nodes, void* tris, CUstream stream);
+
+/* ------------------------------------------------------------------------
  * Spectral utilities (host-side, no GPU needed).
  * ---------------------------------------------------------------------- */
 
