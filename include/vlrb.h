@@ -166,6 +166,39 @@ VLRResult vlrbContextGetLaunchParamBytes(VLRContext context, uint64_t* bytes);
 /* Device address of the FP64 film (width * height * 16 doubles). */
 VLRResult vlrbContextGetFilmDevicePointer(VLRContext context, void** devicePtr);
 
+/* ------------------------------------------------------------------------
+ * Learned path-guiding network (no counterpart in the reference, which has
+ * no guiding).  A hash-grid position encoding (16 levels x 2 features,
+ * 2^log2TableSize entries per level) and spherical-harmonic encodings of the
+ * outgoing direction and shading normal feed a 64-64-64-64-48 BF16 MLP on
+ * the tensor cores; its 40 used outputs are 8 von Mises-Fisher lobes, 5 raw
+ * values each: direction (3, normalised), log concentration, mixture logit.
+ *
+ * Parameters: numWeights FP32 weights, layers back to back, each row-major
+ * [out][in] (64x64, 64x64, 64x64, 48x64; output rows 40..47 are padding and
+ * stay zero), and numGridFloats FP32 grid features [level][entry][2].
+ * Positions are normalised to [0,1]^3 by the box given to SetBounds.
+ * Training samples: 16 floats each = position xyz, weight (radiance / pdf),
+ * outgoing direction (xyz, pad), shading normal (xyz, pad), incident
+ * direction (xyz, pad).  The loss is sum_j (w_j / sum w) * -log q(wi_j).
+ * ---------------------------------------------------------------------- */
+typedef struct VLRBGuideNet_API* VLRBGuideNet;
+VLRResult vlrbGuideNetCreate(uint32_t log2TableSize, uint64_t seed, VLRBGuideNet* net);
+VLRResult vlrbGuideNetDestroy(VLRBGuideNet net);
+VLRResult vlrbGuideNetSetBounds(VLRBGuideNet net, const float* lo, const float* hi);
+VLRResult vlrbGuideNetGetSizes(VLRBGuideNet net, uint32_t* numWeights, uint64_t* numGridFloats);
+VLRResult vlrbGuideNetGetParams(VLRBGuideNet net, float* weights, float* grid);
+VLRResult vlrbGuideNetSetParams(VLRBGuideNet net, const float* weights, const float* grid);
+/* raw[n x 40] network outputs for n queries (host arrays of n x 3 floats). */
+VLRResult vlrbGuideNetInferHost(VLRBGuideNet net, uint32_t n, const float* pos, const float* wo,
+                                const float* nrm, float* raw);
+/* Gradients of the batch loss (no parameter update); loss may be NULL. */
+VLRResult vlrbGuideNetGradientsHost(VLRBGuideNet net, uint32_t n, const float* samples, float* weightGrad,
+                                    float* gridGrad, float* loss);
+/* `steps` Adam steps on the same batch; lossPerStep[steps] may be NULL. */
+VLRResult vlrbGuideNetTrainHost(VLRBGuideNet net, uint32_t n, const float* samples, float learningRate,
+                                uint32_t steps, float* lossPerStep);
+
 #if defined(__cplusplus)
 }
 #endif
