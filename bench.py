@@ -161,6 +161,109 @@ def run_reference(args):
     return 0
 
 
+# ---- time to 1% error, guided vs plain path tracing (glossy-caustic scene)
+RMSE_W = RMSE_H = 1024
+RMSE_BLOCK = 8
+RMSE_TARGET = 0.01
+RMSE_REF_SPP = 4096
+RMSE_CHUNK_SPP = 4
+RMSE_CAP_S = 40.0
+
+
+class _FilmView:
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "version": 3, "data": (ptr, False)}
+
+
+def _cmf_y():
+    import ctypes
+    from vlr_b200 import lib
+    L = lib()
+    L.vlrbCmfStrata.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    xyz = np.zeros(48, np.float32)
+    integ = ctypes.c_float()
+    L.vlrbCmfStrata(xyz.ctypes.data_as(ctypes.c_void_p), ctypes.byref(integ))
+    return xyz[16:32].astype(np.float64)
+
+
+def time_to_rmse():
+    """Device time until the image is within RMSE_TARGET of an FP64 plain-PT
+    reference (RMSE_REF_SPP spp, independent RNG seed), for plain and for
+    guided path tracing with online training included in the time.  Error:
+    RMSE of RMSE_BLOCK^2-pixel block means of CIE Y, relative to the
+    reference mean (block means keep the reference's own noise well below
+    the target).  A method that has not reached the target after RMSE_CAP_S
+    seconds reports its error there and an extrapolated time assuming error
+    ~ 1/sqrt(time)."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    W, H, b = RMSE_W, RMSE_H, RMSE_BLOCK
+    cy = torch.tensor(_cmf_y(), device="cuda")
+
+    def make(guided, seed):
+        ctx = V.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = scenes.cornell_box(ctx, W, H, glass="sphere", light_scale=0.1)
+        ctx.setScene(scene)
+        ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 22, rng_seed=seed,
+                       consistent_dielectric_pdf=True)
+        if guided:
+            ctx.setGuiding(enabled=True, train=True)
+        return ctx, cam, keep
+
+    def blocks(ctx):
+        f = torch.as_tensor(_FilmView(ctx.film_device_ptr(), W * H * 16), device="cuda").view(H, W, 16)
+        y = f @ cy
+        return y.view(H // b, b, W // b, b).mean(dim=(1, 3))
+
+    ctx, cam, keep = make(False, 0x9E3779B97F4A7C15)
+    ctx.render_samples(cam, True, RMSE_REF_SPP)
+    ref = blocks(ctx) / RMSE_REF_SPP
+    torch.cuda.synchronize()
+    ctx.close()
+    ref_mean = ref.mean().item()
+    out = {"scene": "Cornell box, 20,022-triangle GGX dielectric sphere (IOR 1.5, roughness 0.02), light 0.1x area",
+           "resolution": [W, H], "max_path_length": MAX_PATH_LENGTH, "target": RMSE_TARGET,
+           "error": f"RMSE of {b}x{b}-pixel block means of CIE Y / reference mean",
+           "reference": f"plain PT, {RMSE_REF_SPP} spp, FP64 film, independent seed",
+           "dielectric_pdf": "consistent (the reference's MicrofacetScattering pdf is 0 for exits: "
+                             "NEE double counting and fireflies)"}
+    for name, guided in (("plain", False), ("guided", True)):
+        ctx, cam, keep = make(guided, 0)
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t = 0.0
+        n = 0
+        curve = []
+        reached = None
+        while t < RMSE_CAP_S:
+            e0.record(stream)
+            ctx.render_samples(cam, n == 0, RMSE_CHUNK_SPP, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            t += e0.elapsed_time(e1) * 1e-3
+            n += RMSE_CHUNK_SPP
+            err = (torch.sqrt(torch.mean((blocks(ctx) / n - ref) ** 2)) / ref_mean).item()
+            if n in (4, 16, 64, 256, 1024, 4096) or err <= RMSE_TARGET:
+                curve.append([n, round(t, 4), err])
+            if err <= RMSE_TARGET:
+                reached = t
+                break
+        r = {"seconds": reached, "spp": n, "error_at_end": err, "seconds_at_end": t, "curve": curve}
+        if reached is None:
+            r["seconds_extrapolated"] = t * (err / RMSE_TARGET) ** 2
+        if guided:
+            r["guiding"] = ctx.guiding_stats()
+        seg = ctx.stats()["pathSegments"]
+        r["segments_per_s"] = seg / t / 1e9
+        out[name] = r
+        ctx.close()
+    tp = out["plain"]["seconds"] or out["plain"]["seconds_extrapolated"]
+    tg = out["guided"]["seconds"] or out["guided"]["seconds_extrapolated"]
+    out["guided_over_plain"] = tg / tp
+    return out
+
+
 # Algorithmic bytes per unit of work of each wavefront stage (SoA path state,
 # counted once per read or write; BVH traffic excluded):
 #   trace: queue index 4 + ray 32 + hit 16 + bucket append 4          = 56 B / ray
@@ -179,6 +282,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vlr_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-1%%-error measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -302,6 +406,13 @@ def main():
         except Exception:
             pass
 
+    rmse = None
+    if rank == 0 and world == 1 and not args.no_rmse:
+        try:
+            rmse = time_to_rmse()
+        except Exception as ex:  # reported, never fatal for the GPU line
+            rmse = {"error": str(ex)}
+
     if rank == 0:
         base = None
         if world == 1 and not args.no_cpu_baseline:
@@ -327,6 +438,7 @@ def main():
             "gpu_launches": int(launches),
             "gpu_launches_per_step": launches_per_step,
             "clocks": clocks.summary(),
+            "time_to_rmse": rmse,
         }
         print(json.dumps(line))
     ctx.close()

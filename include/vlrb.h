@@ -73,6 +73,13 @@ typedef struct VLRBRenderOptions {
     uint32_t maxPathLength;       /* hits after which a path stops scattering (reference: 25) */
     uint32_t maxPathsInFlight;    /* path slots per launch (memory ~ 200 B each) */
     uint32_t lightPathsPerFrame;  /* LVC-BPT light subpaths per frame, 0 = one per pixel */
+    uint64_t rngSeed;             /* seed of the per-path RNG states, 0 = the reference's
+                                     591842031321323413 (context.cpp:1176-1190) */
+    uint32_t consistentDielectricPdf;  /* 0: MicrofacetScattering pdf exactly as the reference,
+                                     which is 0 for every transmission out of the medium
+                                     (materials.cu:1448-1513), so MIS double-counts NEE
+                                     through exits; 1: pdf consistent with the sampled
+                                     density and the value (unbiased MIS) */
 } VLRBRenderOptions;
 
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options);
@@ -87,6 +94,37 @@ typedef struct VLRBRenderStats {
 } VLRBRenderStats;
 
 VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);
+
+/* Learned path guiding of the path tracer (no counterpart in the reference).
+ * With `train`, every launch records training samples at the Matte,
+ * LambertianScattering and UE4 vertices of its first `recordBounces` bounces
+ * and is followed by `stepsPerLaunch` Adam steps on about `samplesPerStep` of
+ * them.  With `enabled`, those vertices sample the next direction from the
+ * network's vMF mixture or the BSDF with probability 1/2 each and weight by
+ * the combined density (one-sample MIS: unbiased whatever the network
+ * learned); when training too, guided sampling starts after `warmupLaunches`
+ * launches.  The network is created on first use and kept across frames. */
+typedef struct VLRBGuidingOptions {
+    bool enabled;
+    bool train;
+    uint32_t log2TableSize;       /* hash-grid entries per level = 2^log2TableSize (8..24, default 19) */
+    float learningRate;           /* default 1e-2 */
+    uint32_t samplesPerStep;      /* default 2^18 */
+    uint32_t stepsPerLaunch;      /* default 1 */
+    uint32_t recordBounces;       /* 1..8, default 4 */
+    uint32_t warmupLaunches;      /* default 4 */
+} VLRBGuidingOptions;
+
+typedef struct VLRBGuidingStats {
+    float lastLoss;               /* batch loss of the latest training step */
+    uint64_t trainingSteps;
+    uint64_t guidedLaunches;
+    uint32_t lastSamples;         /* training samples the latest launch recorded */
+} VLRBGuidingStats;
+
+VLRResult vlrbContextSetGuiding(VLRContext context, const VLRBGuidingOptions* options);
+VLRResult vlrbContextGetGuiding(VLRContext context, VLRBGuidingOptions* options);
+VLRResult vlrbContextGetGuidingStats(VLRContext context, VLRBGuidingStats* stats);
 
 /* Copies the FP64 spectral film (width * height * 16 doubles, strata of
  * 29.375 nm over 360-830 nm, sum over accumulated samples) to host memory. */
@@ -151,12 +189,13 @@ VLRResult vlrbCmfStrata(float xyz[48], float* integralCMF);
  * Kernel timing.  With profiling on, every wavefront stage is bracketed by
  * CUDA events on the render stream (adds a host synchronisation per render
  * call); times accumulate until reset.  Stages: 0 camera, 1 trace
- * (closest hit + material sort), 2 shade, 3 shadow rays, 4 film.
+ * (closest hit + material sort), 2 shade, 3 shadow rays, 4 film, 5 guiding
+ * (network inference, training records, training steps).
  * launchCount counts every kernel this library launched for rendering,
  * profiling on or off.
  * ---------------------------------------------------------------------- */
 VLRResult vlrbContextSetProfiling(VLRContext context, bool enabled);
-VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[5], uint64_t stageLaunches[5],
+VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[6], uint64_t stageLaunches[6],
                                     uint64_t* launchCount);
 VLRResult vlrbContextResetKernelTimes(VLRContext context);
 /* Bytes of kernel parameters passed host-to-device with the counted launches

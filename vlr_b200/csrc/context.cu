@@ -440,6 +440,7 @@ void Context::buildScene(cudaStream_t stream) {
     sg.tan = upload(f.tan, stream);
     sg.tri = upload(f.tri, stream);
     sg.triMaterial = upload(f.triMaterial, stream);
+    for (MatDesc &md : f.mats) md.bsdfFlags = options.consistentDielectricPdf ? kBsdfConsistentPdf : 0u;
     sg.mats = upload(f.mats, stream);
     if (f.pos.empty()) { f.lo = V3(0.0f); f.hi = V3(0.0f); }
     sg.bounds.lo = f.lo;
@@ -564,16 +565,70 @@ void Context::setupCamera(const Camera* cam) {
 }
 
 void Context::ensurePathBuffers(uint32_t paths) {
-    if (paths <= pathCapacity) return;
-    pathMem.resize(pathBufferBytes(paths));
-    carvePathBuffers(pathMem.ptr, paths, &pb);
+    const uint64_t seed = options.rngSeed ? options.rngSeed : 591842031321323413ull;
+    if (paths <= pathCapacity && seed == pathSeed) return;
+    if (paths > pathCapacity) {
+        if (pathCapacity > 0) {
+            // keep the running totals across the reallocation
+            unsigned long long t[2];
+            ck(cudaMemcpy(t, pb.totals, 16, cudaMemcpyDeviceToHost), "totals");
+            totalsBase[0] += t[0];
+            totalsBase[1] += t[1];
+        }
+        pathMem.resize(pathBufferBytes(paths));
+        carvePathBuffers(pathMem.ptr, paths, &pb);
+        ck(cudaMemset(pb.totals, 0, 16), "totals");
+        pathCapacity = paths;
+    }
+    pathSeed = seed;
+    paths = pathCapacity;
     std::vector<uint64_t> seeds(paths);
     // Per-slot PCG32 states from std::mt19937_64, slot order = pixel order for
     // the first sample of each pixel (context.cpp:1176-1190).
-    seedPathRngs(seeds.data(), paths, 591842031321323413ull);
+    seedPathRngs(seeds.data(), paths, seed);
     ck(cudaMemcpy(pb.rng, seeds.data(), size_t(paths) * 8, cudaMemcpyHostToDevice), "seed rngs");
-    ck(cudaMemset(pb.totals, 0, 16), "totals");
-    pathCapacity = paths;
+}
+
+void Context::ensureGuiding(uint32_t paths) {
+    const GuidingOptions &g = guiding;
+    if (!guideNet || guideNet->net.log2Table != g.log2TableSize) {
+        guideNet.reset(new guide::GuideNet(g.log2TableSize, 0x5EED0001ull));
+        guideLaunches = 0;
+        guidingStats = GuidingStats{};
+    }
+    const float lo[3] = { sg.bounds.lo.x, sg.bounds.lo.y, sg.bounds.lo.z };
+    const float hi[3] = { sg.bounds.hi.x, sg.bounds.hi.y, sg.bounds.hi.z };
+    guideNet->setBounds(lo, hi);
+    const uint32_t rec = std::min<uint32_t>(std::max<uint32_t>(g.recordBounces, 1u), kMaxRecBounces);
+    const uint32_t cap = 2 * g.samplesPerStep;
+    if (paths > guideCapacityPaths || rec != guideRecBounces || cap != guideSampleCapacity) {
+        guideMem.resize(guideBufferBytes(paths, rec, cap));
+        ck(cudaMemset(guideMem.ptr, 0, guideMem.bytes), "guide buffers");
+        carveGuideBuffers(guideMem.ptr, paths, rec, cap, &gframe);
+        guideCapacityPaths = paths;
+        guideRecBounces = rec;
+        guideSampleCapacity = cap;
+    }
+}
+
+uint32_t Context::guideSamplesRecorded() const {
+    if (!gframe.counts) return 0;
+    uint32_t n = 0;
+    ck(cudaMemcpy(&n, gframe.counts, 4, cudaMemcpyDeviceToHost), "guide counts");
+    return std::min(n, guideSampleCapacity);
+}
+
+// Training steps on the samples the last launch recorded; the sample count
+// stays on the device.
+void Context::trainGuide(cudaStream_t stream) {
+    for (uint32_t s = 0; s < guiding.stepsPerLaunch; ++s) {
+        timer.begin(kStageGuide, stream, 64);
+        guideNet->gradients(gframe.samples, guideSampleCapacity, stream, gframe.counts);
+        guideNet->step(guiding.learningRate, stream);
+        timer.end(stream);
+        timer.totalLaunches += 5;
+        ++guidingStats.trainingSteps;
+    }
 }
 
 void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
@@ -633,6 +688,18 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 bptRenderLaunch(sg, pb, lightPb, bb, fl, bf, lightPaths, wls, wlPdf, numSMs, stream, &timer);
                 k = 1;
             }
+            else if (guiding.enabled || guiding.train) {
+                ensureGuiding(pathCapacity);
+                gframe.record = guiding.train;
+                gframe.sample = guiding.enabled && (!guiding.train || guideLaunches >= guiding.warmupLaunches);
+                gframe.net = guideNet->net;
+                gframe.stamp = ++guideStamp;
+                gframe.targetSamples = guiding.samplesPerStep;
+                ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer, &gframe);
+                if (gframe.sample) ++guidingStats.guidedLaunches;
+                if (guiding.train) trainGuide(stream);
+                ++guideLaunches;
+            }
             else {
                 ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer);
             }
@@ -658,8 +725,8 @@ void Context::readStats(RenderStats* out) {
         ck(cudaMemcpy(&e, sg.bvh.errorFlag, 4, cudaMemcpyDeviceToHost), "bvh flag");
         if (e) throw std::runtime_error("BVH traversal met an out-of-range node reference");
     }
-    out->segments = t[0] + tl[0];
-    out->shadowRays = t[1] + tl[1];
+    out->segments = t[0] + tl[0] + totalsBase[0];
+    out->shadowRays = t[1] + tl[1] + totalsBase[1];
     if (bptCapacityPaths > 0) {
         uint32_t c[2];
         ck(cudaMemcpy(c, bb.counters, 8, cudaMemcpyDeviceToHost), "overflow");

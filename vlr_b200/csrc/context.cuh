@@ -5,6 +5,9 @@
 #include "api_objects.h"
 #include "pt.cuh"
 #include "bpt.cuh"
+#include "guide_net.h"
+
+#include <memory>
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -29,6 +32,26 @@ struct RenderOptions {
     uint32_t maxPathLength = 25;      // path_tracing.cu:78, lvc_bpt.cu:216,513
     uint32_t maxPathsInFlight = 1u << 22;
     uint32_t lightPathsPerFrame = 0;  // 0: width * height
+    uint64_t rngSeed = 0;             // 0: 591842031321323413 (context.cpp:1176-1190)
+    bool consistentDielectricPdf = false;   // see mfBsdfPDF; false = the reference's pdf
+};
+
+// Learned guiding of the path tracer (vlrbContextSetGuiding).
+struct GuidingOptions {
+    bool enabled = false;             // guided sampling at Matte / LambertianScattering / UE4 vertices
+    bool train = false;               // record samples and train after every launch
+    uint32_t log2TableSize = 19;
+    float learningRate = 1e-2f;
+    uint32_t samplesPerStep = 1u << 18;
+    uint32_t stepsPerLaunch = 1;
+    uint32_t recordBounces = 4;
+    uint32_t warmupLaunches = 4;      // launches that train on plain BSDF sampling first
+};
+
+struct GuidingStats {
+    float lastLoss = 0.0f;
+    uint64_t trainingSteps = 0;
+    uint64_t guidedLaunches = 0;
 };
 
 struct RenderStats {
@@ -61,6 +84,7 @@ public:
     void* outputDevicePtr() const { return output.ptr; }
     void* filmDevicePtr() const { return film.ptr; }
     uint32_t numTriangles() const { return sg.numTris; }
+    uint32_t guideSamplesRecorded() const;
 
     CUcontext cuContext;
     bool logging;
@@ -69,6 +93,8 @@ public:
     Scene* scene = nullptr;
     VLRRenderer renderer = VLRRenderer_PathTracing;
     RenderOptions options;
+    GuidingOptions guiding;
+    GuidingStats guidingStats;
     RenderStats stats;
     StageTimer timer;
     uint32_t numAccumFrames = 0;
@@ -78,6 +104,16 @@ private:
     void buildScene(cudaStream_t stream);
     void setupCamera(const Camera* cam);
     void ensurePathBuffers(uint32_t paths);
+    void ensureGuiding(uint32_t paths);
+    void trainGuide(cudaStream_t stream);
+
+public:
+    std::unique_ptr<guide::GuideNet> guideNet;
+private:
+    DeviceBuffer guideMem;
+    GuideFrame gframe{};
+    uint32_t guideCapacityPaths = 0, guideLaunches = 0, guideRecBounces = 0, guideSampleCapacity = 0;
+    uint32_t guideStamp = 0;
 
     SceneGPU sg{};
     std::vector<std::unique_ptr<DeviceBuffer>> sceneBufs;
@@ -87,6 +123,8 @@ private:
     std::mt19937_64 bptRng{ 459182033132123413ull };
     BptBuffers bb{};
     uint32_t pathCapacity = 0;
+    uint64_t pathSeed = 0;
+    unsigned long long totalsBase[2] = { 0, 0 };
     uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0, bptEyeCapacity = 0;
     CUarray outArray = nullptr;
     uint32_t* hostCounters = nullptr;

@@ -596,12 +596,16 @@ struct BsdfRev {
     float dirPDF;
 };
 
+// Bsdf::flags of a MicrofacetBSDF: evaluate the pdf of transmission out of
+// the medium consistently with the value (see mfBsdfPDF).
+constexpr uint32_t kBsdfConsistentPdf = 1u;
+
 // All BSDF parameters in one flat record (largest member: MicrofacetBSDF).
 struct Bsdf {
     uint32_t kind;
     S4 a, b, c;         // per-kind spectra
     float f0, f1, f2;   // per-kind scalars
-    uint32_t flags;     // SpecularBSDF: dispersive
+    uint32_t flags;     // SpecularBSDF: dispersive; MicrofacetBSDF: kBsdfConsistentPdf
 };
 
 // MatteBRDF (materials.cu:584-651)
@@ -843,6 +847,15 @@ VLRB_HD S4 mfBsdfEval(const Bsdf &B, const BsdfQuery &q, const V3 &d, S4* revVal
     }
     return S4::zero();
 }
+// The reference's pdf builds the transmission half vector without the
+// orientation flip its value function applies to paths leaving the medium
+// (evaluatePDFInternal, materials.cu:1448-1513, vs evaluateInternal,
+// :1385-1446), so every transmission out of the
+// dielectric gets pdf 0: MIS then gives NEE full weight through the exit
+// although BSDF sampling also reaches those paths (double counting), and the
+// unsuppressed NEE values near the GGX peak are fireflies.  Kept by default
+// for parity; Bsdf::flags & kBsdfConsistentPdf applies the same flip as the
+// value function.
 VLRB_HD float mfBsdfPDF(const Bsdf &B, const BsdfQuery &q, const V3 &d, float* revPDF) {
     if (revPDF) *revPDF = 0.0f;
     bool entering = q.dirLocal.z >= 0.0f;
@@ -856,7 +869,10 @@ VLRB_HD float mfBsdfPDF(const Bsdf &B, const BsdfQuery &q, const V3 &d, float* r
     if (nvnl == 0) return 0.0f;
     V3 m;
     if (nvnl > 0) m = halfVector(dirV, dirL);
-    else m = normalize(-(eEnter[q.wlHint] * dirV + eExit[q.wlHint] * dirL));
+    else {
+        m = normalize(-(eEnter[q.wlHint] * dirV + eExit[q.wlHint] * dirL));
+        if ((B.flags & kBsdfConsistentPdf) && !entering) m = -m;
+    }
     float dotHV = dot(dirV, m);
     if (dotHV <= 0) return 0.0f;
     float mPDF = ggx.pdf(dirV, m);

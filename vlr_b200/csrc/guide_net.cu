@@ -51,7 +51,8 @@ __global__ void adamKernel(float* param, float* grad, float* m, float* v, size_t
     (void)rowMask;
 }
 
-__global__ void sumWeightsKernel(const Sample* s, uint32_t n, float* out) {
+__global__ void sumWeightsKernel(const Sample* s, uint32_t n, const uint32_t* countDev, float* out) {
+    if (countDev) n = min(*countDev, n);
     float acc = 0.0f;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         acc += s[i].posWeight.w;
@@ -172,15 +173,15 @@ void GuideNet::inferArrays(const float* pos, const float* wo, const float* nrm, 
     ck(cudaGetLastError(), "infer launch");
 }
 
-void GuideNet::gradients(const Sample* samples, uint32_t n, cudaStream_t stream) {
+void GuideNet::gradients(const Sample* samples, uint32_t n, cudaStream_t stream, const uint32_t* countDev) {
     ck(cudaMemsetAsync(scalars, 0, 8 * 4, stream), "scalars");
     if (n == 0) return;
-    sumWeightsKernel<<<numSMs * 4, 256, 0, stream>>>(samples, n, scalars);
+    sumWeightsKernel<<<numSMs * 4, 256, 0, stream>>>(samples, n, countDev, scalars);
     ck(cudaFuncSetAttribute(guideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmemBytes),
        "smem attr");
     const uint32_t tiles = (n + kRows - 1) / kRows;
     const uint32_t grid = tiles < uint32_t(numSMs) ? tiles : uint32_t(numSMs);
-    TrainArgs a{ samples, n, scalars, dwSlabs, scalars + 1, err };
+    TrainArgs a{ samples, n, countDev, scalars, dwSlabs, scalars + 1, err };
     guideTrainKernel<<<grid, kRows, kTrainSmemBytes, stream>>>(net, a);
     reduceDwKernel<<<(kDwSlabFloats + 255) / 256, 256, 0, stream>>>(dwSlabs, grid, net.wGrad);
     ck(cudaGetLastError(), "train launch");

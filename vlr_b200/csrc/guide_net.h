@@ -23,7 +23,9 @@ public:
                      cudaStream_t stream);
     // Gradients of the batch loss into net.wGrad / net.gridGrad (the grid
     // gradient accumulates; the optimiser step consumes it).
-    void gradients(const Sample* samples, uint32_t n, cudaStream_t stream);
+    // countDev (optional): device word holding the number of valid samples
+    // (at most n); the launch then needs no host round trip.
+    void gradients(const Sample* samples, uint32_t n, cudaStream_t stream, const uint32_t* countDev = nullptr);
     void step(float lr, cudaStream_t stream);
     uint32_t errorBits() const;
     float lastLoss() const;

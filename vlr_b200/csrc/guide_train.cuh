@@ -34,7 +34,8 @@ constexpr uint32_t kDwSlabFloats = kNumLayers * kHidden * kHidden;   // per CTA
 
 struct TrainArgs {
     const Sample* samples;
-    uint32_t count;
+    uint32_t count;            // buffer capacity (or the exact count when countDev is null)
+    const uint32_t* countDev;  // device sample count (clamped to count), or null
     const float* weightSum;    // device: sum of the batch's sample weights
     float* dwSlabs;            // [gridDim.x][4][64][64]
     float* lossSum;            // device accumulator of the batch loss
@@ -137,9 +138,10 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
         __syncthreads();
     };
 
-    for (uint32_t tile = blockIdx.x; ok && tile * kRows < a.count; tile += gridDim.x) {
+    const uint32_t count = a.countDev ? min(*a.countDev, a.count) : a.count;
+    for (uint32_t tile = blockIdx.x; ok && tile * kRows < count; tile += gridDim.x) {
         const uint32_t row = tile * kRows + tid;
-        const bool valid = row < a.count;
+        const bool valid = row < count;
         Sample s;
         if (valid) s = a.samples[row];
         else s = Sample{ make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 1.f, 0.f),

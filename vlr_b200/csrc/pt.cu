@@ -16,6 +16,7 @@
 // Queue lengths live in device counters, so a launch never synchronises with
 // the host and its fixed kernel sequence can be captured in a CUDA graph.
 #include "pt.cuh"
+#include "guide_mlp.cuh"
 #include "tables.cuh"
 #include "wavefront.cuh"
 
@@ -136,7 +137,33 @@ __device__ __forceinline__ void shadeMiss(const SceneGPU &S, const PathBuffers &
     contrib += toS4(pb.alpha[p]) * Le * MIS;
 }
 
-__global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
+__device__ __forceinline__ float4* recField(const GuideFrame &gf, uint32_t P, uint32_t b, uint32_t f) {
+    return gf.rec + (static_cast<size_t>(b) * kRecFields + f) * P;
+}
+
+// Completes the training record of the previous bounce with the path's
+// contribution before anything of this vertex is added.
+__device__ __forceinline__ void completeRecord(const GuideFrame &gf, uint32_t P, uint32_t bounce, uint32_t p,
+                                               uint32_t flags, const S4 &contrib) {
+    if (!(flags & kFlagRecordPending) || bounce == 0) return;
+    const uint32_t b = bounce - 1;
+    recField(gf, P, b, 5)[p] = toF4(contrib);
+    gf.recStamp[static_cast<size_t>(b) * P + p] = gf.stamp;
+}
+
+__device__ __forceinline__ void loadMixture(const GuideFrame &gf, uint32_t P, uint32_t p, guide::Mixture &m) {
+#pragma unroll
+    for (int k = 0; k < guide::kLobes; ++k) m.lobe[k] = gf.lobes[static_cast<size_t>(k) * P + p];
+    const float4 w0 = gf.lobeWeights[p], w1 = gf.lobeWeights[static_cast<size_t>(P) + p];
+    m.weight[0] = w0.x; m.weight[1] = w0.y; m.weight[2] = w0.z; m.weight[3] = w0.w;
+    m.weight[4] = w1.x; m.weight[5] = w1.y; m.weight[6] = w1.z; m.weight[7] = w1.w;
+}
+
+// Three resident 256-thread blocks per SM (85 registers): the kernel is
+// bound by memory latency, and the extra warps hide more of it than the
+// few spilled registers cost.
+template <bool kGuide>
+__global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb, FrameParams fp, GuideFrame gf) {
     uint32_t* ctr = bounceCounters(pb, fp.bounce);
     uint32_t* next = bounceCounters(pb, fp.bounce + 1);
     __shared__ uint32_t sOff[kNumShadeBuckets + 1];
@@ -157,8 +184,9 @@ __global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, F
         uint32_t flags = pb.flags[p];
         uint32_t pathLength = ((flags >> 8) & 0xFFFFu) + 1;
         bool maxLengthTerminate = pathLength >= fp.maxPathLength;
-        flags = (flags & 0x1Fu) | (pathLength << 8) | (maxLengthTerminate ? 0x20u : 0u);
         S4 contrib = toS4(pb.contrib[p]);
+        if constexpr (kGuide) completeRecord(gf, P, fp.bounce, p, flags, contrib);
+        flags = (flags & 0x1Fu) | (pathLength << 8) | (maxLengthTerminate ? 0x20u : 0u);
         if (k == kNumBsdfKinds) {
             shadeMiss(S, pb, p, wls, pathLength, contrib);
             pb.contrib[p] = toF4(contrib);
@@ -204,6 +232,12 @@ __global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, F
         q.wlHint = wls.selected;
         q.filter = dir::All;
         q.importanceMode = 0;
+        bool guided = false;
+        guide::Mixture mix;
+        if constexpr (kGuide) {
+            guided = gf.sample && isGuidedKind(k);
+            if (guided) loadMixture(gf, P, p, mix);
+        }
         // next-event estimation
         if (bsdfHasNonDelta(bsdf) && S.lightInsts.n > 0) {
             float uLight = rng.uniform();
@@ -268,7 +302,11 @@ __global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, F
                 float lightPDF = lightProb * ls.areaPDF;
                 S4 fs = bsdfEval(bsdf, q, gnLocal, dirSn, nullptr);
                 float cosLight = ls.sp.atInfinity ? absDot(-shadowDir, ls.sp.gn) : absDot(-shadowDir, ls.sp.gn);
-                float bsdfPdfV = bsdfPDF(bsdf, q, dirSn, nullptr) * cosLight * recSqDist;
+                float dirPdfV = bsdfPDF(bsdf, q, dirSn, nullptr);
+                if constexpr (kGuide) {
+                    if (guided) dirPdfV = 0.5f * dirPdfV + 0.5f * guide::mixturePdf(mix, shadowDir);
+                }
+                float bsdfPdfV = dirPdfV * cosLight * recSqDist;
                 float MIS = 1.0f;
                 if (!ls.delta && !isinf(lightPDF))
                     MIS = (lightPDF * lightPDF) / (lightPDF * lightPDF + bsdfPdfV * bsdfPdfV);
@@ -285,20 +323,54 @@ __global__ void __launch_bounds__(256) shadeKernel(SceneGPU S, PathBuffers pb, F
                 }
             }
         }
-        // BSDF sampling
+        // BSDF sampling (guided kinds: one-sample MIS of BSDF and mixture)
         float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
-        pb.rng[p] = rng.state;
         BsdfSample bs;
-        S4 fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
-        if (fs.isZero() || bs.dirPDF == 0.0f) continue;
+        S4 fs;
+        if constexpr (kGuide) {
+            if (guided) {
+                const float uSel = rng.uniform();
+                V3 wiW;
+                float pB;
+                if (uSel < 0.5f) {
+                    wiW = guide::mixtureSample(mix, uc, ud0, ud1);
+                    bs.dirLocal = sp.frame.toLocal(wiW);
+                    fs = bsdfEval(bsdf, q, gnLocal, bs.dirLocal, nullptr);
+                    pB = bsdfPDF(bsdf, q, bs.dirLocal, nullptr);
+                    bs.sampledType = dir::LowFreq | (dot(bs.dirLocal, gnLocal) > 0.0f ? dir::Reflection
+                                                                                       : dir::Transmission);
+                }
+                else {
+                    fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
+                    pB = bs.dirPDF;
+                    wiW = sp.frame.fromLocal(bs.dirLocal);
+                }
+                bs.dirPDF = 0.5f * pB + 0.5f * guide::mixturePdf(mix, wiW);
+            }
+            else fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
+        }
+        else fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
+        pb.rng[p] = rng.state;
+        if (fs.isZero() || !(bs.dirPDF > 0.0f)) continue;
         if (dir::isDispersive(bs.sampledType) && !wls.single) {
             bs.dirPDF /= kNumLambdas;
             flags |= 0x10u;
             pb.flags[p] = flags;
         }
         float cosFactor = dot(bs.dirLocal, gnLocal);
-        alpha *= fs * (fabsf(cosFactor) / bs.dirPDF);
         V3 dirIn = sp.frame.fromLocal(bs.dirLocal);
+        if constexpr (kGuide) {
+            if (gf.record && fp.bounce < gf.recBounces && isGuidedKind(k)) {
+                recField(gf, P, fp.bounce, 0)[p] = make_float4(sp.position.x, sp.position.y, sp.position.z, 0.0f);
+                recField(gf, P, fp.bounce, 1)[p] = make_float4(sp.frame.z.x, sp.frame.z.y, sp.frame.z.z, 0.0f);
+                recField(gf, P, fp.bounce, 2)[p] = make_float4(-rayDir.x, -rayDir.y, -rayDir.z, 0.0f);
+                recField(gf, P, fp.bounce, 3)[p] = make_float4(dirIn.x, dirIn.y, dirIn.z, 0.0f);
+                recField(gf, P, fp.bounce, 4)[p] = toF4(alpha);
+                flags |= kFlagRecordPending;
+                pb.flags[p] = flags;
+            }
+        }
+        alpha *= fs * (fabsf(cosFactor) / bs.dirPDF);
         V3 org = offsetRayOrigin(sp.position, cosFactor > 0.0f ? sp.gn : -sp.gn);
         pb.alpha[p] = toF4(alpha);
         pb.prevDirPDF[p] = bs.dirPDF;
@@ -322,6 +394,110 @@ __global__ void __launch_bounds__(256) shadowKernel(SceneGPU S, PathBuffers pb, 
             pb.contrib[p] = c;
         }
     }
+}
+
+// ---- learned guiding: network queries straight from the sorted hit queues
+struct GuidedHitSrc {
+    SceneGPU S;
+    PathBuffers pb;
+    FrameParams fp;
+    guide::Net net;
+    __device__ void counts(uint32_t c[3]) const {
+        const uint32_t* ctr = bounceCounters(pb, fp.bounce);
+        c[0] = ctr[kCntBucket0 + kMatte];
+        c[1] = ctr[kCntBucket0 + kLambertianBSDF];
+        c[2] = ctr[kCntBucket0 + kUE4];
+    }
+    __device__ uint32_t count() const {
+        uint32_t c[3];
+        counts(c);
+        return c[0] + c[1] + c[2];
+    }
+    __device__ uint32_t pathOf(uint32_t i) const {
+        uint32_t c[3];
+        counts(c);
+        uint32_t k = kMatte;
+        if (i >= c[0]) { i -= c[0]; k = kLambertianBSDF; if (i >= c[1]) { i -= c[1]; k = kUE4; } }
+        return pb.buckets[k * fp.numPaths + i];
+    }
+    __device__ bool load(uint32_t i, float3* p01, V3* wo, V3* nrm) const {
+        const uint32_t p = pathOf(i);
+        const float4 h = pb.hit[p];
+        SurfPt sp;
+        float hyp;
+        decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, &hyp);
+        const float4 d = pb.rayDir[p];
+        *p01 = guide::normalisedPosition(net, sp.position.x, sp.position.y, sp.position.z);
+        *wo = V3(-d.x, -d.y, -d.z);
+        *nrm = sp.frame.z;
+        return true;
+    }
+};
+
+struct MixtureDst {
+    GuidedHitSrc src;
+    float4* lobes;
+    float4* lobeWeights;
+    __device__ void store(uint32_t i, const float y[guide::kOut]) const {
+        const uint32_t p = src.pathOf(i);
+        const uint32_t P = src.fp.numPaths;
+        guide::Mixture m;
+        guide::decodeMixture(y, m);
+#pragma unroll
+        for (int k = 0; k < guide::kLobes; ++k) lobes[static_cast<size_t>(k) * P + p] = m.lobe[k];
+        lobeWeights[p] = make_float4(m.weight[0], m.weight[1], m.weight[2], m.weight[3]);
+        lobeWeights[static_cast<size_t>(P) + p] = make_float4(m.weight[4], m.weight[5], m.weight[6], m.weight[7]);
+    }
+};
+
+__device__ __forceinline__ uint32_t mixBits(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u ^ c * 0xC2B2AE3Du;
+    h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12; h *= 0x297A2D39u; h ^= h >> 15;
+    return h;
+}
+
+// Turns the launch's complete records into training samples: weight =
+// mean over the 4 wavelengths of (contribution gathered after the vertex) /
+// (throughput at the vertex), i.e. incident radiance x BSDF x cos / pdf of the
+// sampled direction.  A random subset of about targetSamples is kept.
+__global__ void __launch_bounds__(256) guideFinalizeKernel(PathBuffers pb, FrameParams fp, GuideFrame gf) {
+    const uint32_t P = fp.numPaths;
+    const uint32_t last = gf.counts[2];
+    const float accept = last > gf.targetSamples ? static_cast<float>(gf.targetSamples) / last : 1.0f;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const float4 cEnd = pb.contrib[p];
+        for (uint32_t b = 0; b < gf.recBounces; ++b) {
+            if (gf.recStamp[static_cast<size_t>(b) * P + p] != gf.stamp) continue;
+            const float4 beta = recField(gf, P, b, 4)[p];
+            const float4 snap = recField(gf, P, b, 5)[p];
+            const float bt[4] = { beta.x, beta.y, beta.z, beta.w };
+            const float dc[4] = { cEnd.x - snap.x, cEnd.y - snap.y, cEnd.z - snap.z, cEnd.w - snap.w };
+            float w = 0.0f;
+            for (int i = 0; i < 4; ++i)
+                if (bt[i] > 0.0f) w += fmaxf(dc[i], 0.0f) / bt[i];
+            w *= 0.25f;
+            if (!(w > 0.0f) || !isfinite(w)) continue;
+            atomicAdd(gf.counts + 1, 1u);
+            const float u = (mixBits(p, b, gf.stamp) >> 8) * (1.0f / 16777216.0f);
+            if (u >= accept) continue;
+            const uint32_t slot = atomicAdd(gf.counts, 1u);
+            if (slot >= gf.sampleCapacity) continue;
+            const float4 pos = recField(gf, P, b, 0)[p];
+            guide::Sample smp;
+            smp.posWeight = make_float4(pos.x, pos.y, pos.z, w);
+            smp.nrm = recField(gf, P, b, 1)[p];
+            smp.wo = recField(gf, P, b, 2)[p];
+            smp.wi = recField(gf, P, b, 3)[p];
+            gf.samples[slot] = smp;
+        }
+    }
+}
+
+// Start of a recording launch: accepted = 0, last = this, this = 0.
+__global__ void guideCountsKernel(uint32_t* counts) {
+    counts[2] = counts[1] > 0 ? counts[1] : counts[2];
+    counts[1] = 0;
+    counts[0] = 0;
 }
 
 __global__ void __launch_bounds__(256) filmKernel(PathBuffers pb, Film film, FrameParams fp) {
@@ -426,6 +602,31 @@ void carvePathBuffers(void* base, uint32_t P, PathBuffers* pb) {
     pb->totals = reinterpret_cast<unsigned long long*>(take(16));
 }
 
+size_t guideBufferBytes(uint32_t P, uint32_t recBounces, uint32_t sampleCapacity) {
+    size_t b = 0;
+    b += a256(size_t(P) * 16 * guide::kLobes);
+    b += a256(size_t(P) * 16 * 2);
+    b += a256(size_t(P) * 16 * kRecFields * recBounces);
+    b += a256(size_t(P) * 4 * recBounces);
+    b += a256(size_t(sampleCapacity) * sizeof(guide::Sample));
+    b += a256(64);
+    return b;
+}
+
+void carveGuideBuffers(void* base, uint32_t P, uint32_t recBounces, uint32_t sampleCapacity, GuideFrame* gf) {
+    char* s = static_cast<char*>(base);
+    auto take = [&](size_t bytes) { char* r = s; s += a256(bytes); return r; };
+    gf->lobes = reinterpret_cast<float4*>(take(size_t(P) * 16 * guide::kLobes));
+    gf->lobeWeights = reinterpret_cast<float4*>(take(size_t(P) * 16 * 2));
+    gf->rec = reinterpret_cast<float4*>(take(size_t(P) * 16 * kRecFields * recBounces));
+    gf->recStamp = reinterpret_cast<uint32_t*>(take(size_t(P) * 4 * recBounces));
+    gf->samples = reinterpret_cast<guide::Sample*>(take(size_t(sampleCapacity) * sizeof(guide::Sample)));
+    gf->counts = reinterpret_cast<uint32_t*>(take(64));
+    gf->err = gf->counts + 8;
+    gf->recBounces = recBounces;
+    gf->sampleCapacity = sampleCapacity;
+}
+
 void seedPathRngs(uint64_t* states, uint32_t n, uint64_t seed) {
     std::mt19937_64 gen(seed);
     for (uint32_t i = 0; i < n; ++i) states[i] = gen();
@@ -465,7 +666,7 @@ void StageTimer::collect() {
 }
 
 void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fpIn,
-                    int numSMs, cudaStream_t stream, StageTimer* timer) {
+                    int numSMs, cudaStream_t stream, StageTimer* timer, const GuideFrame* gfp) {
     FrameParams fp = fpIn;
     if (fp.maxPathLength == 0 || fp.maxPathLength > kMaxBounces)
         throw std::runtime_error("maxPathLength out of range");
@@ -477,16 +678,38 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
     T.begin(kStageCamera, stream, pMain);
     cameraKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
     T.end(stream);
+    const bool guiding = gfp && (gfp->sample || gfp->record);
+    if (guiding && gfp->record) {
+        T.begin(kStageGuide, stream, sizeof(void*));
+        guideCountsKernel<<<1, 1, 0, stream>>>(gfp->counts);
+        T.end(stream);
+    }
     for (uint32_t b = 0; b < fp.maxPathLength; ++b) {
         fp.bounce = b;
         T.begin(kStageTrace, stream, pMain);
         traceKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
         T.end(stream);
-        T.begin(kStageShade, stream, pMain);
-        shadeKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        if (guiding && gfp->sample) {
+            GuidedHitSrc src{ scene, pb, fp, gfp->net };
+            MixtureDst dst{ src, gfp->lobes, gfp->lobeWeights };
+            auto kern = guide::guideInferKernel<GuidedHitSrc, MixtureDst>;
+            ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, guide::kInferSmemBytes),
+               "infer smem");
+            T.begin(kStageGuide, stream, sizeof(guide::Net) + 2 * sizeof(GuidedHitSrc));
+            kern<<<numSMs * 3, guide::kRows, guide::kInferSmemBytes, stream>>>(gfp->net, src, dst, gfp->err);
+            T.end(stream);
+        }
+        T.begin(kStageShade, stream, pMain + (guiding ? sizeof(GuideFrame) : 0));
+        if (guiding) shadeKernel<true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
+        else shadeKernel<false><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
         T.end(stream);
         T.begin(kStageShadow, stream, pMain);
         shadowKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
+        T.end(stream);
+    }
+    if (guiding && gfp->record) {
+        T.begin(kStageGuide, stream, sizeof(PathBuffers) + sizeof(FrameParams) + sizeof(GuideFrame));
+        guideFinalizeKernel<<<grid, 256, 0, stream>>>(pb, fp, *gfp);
         T.end(stream);
     }
     T.begin(kStageFilm, stream, sizeof(PathBuffers) + sizeof(Film) + sizeof(FrameParams));

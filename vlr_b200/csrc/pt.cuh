@@ -2,6 +2,7 @@
 #pragma once
 
 #include "scene_gpu.cuh"
+#include "guide.cuh"
 #include <cuda_runtime.h>
 
 namespace vlrb {
@@ -57,6 +58,42 @@ struct Film {
     uint32_t width, height;
 };
 
+// Learned guiding for one launch.  `sample`: guided kinds (Matte,
+// LambertianScattering, UE4) draw their next direction from the network's
+// vMF mixture or the BSDF with probability 1/2 each and weight by the
+// combined density (one-sample MIS).  `record`: every guided-kind vertex of
+// the first recBounces bounces stores a training record; after the launch
+// each record becomes a training sample (position, directions, weight =
+// radiance carried back along wi x BSDF x cos / pdf, per path).
+constexpr uint32_t kMaxRecBounces = 8;
+constexpr uint32_t kRecFields = 6;          // pos, normal, wo, wi, throughput, contribution snapshot
+constexpr uint32_t kFlagRecordPending = 1u << 24;
+
+struct GuideFrame {
+    bool sample;
+    bool record;
+    uint32_t recBounces;
+    guide::Net net;
+    float4* lobes;             // [kLobes][P]  (mu, kappa)
+    float4* lobeWeights;       // [2][P]       mixture weights
+    float4* rec;               // [recBounces][kRecFields][P]
+    uint32_t* recStamp;        // [recBounces][P] frame stamp once a record is complete
+    uint32_t stamp;
+    guide::Sample* samples;    // training-sample buffer
+    uint32_t sampleCapacity;
+    uint32_t targetSamples;    // samples wanted per launch
+    uint32_t* counts;          // [0] accepted, [1] candidates this launch, [2] candidates last launch
+    uint32_t* err;
+};
+
+__host__ __device__ constexpr bool isGuidedKind(uint32_t k) {
+    return k == kMatte || k == kLambertianBSDF || k == kUE4;
+}
+
+size_t guideBufferBytes(uint32_t numPaths, uint32_t recBounces, uint32_t sampleCapacity);
+// Carves the per-path guiding buffers (lobes, records, samples, counters).
+void carveGuideBuffers(void* base, uint32_t numPaths, uint32_t recBounces, uint32_t sampleCapacity, GuideFrame* gf);
+
 size_t pathBufferBytes(uint32_t numPaths);
 void carvePathBuffers(void* base, uint32_t numPaths, PathBuffers* pb);
 
@@ -73,7 +110,8 @@ struct PTStats {
 // counterHost (pinned, optional) receives the per-bounce counters after the
 // launch for statistics.
 // Optional per-stage timing with CUDA events on the launching stream.
-enum PtStage : uint32_t { kStageCamera = 0, kStageTrace, kStageShade, kStageShadow, kStageFilm, kNumPtStages };
+enum PtStage : uint32_t { kStageCamera = 0, kStageTrace, kStageShade, kStageShadow, kStageFilm, kStageGuide,
+                          kNumPtStages };
 struct StageTimer {
     bool enabled = false;
     static constexpr uint32_t kSlots = 3 * kMaxBounces + 4;
@@ -94,7 +132,7 @@ struct StageTimer {
 };
 
 void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &film, const FrameParams &fp,
-                    int numSMs, cudaStream_t stream, StageTimer* timer = nullptr);
+                    int numSMs, cudaStream_t stream, StageTimer* timer = nullptr, const GuideFrame* guide = nullptr);
 
 // Convert the FP64 film to RGBA32F: XYZ / frames * (W*H) -> Rec.709 D65
 // (post_process.cu:93-163).

@@ -23,7 +23,7 @@ struct MatDesc {
     float f[4];             // per-kind scalars
     UpSpec emit;            // emittance
     float emitScale;
-    uint32_t pad;
+    uint32_t bsdfFlags;     // Bsdf::flags bits chosen at scene build (kBsdfConsistentPdf)
 };
 
 // A discrete distribution in the reference's layout (shared/shared.h:182-231):
@@ -139,6 +139,7 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
         B.b = mengEvaluate(T, m.sp[1], wls);
         B.c = mengEvaluate(T, m.sp[2], wls);
         if (m.bsdfKind == kSpecularBSDF) B.flags = wls.single ? 0u : 1u;
+        if (m.bsdfKind == kMicrofacetBSDF) B.flags = m.bsdfFlags & kBsdfConsistentPdf;
         break;
     case kMicrofacetBRDF:
         B.b = mengEvaluate(T, m.sp[1], wls);

@@ -1161,6 +1161,11 @@ VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOption
     c->options.maxPathLength = options->maxPathLength;
     c->options.maxPathsInFlight = options->maxPathsInFlight;
     c->options.lightPathsPerFrame = options->lightPathsPerFrame;
+    c->options.rngSeed = options->rngSeed;
+    if (c->options.consistentDielectricPdf != (options->consistentDielectricPdf != 0)) {
+        c->options.consistentDielectricPdf = options->consistentDielectricPdf != 0;
+        c->markDirty();
+    }
     return VLRResult_NoError;
 }
 
@@ -1170,7 +1175,50 @@ VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* opt
     options->maxPathLength = c->options.maxPathLength;
     options->maxPathsInFlight = c->options.maxPathsInFlight;
     options->lightPathsPerFrame = c->options.lightPathsPerFrame;
+    options->rngSeed = c->options.rngSeed;
+    options->consistentDielectricPdf = c->options.consistentDielectricPdf ? 1u : 0u;
     return VLRResult_NoError;
+}
+
+VLRResult vlrbContextSetGuiding(VLRContext context, const VLRBGuidingOptions* o) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!o || o->log2TableSize < 8 || o->log2TableSize > 24 || !(o->learningRate > 0.0f) ||
+        o->samplesPerStep == 0 || o->samplesPerStep > (1u << 24) || o->recordBounces == 0 ||
+        o->recordBounces > kMaxRecBounces)
+        return VLRResult_InvalidArgument;
+    GuidingOptions &g = c->guiding;
+    g.enabled = o->enabled;
+    g.train = o->train;
+    g.log2TableSize = o->log2TableSize;
+    g.learningRate = o->learningRate;
+    g.samplesPerStep = o->samplesPerStep;
+    g.stepsPerLaunch = o->stepsPerLaunch;
+    g.recordBounces = o->recordBounces;
+    g.warmupLaunches = o->warmupLaunches;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextGetGuiding(VLRContext context, VLRBGuidingOptions* o) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!o) return VLRResult_InvalidArgument;
+    const GuidingOptions &g = c->guiding;
+    *o = VLRBGuidingOptions{ g.enabled, g.train, g.log2TableSize, g.learningRate, g.samplesPerStep,
+                             g.stepsPerLaunch, g.recordBounces, g.warmupLaunches };
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextGetGuidingStats(VLRContext context, VLRBGuidingStats* st) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!st) return VLRResult_InvalidArgument;
+    API_TRY
+    st->lastLoss = c->guideNet ? c->guideNet->lastLoss() : 0.0f;
+    st->trainingSteps = c->guidingStats.trainingSteps;
+    st->guidedLaunches = c->guidingStats.guidedLaunches;
+    st->lastSamples = c->guideSamplesRecorded();
+    if (c->guideNet && c->guideNet->errorBits())
+        throw std::runtime_error("guiding network: tensor-core wait timed out");
+    return VLRResult_NoError;
+    API_CATCH("vlrbContextGetGuidingStats")
 }
 
 VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats) {
@@ -1210,11 +1258,11 @@ VLRResult vlrbContextSetProfiling(VLRContext context, bool enabled) {
     return VLRResult_NoError;
 }
 
-VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[5], uint64_t stageLaunches[5],
+VLRResult vlrbContextGetKernelTimes(VLRContext context, double stageMs[6], uint64_t stageLaunches[6],
                                     uint64_t* launchCount) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!stageMs || !stageLaunches || !launchCount) return VLRResult_InvalidArgument;
-    for (int i = 0; i < 5; ++i) { stageMs[i] = c->timer.ms[i]; stageLaunches[i] = c->timer.launches[i]; }
+    for (int i = 0; i < 6; ++i) { stageMs[i] = c->timer.ms[i]; stageLaunches[i] = c->timer.launches[i]; }
     *launchCount = c->timer.totalLaunches;
     return VLRResult_NoError;
 }

@@ -31,12 +31,25 @@ class VLRShaderNodePlug(ctypes.Structure):
 
 class VLRBRenderOptions(ctypes.Structure):
     _fields_ = [("maxPathLength", ctypes.c_uint32), ("maxPathsInFlight", ctypes.c_uint32),
-                ("lightPathsPerFrame", ctypes.c_uint32)]
+                ("lightPathsPerFrame", ctypes.c_uint32), ("rngSeed", ctypes.c_uint64),
+                ("consistentDielectricPdf", ctypes.c_uint32)]
 
 
 class VLRBRenderStats(ctypes.Structure):
     _fields_ = [("pathSegments", ctypes.c_uint64), ("shadowRays", ctypes.c_uint64), ("frames", ctypes.c_uint64),
                 ("lightVertexOverflow", ctypes.c_uint32), ("numTriangles", ctypes.c_uint32)]
+
+
+class VLRBGuidingOptions(ctypes.Structure):
+    _fields_ = [("enabled", ctypes.c_bool), ("train", ctypes.c_bool), ("log2TableSize", ctypes.c_uint32),
+                ("learningRate", ctypes.c_float), ("samplesPerStep", ctypes.c_uint32),
+                ("stepsPerLaunch", ctypes.c_uint32), ("recordBounces", ctypes.c_uint32),
+                ("warmupLaunches", ctypes.c_uint32)]
+
+
+class VLRBGuidingStats(ctypes.Structure):
+    _fields_ = [("lastLoss", ctypes.c_float), ("trainingSteps", ctypes.c_uint64),
+                ("guidedLaunches", ctypes.c_uint64), ("lastSamples", ctypes.c_uint32)]
 
 
 RENDERER_PATH_TRACING = 0
@@ -89,10 +102,13 @@ def _api():
         "vlrbContextSetRenderOptions": [v, ctypes.POINTER(VLRBRenderOptions)],
         "vlrbContextGetRenderOptions": [v, ctypes.POINTER(VLRBRenderOptions)],
         "vlrbContextGetStats": [v, ctypes.POINTER(VLRBRenderStats)],
+        "vlrbContextSetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
+        "vlrbContextGetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
+        "vlrbContextGetGuidingStats": [v, ctypes.POINTER(VLRBGuidingStats)],
         "vlrbContextReadFilm": [v, v],
         "vlrbContextGetOutputDevicePointer": [v, ctypes.POINTER(v)],
         "vlrbContextSetProfiling": [v, ctypes.c_bool],
-        "vlrbContextGetKernelTimes": [v, ctypes.POINTER(ctypes.c_double * 5), ctypes.POINTER(ctypes.c_uint64 * 5),
+        "vlrbContextGetKernelTimes": [v, ctypes.POINTER(ctypes.c_double * 6), ctypes.POINTER(ctypes.c_uint64 * 6),
                                       ctypes.POINTER(ctypes.c_uint64)],
         "vlrbContextResetKernelTimes": [v],
         "vlrbContextGetLaunchParamBytes": [v, ctypes.POINTER(ctypes.c_uint64)],
@@ -287,7 +303,8 @@ class Context:
     def setRenderer(self, renderer):
         check(_api().vlrContextSetRenderer(self.h, renderer), "setRenderer")
 
-    def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None):
+    def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None, rng_seed=None,
+                   consistent_dielectric_pdf=None):
         o = VLRBRenderOptions()
         check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
         if max_path_length is not None:
@@ -296,7 +313,32 @@ class Context:
             o.maxPathsInFlight = max_paths_in_flight
         if light_paths_per_frame is not None:
             o.lightPathsPerFrame = light_paths_per_frame
+        if rng_seed is not None:
+            o.rngSeed = rng_seed
+        if consistent_dielectric_pdf is not None:
+            o.consistentDielectricPdf = int(bool(consistent_dielectric_pdf))
         check(_api().vlrbContextSetRenderOptions(self.h, ctypes.byref(o)), "setOptions")
+
+    def setGuiding(self, enabled=None, train=None, **kw):
+        """vlrbContextSetGuiding; keyword names are the C struct's fields
+        (log2TableSize, learningRate, samplesPerStep, stepsPerLaunch,
+        recordBounces, warmupLaunches)."""
+        o = VLRBGuidingOptions()
+        check(_api().vlrbContextGetGuiding(self.h, ctypes.byref(o)), "getGuiding")
+        if enabled is not None:
+            o.enabled = enabled
+        if train is not None:
+            o.train = train
+        for k, val in kw.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown guiding option {k}")
+            setattr(o, k, val)
+        check(_api().vlrbContextSetGuiding(self.h, ctypes.byref(o)), "setGuiding")
+
+    def guiding_stats(self):
+        st = VLRBGuidingStats()
+        check(_api().vlrbContextGetGuidingStats(self.h, ctypes.byref(st)), "getGuidingStats")
+        return {k: getattr(st, k) for k, _ in VLRBGuidingStats._fields_}
 
     def render(self, camera, first_frame, limit=1 << 30, stream=0):
         """One sample per pixel, exactly like vlrContextRender."""
@@ -331,14 +373,14 @@ class Context:
         check(_api().vlrbContextSetProfiling(self.h, bool(on)), "setProfiling")
 
     def kernel_times(self, reset=False):
-        ms = (ctypes.c_double * 5)()
-        ln = (ctypes.c_uint64 * 5)()
+        ms = (ctypes.c_double * 6)()
+        ln = (ctypes.c_uint64 * 6)()
         total = ctypes.c_uint64()
         check(_api().vlrbContextGetKernelTimes(self.h, ctypes.byref(ms), ctypes.byref(ln), ctypes.byref(total)),
               "getKernelTimes")
         if reset:
             check(_api().vlrbContextResetKernelTimes(self.h), "resetKernelTimes")
-        names = ("camera", "trace", "shade", "shadow", "film")
+        names = ("camera", "trace", "shade", "shadow", "film", "guide")
         return {n: {"ms": ms[i], "launches": ln[i]} for i, n in enumerate(names)}, total.value
 
     def launch_param_bytes(self):
