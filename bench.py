@@ -264,6 +264,99 @@ def time_to_rmse():
     return out
 
 
+# ---- the other scope-table workloads, reported beside the headline line
+BATCH_BYTES_PER_QUERY = 116     # in: wo 12, material 4, roughness 8, ior 4, albedo 12, metallic 4, u 12,
+                                # wavelength u 8; out: value 16, pdf 4, wi 12, eval value 16, eval pdf 4
+
+
+def bsdf_batch_workload(hbm_peak):
+    """2^20-query BSDF shading batches (device-resident SoA, 8 distinct
+    batches rotated so the 0.97 GB working set exceeds L2), CUDA-event
+    timed; the CPU leg is the reference's BSDF classes built for the host on
+    all cores over a bounded sample."""
+    import torch
+    import vlr_b200 as VB
+    n = 1 << 20
+    dev = torch.device("cuda")
+    batches = []
+    for b in range(8):
+        inp = VB.make_bsdf_batch_inputs(n, seed=100 + b)
+        din = {k: torch.from_numpy(np.ascontiguousarray(inp[k])).to(dev) for k in VB.BATCH_INPUTS}
+        dout = {k: torch.empty((n, c) if c > 1 else n, dtype=torch.float32, device=dev)
+                for k, c in VB.BATCH_OUTPUTS.items()}
+        batches.append((din, dout))
+    stream = torch.cuda.current_stream()
+    for i in range(8):
+        VB.bsdf_batch_device(*batches[i % 8], stream.cuda_stream)
+    iters = 64
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(iters):
+        VB.bsdf_batch_device(*batches[i % 8], stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / iters
+    gbs = n * BATCH_BYTES_PER_QUERY / (ms * 1e-3) / 1e9
+    out = {"workload": "BSDF shading batch, 2^20 queries, six BSDFs uniform, 4 hero wavelengths",
+           "queries_per_s": n / (ms * 1e-3), "ms_per_batch": ms,
+           "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                        "bytes_per_query": BATCH_BYTES_PER_QUERY}}
+    from oracle import ref
+    if ref.available():
+        m = 1 << 16
+        inp = VB.make_bsdf_batch_inputs(m, seed=7)
+        threads = os.cpu_count() or 1
+        t0 = time.time()
+        reps = 0
+        while time.time() - t0 < 3.0:
+            ref.bsdf_batch(inp, threads=threads)
+            reps += 1
+        dt = time.time() - t0
+        out["cpu_baseline"] = {"value": reps * m / dt, "unit": "queries/s", "cores": threads, "kind": "reference",
+                               "sample": f"{reps} x 2^16 queries: the reference's BSDF classes (materials.cu) "
+                                         f"built for the host, OpenMP"}
+    return out
+
+
+def terrain_workloads():
+    """Path tracing and LVC-BPT on the 2,097,152-triangle terrain with 4096
+    instanced icospheres under the 2048x1024 sky (FP64 CDF), 1920x1080,
+    max depth 12; device-timed segments/s after warm-up."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    W, H = 1920, 1080
+    desc = scenes.terrain_scene_desc(W, H)
+    out = {}
+    for name, renderer, spp in (("terrain_pt", V.RENDERER_PATH_TRACING, 8), ("terrain_lvc_bpt", V.RENDERER_BPT, 4)):
+        ctx = V.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = scenes.build_instanced(ctx, desc)
+        ctx.setScene(scene)
+        ctx.setRenderer(renderer)
+        ctx.setOptions(max_path_length=12, max_paths_in_flight=1 << 22)
+        ctx.render_samples(cam, True, 2)
+        torch.cuda.synchronize()
+        s0 = ctx.stats()["pathSegments"]
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.render_samples(cam, False, spp, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        seg = ctx.stats()["pathSegments"] - s0
+        st = ctx.stats()
+        out[name] = {"workload": f"{'path tracing' if renderer == V.RENDERER_PATH_TRACING else 'LVC-BPT'} "
+                                 f"{W}x{H}, {spp} spp, max depth 12, sky with sun (FP64 CDF)",
+                     "triangles": st["numTriangles"], "segments_per_s": seg / (ms * 1e-3) / 1e9,
+                     "unit": "G path segments/s", "ms": ms}
+        if renderer == V.RENDERER_BPT:
+            out[name]["light_vertex_overflow"] = st["lightVertexOverflow"]
+        ctx.close()
+    return out
+
+
 # Algorithmic bytes per unit of work of each wavefront stage (SoA path state,
 # counted once per read or write; BVH traffic excluded):
 #   trace: queue index 4 + ray 32 + hit 16 + bucket append 4          = 56 B / ray
@@ -283,6 +376,7 @@ def main():
     ap.add_argument("--impl", default="vlr_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-1%%-error measurement")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the BSDF-batch and terrain workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -406,6 +500,15 @@ def main():
         except Exception:
             pass
 
+    workloads = None
+    if rank == 0 and world == 1 and not args.no_workloads:
+        workloads = {}
+        for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads):
+            try:
+                workloads.update(fn())
+            except Exception as ex:  # reported, never fatal for the GPU line
+                workloads.setdefault("errors", []).append(str(ex))
+
     rmse = None
     if rank == 0 and world == 1 and not args.no_rmse:
         try:
@@ -439,6 +542,7 @@ def main():
             "gpu_launches_per_step": launches_per_step,
             "clocks": clocks.summary(),
             "time_to_rmse": rmse,
+            "workloads": workloads,
         }
         print(json.dumps(line))
     ctx.close()

@@ -80,10 +80,24 @@ typedef struct VLRBRenderOptions {
                                      (materials.cu:1448-1513), so MIS double-counts NEE
                                      through exits; 1: pdf consistent with the sampled
                                      density and the value (unbiased MIS) */
+    uint32_t blocksPerSM;         /* grid of the wavefront kernels = SMs x this (0 = 8) */
 } VLRBRenderOptions;
 
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options);
 VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* options);
+
+/* Autotuner: times `samplesPerTrial`-spp renders of the bound scene and camera
+ * over paths in flight {2^20 .. 2^23} x blocks per SM {4, 8, 16, 32}, keeps
+ * the fastest pair in the render options and writes up to maxTrials trials
+ * (paths in flight, blocks per SM, segments/s).  The film holds the last
+ * trial afterwards; the next render with firstFrame clears it. */
+typedef struct VLRBAutotuneTrial {
+    uint32_t maxPathsInFlight;
+    uint32_t blocksPerSM;
+    double segmentsPerSecond;
+} VLRBAutotuneTrial;
+VLRResult vlrbContextAutotune(VLRContext context, CUstream stream, VLRCameraConst camera, uint32_t samplesPerTrial,
+                              VLRBAutotuneTrial* trials, uint32_t maxTrials, uint32_t* numTrials);
 
 typedef struct VLRBRenderStats {
     uint64_t pathSegments;        /* extension rays traced (camera rays included) */
@@ -204,6 +218,29 @@ VLRResult vlrbContextGetLaunchParamBytes(VLRContext context, uint64_t* bytes);
 
 /* Device address of the FP64 film (width * height * 16 doubles). */
 VLRResult vlrbContextGetFilmDevicePointer(VLRContext context, void** devicePtr);
+
+/* ------------------------------------------------------------------------
+ * Batched rendering of many contexts (no counterpart in the reference).
+ * vlrbRenderBatchCreate renders every item once (scene build, buffers,
+ * guiding warm-up), then captures all items' launch sequences, each on its
+ * own stream forked from `stream`, into one CUDA graph.  Every
+ * vlrbRenderBatchLaunch replays it: item i renders samples[i] spp (restarting
+ * its accumulation when firstFrame) and all items run concurrently.  Path
+ * tracing only (plain or guided).  itemMs (may be NULL) receives each item's
+ * device time of the latest launch (waits for it).
+ * ---------------------------------------------------------------------- */
+typedef struct VLRBBatchItem {
+    VLRContext context;
+    VLRCameraConst camera;
+    uint32_t samples;
+    bool firstFrame;
+} VLRBBatchItem;
+typedef struct VLRBRenderBatch_API* VLRBRenderBatch;
+VLRResult vlrbRenderBatchCreate(const VLRBBatchItem* items, uint32_t numItems, CUstream stream,
+                                VLRBRenderBatch* batch);
+VLRResult vlrbRenderBatchLaunch(VLRBRenderBatch batch, CUstream stream);
+VLRResult vlrbRenderBatchItemTimes(VLRBRenderBatch batch, float* itemMs);
+VLRResult vlrbRenderBatchDestroy(VLRBRenderBatch batch);
 
 /* ------------------------------------------------------------------------
  * Learned path-guiding network (no counterpart in the reference, which has

@@ -34,7 +34,7 @@ def _render(W, H, spp, glass="box", light_scale=1.0, guided=False, pretrain=0, p
     if pretrain:
         ctx.render_samples(cam, True, pretrain)
     ctx.render_samples(cam, True, spp)
-    y = _y(ctx.read_film())
+    y = _y(ctx.read_film()) / spp
     gst = ctx.guiding_stats() if guided else None
     ctx.close()
     return y, gst

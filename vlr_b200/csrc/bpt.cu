@@ -824,7 +824,7 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
         throw std::runtime_error("LVC-BPT needs at least one light");
     StageTimer dummy;
     StageTimer &T = timer ? *timer : dummy;
-    const int grid = numSMs * 8;
+    const int grid = numSMs * static_cast<int>(fp.blocksPerSM ? fp.blocksPerSM : 8);
     const size_t pBytes = sizeof(BptArgs);
     BptArgs a{};
     a.S = scene;

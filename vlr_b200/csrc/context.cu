@@ -154,9 +154,9 @@ T* Context::upload(const std::vector<T> &v, cudaStream_t stream) {
 void Context::bindOutput(uint32_t w, uint32_t h) {
     width = w;
     height = h;
-    film.resize(size_t(w) * h * kNumStrata * 8);
+    film.resize(size_t(w) * h * kNumStrata * 8 + 256);
     output.resize(size_t(w) * h * 16);
-    ck(cudaMemset(film.ptr, 0, size_t(w) * h * kNumStrata * 8), "film clear");
+    ck(cudaMemset(film.ptr, 0, film.bytes), "film clear");
     ck(cudaMemset(output.ptr, 0, size_t(w) * h * 16), "output clear");
     if (outArray) { cudaFreeArray(reinterpret_cast<cudaArray_t>(outArray)); outArray = nullptr; }
     pathCapacity = 0;
@@ -638,12 +638,12 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
     if (firstFrame) {
         setupCamera(cam);
         numAccumFrames = 0;
-        filmClear(Film{ film.as<double>(), width, height }, stream);
+        filmClear(filmDesc(), stream);
     }
     const uint32_t pixels = width * height;
     if (numAccumFrames + samples > limitFrames)
         samples = limitFrames > numAccumFrames ? limitFrames - numAccumFrames : 0;
-    Film fl{ film.as<double>(), width, height };
+    Film fl = filmDesc();
     if (samples > 0) {
         uint32_t perLaunch = std::max<uint32_t>(1, std::min<uint32_t>(samples, options.maxPathsInFlight / pixels));
         ensurePathBuffers(pixels * perLaunch);
@@ -656,6 +656,7 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
             fp.sppPerLaunch = k;
             fp.numPaths = pixels * k;
             fp.maxPathLength = options.maxPathLength;
+            fp.blocksPerSM = options.blocksPerSM;
             if (renderer == VLRRenderer_BPT) {
                 // One frame per launch: all paths of a frame share its
                 // wavelength samples.  Light subpaths per frame default to a
@@ -693,7 +694,6 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 gframe.record = guiding.train;
                 gframe.sample = guiding.enabled && (!guiding.train || guideLaunches >= guiding.warmupLaunches);
                 gframe.net = guideNet->net;
-                gframe.stamp = ++guideStamp;
                 gframe.targetSamples = guiding.samplesPerStep;
                 ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer, &gframe);
                 if (gframe.sample) ++guidingStats.guidedLaunches;
@@ -708,10 +708,134 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
         numAccumFrames += samples;
         stats.frames += samples;
     }
-    filmToRGBA(fl, numAccumFrames, output.as<float4>(), stream);
+    if (samples > 0) filmAddFrames(fl, samples, stream);
+    filmToRGBA(fl, output.as<float4>(), stream);
     ++timer.totalLaunches;
     timer.paramBytes += sizeof(Film) + 4 + 40 + sizeof(void*);
     if (numAccumFramesOut) *numAccumFramesOut = numAccumFrames;
+}
+
+std::vector<AutotuneTrial> Context::autotune(cudaStream_t stream, const Camera* cam, uint32_t samplesPerTrial) {
+    if (width == 0 || height == 0) throw std::runtime_error("no output buffer bound");
+    const RenderOptions saved = options;
+    const uint32_t pixels = width * height;
+    std::vector<AutotuneTrial> trials;
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    uint32_t frames = 0;
+    for (uint32_t paths : { 1u << 20, 1u << 21, 1u << 22, 1u << 23 }) {
+        // below one sample per pixel per launch the candidate equals the
+        // smallest one that holds a full frame
+        if (paths < pixels && !trials.empty() && trials.back().maxPathsInFlight >= pixels) continue;
+        for (uint32_t bps : { 4u, 8u, 16u, 32u }) {
+            options.maxPathsInFlight = std::max(paths, pixels);
+            options.blocksPerSM = bps;
+            render(stream, cam, true, 1u << 30, samplesPerTrial, &frames);    // warm-up / allocation
+            unsigned long long t0[2], t1[2];
+            ck(cudaStreamSynchronize(stream), "sync");
+            ck(cudaMemcpy(t0, pb.totals, 16, cudaMemcpyDeviceToHost), "totals");
+            ck(cudaEventRecord(e0, stream), "record");
+            render(stream, cam, false, 1u << 30, samplesPerTrial, &frames);
+            ck(cudaEventRecord(e1, stream), "record");
+            ck(cudaEventSynchronize(e1), "sync");
+            ck(cudaMemcpy(t1, pb.totals, 16, cudaMemcpyDeviceToHost), "totals");
+            float ms = 0.0f;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+            trials.push_back({ options.maxPathsInFlight, bps, double(t1[0] - t0[0]) / (ms * 1e-3) });
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    options = saved;
+    const AutotuneTrial* best = &trials[0];
+    for (const auto &t : trials)
+        if (t.segmentsPerSecond > best->segmentsPerSecond) best = &t;
+    options.maxPathsInFlight = best->maxPathsInFlight;
+    options.blocksPerSM = best->blocksPerSM;
+    return trials;
+}
+
+RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : items(std::move(its)) {
+    for (const BatchItem &it : items) {
+        if (!it.ctx || !it.cam || it.samples == 0) throw std::runtime_error("batch item without context, camera or samples");
+        if (it.ctx->renderer != VLRRenderer_PathTracing) throw std::runtime_error("batch rendering is path tracing only");
+    }
+    const size_t n = items.size();
+    streams.resize(n);
+    evBegin.resize(n);
+    evEnd.resize(n);
+    evJoin.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        ck(cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking), "batch stream");
+        ck(cudaEventCreate(&evBegin[i]), "event");
+        ck(cudaEventCreate(&evEnd[i]), "event");
+        ck(cudaEventCreateWithFlags(&evJoin[i], cudaEventDisableTiming), "event");
+    }
+    ck(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+    // One plain render per item outside capture: builds scenes, allocates
+    // path and guiding buffers, and gets guided contexts past their warm-up.
+    for (BatchItem &it : items) {
+        const bool profiling = it.ctx->timer.enabled;
+        it.ctx->timer.enabled = false;
+        uint32_t frames;
+        const uint32_t warm = it.ctx->guiding.train ? std::max(it.samples, it.ctx->guiding.warmupLaunches) : it.samples;
+        it.ctx->render(stream, it.cam, true, 1u << 30, warm, &frames);
+        it.ctx->timer.enabled = profiling;
+    }
+    ck(cudaStreamSynchronize(stream), "batch warm-up");
+    ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        ck(cudaEventRecord(fork, stream), "fork");
+        for (size_t i = 0; i < n; ++i) {
+            BatchItem &it = items[i];
+            ck(cudaStreamWaitEvent(streams[i], fork, 0), "wait fork");
+            ck(cudaEventRecord(evBegin[i], streams[i]), "begin");
+            const bool profiling = it.ctx->timer.enabled;
+            it.ctx->timer.enabled = false;
+            uint32_t frames;
+            it.ctx->render(streams[i], it.cam, it.firstFrame, 1u << 30, it.samples, &frames);
+            it.ctx->timer.enabled = profiling;
+            ck(cudaEventRecord(evEnd[i], streams[i]), "end");
+            ck(cudaEventRecord(evJoin[i], streams[i]), "join");
+            ck(cudaStreamWaitEvent(stream, evJoin[i], 0), "wait join");
+        }
+    }
+    catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    ck(cudaStreamEndCapture(stream, &graph), "end capture");
+    ck(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+}
+
+RenderBatch::~RenderBatch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto s : streams) cudaStreamDestroy(s);
+    for (auto e : evBegin) cudaEventDestroy(e);
+    for (auto e : evEnd) cudaEventDestroy(e);
+    for (auto e : evJoin) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+}
+
+void RenderBatch::launch(cudaStream_t stream) {
+    ck(cudaGraphLaunch(exec, stream), "graph launch");
+    // host-side bookkeeping the replayed graph cannot do
+    for (BatchItem &it : items) {
+        it.ctx->numAccumFrames = it.firstFrame ? it.samples : it.ctx->numAccumFrames + it.samples;
+        it.ctx->stats.frames += it.samples;
+    }
+}
+
+void RenderBatch::itemTimes(std::vector<float>* ms) const {
+    ms->resize(items.size());
+    for (size_t i = 0; i < items.size(); ++i) {
+        ck(cudaEventSynchronize(evEnd[i]), "sync");
+        ck(cudaEventElapsedTime(&(*ms)[i], evBegin[i], evEnd[i]), "elapsed");
+    }
 }
 
 void Context::readStats(RenderStats* out) {

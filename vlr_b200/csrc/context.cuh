@@ -34,6 +34,12 @@ struct RenderOptions {
     uint32_t lightPathsPerFrame = 0;  // 0: width * height
     uint64_t rngSeed = 0;             // 0: 591842031321323413 (context.cpp:1176-1190)
     bool consistentDielectricPdf = false;   // see mfBsdfPDF; false = the reference's pdf
+    uint32_t blocksPerSM = 8;         // wavefront kernel grid = SMs x blocksPerSM
+};
+
+struct AutotuneTrial {
+    uint32_t maxPathsInFlight, blocksPerSM;
+    double segmentsPerSecond;
 };
 
 // Learned guiding of the path tracer (vlrbContextSetGuiding).
@@ -77,12 +83,20 @@ public:
     void markDirty() { ++generation; }
     void render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
                 uint32_t samples, uint32_t* numAccumFrames);
+    // Times short renders over a grid of (paths in flight, blocks per SM),
+    // keeps the fastest in `options`, and returns every trial.  Leaves the
+    // film holding the last trial (the next firstFrame render clears it).
+    std::vector<AutotuneTrial> autotune(cudaStream_t stream, const Camera* cam, uint32_t samplesPerTrial);
     void readOutput(float* host);
     void readFilm(double* host);
     void readStats(RenderStats* out);
     CUarray outputArray();
     void* outputDevicePtr() const { return output.ptr; }
     void* filmDevicePtr() const { return film.ptr; }
+    Film filmDesc() const {
+        return Film{ film.as<double>(), width, height,
+                     reinterpret_cast<uint32_t*>(static_cast<char*>(film.ptr) + size_t(width) * height * kNumStrata * 8) };
+    }
     uint32_t numTriangles() const { return sg.numTris; }
     uint32_t guideSamplesRecorded() const;
 
@@ -113,7 +127,6 @@ private:
     DeviceBuffer guideMem;
     GuideFrame gframe{};
     uint32_t guideCapacityPaths = 0, guideLaunches = 0, guideRecBounces = 0, guideSampleCapacity = 0;
-    uint32_t guideStamp = 0;
 
     SceneGPU sg{};
     std::vector<std::unique_ptr<DeviceBuffer>> sceneBufs;
@@ -130,6 +143,38 @@ private:
     uint32_t* hostCounters = nullptr;
     std::vector<float> envPixelsCache;
     template <typename T> T* upload(const std::vector<T> &v, cudaStream_t stream);
+};
+
+// Many contexts rendered together: each item's launch sequence runs on its
+// own stream forked from the caller's, and the whole batch is captured once
+// into one CUDA graph that every launch replays.  Per-item device times come
+// from event nodes around each branch.  Path tracing only (plain or guided):
+// LVC-BPT draws its per-frame wavelengths on the host, which a replayed graph
+// would freeze.
+struct BatchItem {
+    Context* ctx;
+    const Camera* cam;
+    uint32_t samples;
+    bool firstFrame;
+};
+
+class RenderBatch {
+public:
+    RenderBatch(std::vector<BatchItem> items, cudaStream_t stream);
+    ~RenderBatch();
+    RenderBatch(const RenderBatch &) = delete;
+    RenderBatch &operator=(const RenderBatch &) = delete;
+    void launch(cudaStream_t stream);
+    // device milliseconds of each item in the latest launch
+    void itemTimes(std::vector<float>* ms) const;
+
+    std::vector<BatchItem> items;
+private:
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> evBegin, evEnd, evJoin;
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
 };
 
 } // namespace api

@@ -148,7 +148,7 @@ __device__ __forceinline__ void completeRecord(const GuideFrame &gf, uint32_t P,
     if (!(flags & kFlagRecordPending) || bounce == 0) return;
     const uint32_t b = bounce - 1;
     recField(gf, P, b, 5)[p] = toF4(contrib);
-    gf.recStamp[static_cast<size_t>(b) * P + p] = gf.stamp;
+    gf.recStamp[static_cast<size_t>(b) * P + p] = gf.counts[kCountStamp];
 }
 
 __device__ __forceinline__ void loadMixture(const GuideFrame &gf, uint32_t P, uint32_t p, guide::Mixture &m) {
@@ -463,11 +463,12 @@ __device__ __forceinline__ uint32_t mixBits(uint32_t a, uint32_t b, uint32_t c) 
 __global__ void __launch_bounds__(256) guideFinalizeKernel(PathBuffers pb, FrameParams fp, GuideFrame gf) {
     const uint32_t P = fp.numPaths;
     const uint32_t last = gf.counts[2];
+    const uint32_t stamp = gf.counts[kCountStamp];
     const float accept = last > gf.targetSamples ? static_cast<float>(gf.targetSamples) / last : 1.0f;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
         const float4 cEnd = pb.contrib[p];
         for (uint32_t b = 0; b < gf.recBounces; ++b) {
-            if (gf.recStamp[static_cast<size_t>(b) * P + p] != gf.stamp) continue;
+            if (gf.recStamp[static_cast<size_t>(b) * P + p] != stamp) continue;
             const float4 beta = recField(gf, P, b, 4)[p];
             const float4 snap = recField(gf, P, b, 5)[p];
             const float bt[4] = { beta.x, beta.y, beta.z, beta.w };
@@ -478,7 +479,7 @@ __global__ void __launch_bounds__(256) guideFinalizeKernel(PathBuffers pb, Frame
             w *= 0.25f;
             if (!(w > 0.0f) || !isfinite(w)) continue;
             atomicAdd(gf.counts + 1, 1u);
-            const float u = (mixBits(p, b, gf.stamp) >> 8) * (1.0f / 16777216.0f);
+            const float u = (mixBits(p, b, stamp) >> 8) * (1.0f / 16777216.0f);
             if (u >= accept) continue;
             const uint32_t slot = atomicAdd(gf.counts, 1u);
             if (slot >= gf.sampleCapacity) continue;
@@ -493,11 +494,13 @@ __global__ void __launch_bounds__(256) guideFinalizeKernel(PathBuffers pb, Frame
     }
 }
 
-// Start of a recording launch: accepted = 0, last = this, this = 0.
+// Start of a recording launch: accepted = 0, last = this, this = 0, next
+// stamp.  All on the device, so a captured launch sequence replays correctly.
 __global__ void guideCountsKernel(uint32_t* counts) {
     counts[2] = counts[1] > 0 ? counts[1] : counts[2];
     counts[1] = 0;
     counts[0] = 0;
+    counts[kCountStamp] += 1;
 }
 
 __global__ void __launch_bounds__(256) filmKernel(PathBuffers pb, Film film, FrameParams fp) {
@@ -525,8 +528,11 @@ struct FilmConst {
     float xyzToRgb[9];
 };
 
-__global__ void filmToRGBAKernel(Film film, uint32_t frames, FilmConst fc, float4* out) {
+__global__ void filmAddFramesKernel(uint32_t* frames, uint32_t samples) { *frames += samples; }
+
+__global__ void filmToRGBAKernel(Film film, FilmConst fc, float4* out) {
     const uint32_t n = film.width * film.height;
+    const uint32_t frames = *film.frames ? *film.frames : 1u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double* s = film.strata + static_cast<size_t>(i) * kNumStrata;
         double X = 0, Y = 0, Z = 0;
@@ -673,7 +679,7 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
     StageTimer dummy;
     StageTimer &T = timer ? *timer : dummy;
     ck(cudaMemsetAsync(pb.counters, 0, size_t(kMaxBounces + 1) * kCountersPerBounce * 4, stream), "counters");
-    const int grid = numSMs * 8;
+    const int grid = numSMs * static_cast<int>(fp.blocksPerSM ? fp.blocksPerSM : 8);
     const size_t pMain = sizeof(SceneGPU) + sizeof(PathBuffers) + sizeof(FrameParams);
     T.begin(kStageCamera, stream, pMain);
     cameraKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
@@ -729,16 +735,22 @@ void launchTraceSorted(const SceneGPU &scene, const PathBuffers &pb, const Frame
 
 void filmClear(const Film &film, cudaStream_t stream) {
     ck(cudaMemsetAsync(film.strata, 0, size_t(film.width) * film.height * kNumStrata * 8, stream), "film clear");
+    ck(cudaMemsetAsync(film.frames, 0, 4, stream), "film frames");
 }
 
-void filmToRGBA(const Film &film, uint32_t frames, float4* out, cudaStream_t stream) {
+void filmAddFrames(const Film &film, uint32_t samples, cudaStream_t stream) {
+    filmAddFramesKernel<<<1, 1, 0, stream>>>(film.frames, samples);
+    ck(cudaGetLastError(), "film frames");
+}
+
+void filmToRGBA(const Film &film, float4* out, cudaStream_t stream) {
     FilmConst fc;
     const CmfStrata &cs = hostCmfStrata();
     for (uint32_t k = 0; k < kNumStrata; ++k) { fc.xbar[k] = cs.xbar[k]; fc.ybar[k] = cs.ybar[k]; fc.zbar[k] = cs.zbar[k]; }
     fc.integralCMF = cs.integralCMF;
     for (int k = 0; k < 9; ++k) fc.xyzToRgb[k] = hostColorMatrices().xyzToRec709D65[k];
     const uint32_t n = film.width * film.height;
-    filmToRGBAKernel<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, stream>>>(film, frames ? frames : 1, fc, out);
+    filmToRGBAKernel<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, stream>>>(film, fc, out);
     ck(cudaGetLastError(), "film convert");
 }
 

@@ -50,12 +50,16 @@ struct FrameParams {
     uint32_t numPaths;        // width * height * sppPerLaunch
     uint32_t maxPathLength;   // hits after which a path stops scattering
     uint32_t bounce;          // current bounce (0-based)
+    uint32_t blocksPerSM;     // grid of the wavefront kernels = SMs x this (0: 8)
 };
 
-// Film: 16 FP64 strata per pixel, [pixel][16].
+// Film: 16 FP64 strata per pixel, [pixel][16], and the device count of
+// samples per pixel it holds (kept on the device so that a captured launch
+// sequence replays with the right normalisation).
 struct Film {
     double* strata;
     uint32_t width, height;
+    uint32_t* frames;
 };
 
 // Learned guiding for one launch.  `sample`: guided kinds (Matte,
@@ -68,6 +72,7 @@ struct Film {
 constexpr uint32_t kMaxRecBounces = 8;
 constexpr uint32_t kRecFields = 6;          // pos, normal, wo, wi, throughput, contribution snapshot
 constexpr uint32_t kFlagRecordPending = 1u << 24;
+constexpr uint32_t kCountStamp = 3;
 
 struct GuideFrame {
     bool sample;
@@ -77,12 +82,12 @@ struct GuideFrame {
     float4* lobes;             // [kLobes][P]  (mu, kappa)
     float4* lobeWeights;       // [2][P]       mixture weights
     float4* rec;               // [recBounces][kRecFields][P]
-    uint32_t* recStamp;        // [recBounces][P] frame stamp once a record is complete
-    uint32_t stamp;
+    uint32_t* recStamp;        // [recBounces][P] launch stamp once a record is complete
     guide::Sample* samples;    // training-sample buffer
     uint32_t sampleCapacity;
     uint32_t targetSamples;    // samples wanted per launch
-    uint32_t* counts;          // [0] accepted, [1] candidates this launch, [2] candidates last launch
+    uint32_t* counts;          // [0] accepted, [1] candidates this launch, [2] candidates last launch,
+                               // [kCountStamp] launch stamp
     uint32_t* err;
 };
 
@@ -141,7 +146,8 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
 void launchTraceSorted(const SceneGPU &scene, const PathBuffers &pb, const FrameParams &fp, int grid,
                        cudaStream_t stream);
 
-void filmToRGBA(const Film &film, uint32_t numAccumFrames, float4* out, cudaStream_t stream);
+void filmToRGBA(const Film &film, float4* out, cudaStream_t stream);
 void filmClear(const Film &film, cudaStream_t stream);
+void filmAddFrames(const Film &film, uint32_t samples, cudaStream_t stream);
 
 } // namespace vlrb

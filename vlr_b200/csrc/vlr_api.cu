@@ -1156,8 +1156,9 @@ VLRResult vlrbContextRenderSamples(VLRContext context, CUstream stream, VLRCamer
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!options || options->maxPathLength == 0 || options->maxPathLength > kMaxBounces ||
-        options->maxPathsInFlight == 0)
+        options->maxPathsInFlight == 0 || options->blocksPerSM > 64)
         return VLRResult_InvalidArgument;
+    c->options.blocksPerSM = options->blocksPerSM ? options->blocksPerSM : 8;
     c->options.maxPathLength = options->maxPathLength;
     c->options.maxPathsInFlight = options->maxPathsInFlight;
     c->options.lightPathsPerFrame = options->lightPathsPerFrame;
@@ -1177,6 +1178,71 @@ VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* opt
     options->lightPathsPerFrame = c->options.lightPathsPerFrame;
     options->rngSeed = c->options.rngSeed;
     options->consistentDielectricPdf = c->options.consistentDielectricPdf ? 1u : 0u;
+    options->blocksPerSM = c->options.blocksPerSM;
+    return VLRResult_NoError;
+}
+
+VLRResult vlrbContextAutotune(VLRContext context, CUstream stream, VLRCameraConst camera, uint32_t samplesPerTrial,
+                              VLRBAutotuneTrial* trials, uint32_t maxTrials, uint32_t* numTrials) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    VLRResult e2 = VLRResult_NoError;
+    const api::Camera* cam = checked<const api::Camera>(camera, &e2, kindCamera);
+    if (!cam || samplesPerTrial == 0 || (maxTrials > 0 && !trials)) return VLRResult_InvalidArgument;
+    API_TRY
+    std::vector<AutotuneTrial> t = c->autotune(reinterpret_cast<cudaStream_t>(stream), cam, samplesPerTrial);
+    for (uint32_t i = 0; i < maxTrials && i < t.size(); ++i)
+        trials[i] = VLRBAutotuneTrial{ t[i].maxPathsInFlight, t[i].blocksPerSM, t[i].segmentsPerSecond };
+    if (numTrials) *numTrials = static_cast<uint32_t>(t.size());
+    return VLRResult_NoError;
+    API_CATCH("vlrbContextAutotune")
+}
+
+struct VLRBRenderBatch_API {
+    std::unique_ptr<api::RenderBatch> impl;
+};
+
+VLRResult vlrbRenderBatchCreate(const VLRBBatchItem* items, uint32_t numItems, CUstream stream,
+                                VLRBRenderBatch* batch) {
+    if (!items || numItems == 0 || !batch) return VLRResult_InvalidArgument;
+    std::vector<api::BatchItem> its;
+    for (uint32_t i = 0; i < numItems; ++i) {
+        CHECK_HANDLE(c, Context, kindContext, items[i].context);
+        VLRResult e2 = VLRResult_NoError;
+        const api::Camera* cam = checked<const api::Camera>(items[i].camera, &e2, kindCamera);
+        if (!cam || items[i].samples == 0) return VLRResult_InvalidArgument;
+        if (c->renderer != VLRRenderer_PathTracing) return VLRResult_InvalidArgument;
+        its.push_back(api::BatchItem{ c, cam, items[i].samples, items[i].firstFrame });
+    }
+    API_TRY
+    auto* b = new VLRBRenderBatch_API;
+    b->impl.reset(new api::RenderBatch(std::move(its), reinterpret_cast<cudaStream_t>(stream)));
+    *batch = b;
+    return VLRResult_NoError;
+    API_CATCH("vlrbRenderBatchCreate")
+}
+
+VLRResult vlrbRenderBatchLaunch(VLRBRenderBatch batch, CUstream stream) {
+    if (!batch) return VLRResult_InvalidInstance;
+    API_TRY
+    batch->impl->launch(reinterpret_cast<cudaStream_t>(stream));
+    return VLRResult_NoError;
+    API_CATCH("vlrbRenderBatchLaunch")
+}
+
+VLRResult vlrbRenderBatchItemTimes(VLRBRenderBatch batch, float* itemMs) {
+    if (!batch) return VLRResult_InvalidInstance;
+    if (!itemMs) return VLRResult_InvalidArgument;
+    API_TRY
+    std::vector<float> ms;
+    batch->impl->itemTimes(&ms);
+    for (size_t i = 0; i < ms.size(); ++i) itemMs[i] = ms[i];
+    return VLRResult_NoError;
+    API_CATCH("vlrbRenderBatchItemTimes")
+}
+
+VLRResult vlrbRenderBatchDestroy(VLRBRenderBatch batch) {
+    if (!batch) return VLRResult_InvalidInstance;
+    delete batch;
     return VLRResult_NoError;
 }
 

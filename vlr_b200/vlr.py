@@ -32,7 +32,12 @@ class VLRShaderNodePlug(ctypes.Structure):
 class VLRBRenderOptions(ctypes.Structure):
     _fields_ = [("maxPathLength", ctypes.c_uint32), ("maxPathsInFlight", ctypes.c_uint32),
                 ("lightPathsPerFrame", ctypes.c_uint32), ("rngSeed", ctypes.c_uint64),
-                ("consistentDielectricPdf", ctypes.c_uint32)]
+                ("consistentDielectricPdf", ctypes.c_uint32), ("blocksPerSM", ctypes.c_uint32)]
+
+
+class VLRBAutotuneTrial(ctypes.Structure):
+    _fields_ = [("maxPathsInFlight", ctypes.c_uint32), ("blocksPerSM", ctypes.c_uint32),
+                ("segmentsPerSecond", ctypes.c_double)]
 
 
 class VLRBRenderStats(ctypes.Structure):
@@ -50,6 +55,11 @@ class VLRBGuidingOptions(ctypes.Structure):
 class VLRBGuidingStats(ctypes.Structure):
     _fields_ = [("lastLoss", ctypes.c_float), ("trainingSteps", ctypes.c_uint64),
                 ("guidedLaunches", ctypes.c_uint64), ("lastSamples", ctypes.c_uint32)]
+
+
+class VLRBBatchItem(ctypes.Structure):
+    _fields_ = [("context", ctypes.c_void_p), ("camera", ctypes.c_void_p), ("samples", ctypes.c_uint32),
+                ("firstFrame", ctypes.c_bool)]
 
 
 RENDERER_PATH_TRACING = 0
@@ -103,6 +113,12 @@ def _api():
         "vlrbContextGetRenderOptions": [v, ctypes.POINTER(VLRBRenderOptions)],
         "vlrbContextGetStats": [v, ctypes.POINTER(VLRBRenderStats)],
         "vlrbContextSetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
+        "vlrbRenderBatchCreate": [ctypes.POINTER(VLRBBatchItem), ctypes.c_uint32, v, ctypes.POINTER(c_void_p)],
+        "vlrbRenderBatchLaunch": [v, v],
+        "vlrbRenderBatchItemTimes": [v, ctypes.POINTER(ctypes.c_float)],
+        "vlrbRenderBatchDestroy": [v],
+        "vlrbContextAutotune": [v, v, v, ctypes.c_uint32, ctypes.POINTER(VLRBAutotuneTrial), ctypes.c_uint32,
+                                ctypes.POINTER(ctypes.c_uint32)],
         "vlrbContextGetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
         "vlrbContextGetGuidingStats": [v, ctypes.POINTER(VLRBGuidingStats)],
         "vlrbContextReadFilm": [v, v],
@@ -304,7 +320,7 @@ class Context:
         check(_api().vlrContextSetRenderer(self.h, renderer), "setRenderer")
 
     def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None, rng_seed=None,
-                   consistent_dielectric_pdf=None):
+                   consistent_dielectric_pdf=None, blocks_per_sm=None):
         o = VLRBRenderOptions()
         check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
         if max_path_length is not None:
@@ -317,7 +333,23 @@ class Context:
             o.rngSeed = rng_seed
         if consistent_dielectric_pdf is not None:
             o.consistentDielectricPdf = int(bool(consistent_dielectric_pdf))
+        if blocks_per_sm is not None:
+            o.blocksPerSM = blocks_per_sm
         check(_api().vlrbContextSetRenderOptions(self.h, ctypes.byref(o)), "setOptions")
+
+    def autotune(self, camera, samples_per_trial=4, stream=0):
+        """vlrbContextAutotune: returns the trials; the fastest configuration
+        is kept in the render options."""
+        trials = (VLRBAutotuneTrial * 32)()
+        n = ctypes.c_uint32()
+        check(_api().vlrbContextAutotune(self.h, c_void_p(stream), camera.h, samples_per_trial, trials, 32,
+                                         ctypes.byref(n)), "vlrbContextAutotune")
+        return [(t.maxPathsInFlight, t.blocksPerSM, t.segmentsPerSecond) for t in trials[:n.value]]
+
+    def options(self):
+        o = VLRBRenderOptions()
+        check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
+        return {k: getattr(o, k) for k, _ in VLRBRenderOptions._fields_}
 
     def setGuiding(self, enabled=None, train=None, **kw):
         """vlrbContextSetGuiding; keyword names are the C struct's fields
@@ -399,8 +431,41 @@ class Context:
         return {k: getattr(s, k) for k, _ in VLRBRenderStats._fields_}
 
 
+class RenderBatch:
+    """vlrbRenderBatch*: items = [(context, camera, samples, first_frame)]."""
+
+    def __init__(self, items, stream=0):
+        self.n = len(items)
+        arr = (VLRBBatchItem * self.n)()
+        for i, (ctx, cam, spp, first) in enumerate(items):
+            arr[i] = VLRBBatchItem(ctx.h.value if hasattr(ctx.h, "value") else ctx.h, cam.h.value
+                                   if hasattr(cam.h, "value") else cam.h, spp, first)
+        self.h = c_void_p()
+        check(_api().vlrbRenderBatchCreate(arr, self.n, c_void_p(stream), ctypes.byref(self.h)), "batchCreate")
+
+    def launch(self, stream=0):
+        check(_api().vlrbRenderBatchLaunch(self.h, c_void_p(stream)), "batchLaunch")
+
+    def item_times(self):
+        ms = (ctypes.c_float * self.n)()
+        check(_api().vlrbRenderBatchItemTimes(self.h, ms), "batchItemTimes")
+        return list(ms)
+
+    def close(self):
+        if self.h:
+            _api().vlrbRenderBatchDestroy(self.h)
+            self.h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def quat_rotate_y(angle):
     return (0.0, math.sin(angle / 2), 0.0, math.cos(angle / 2))
 
 
-__all__ = ["Context", "rgb", "Spectrum", "VLRError", "quat_rotate_y", "RENDERER_PATH_TRACING", "RENDERER_BPT"]
+__all__ = ["Context", "RenderBatch", "rgb", "Spectrum", "VLRError", "quat_rotate_y", "RENDERER_PATH_TRACING",
+           "RENDERER_BPT"]
