@@ -125,7 +125,7 @@ typedef struct VLRBGuidingOptions {
     float learningRate;           /* default 1e-2 */
     uint32_t samplesPerStep;      /* default 2^18 */
     uint32_t stepsPerLaunch;      /* default 1 */
-    uint32_t recordBounces;       /* 1..8, default 4 */
+    uint32_t recordBounces;       /* bounces that are guided and recorded, 1..8, default 4 */
     uint32_t warmupLaunches;      /* default 4 */
 } VLRBGuidingOptions;
 

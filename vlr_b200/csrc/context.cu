@@ -784,30 +784,34 @@ RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : item
         it.ctx->timer.enabled = profiling;
     }
     ck(cudaStreamSynchronize(stream), "batch warm-up");
-    ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    // Captured on a stream of its own: the caller's may be the legacy default
+    // stream, which cannot be captured.  Launches go to the caller's stream.
+    ck(cudaStreamCreateWithFlags(&captureStream, cudaStreamNonBlocking), "capture stream");
+    ck(cudaStreamBeginCapture(captureStream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-        ck(cudaEventRecord(fork, stream), "fork");
+        ck(cudaEventRecord(fork, captureStream), "fork");
         for (size_t i = 0; i < n; ++i) {
             BatchItem &it = items[i];
             ck(cudaStreamWaitEvent(streams[i], fork, 0), "wait fork");
-            ck(cudaEventRecord(evBegin[i], streams[i]), "begin");
+            ck(cudaEventRecordWithFlags(evBegin[i], streams[i], cudaEventRecordExternal), "begin");
             const bool profiling = it.ctx->timer.enabled;
             it.ctx->timer.enabled = false;
             uint32_t frames;
             it.ctx->render(streams[i], it.cam, it.firstFrame, 1u << 30, it.samples, &frames);
             it.ctx->timer.enabled = profiling;
-            ck(cudaEventRecord(evEnd[i], streams[i]), "end");
+            ck(cudaEventRecordWithFlags(evEnd[i], streams[i], cudaEventRecordExternal), "end");
             ck(cudaEventRecord(evJoin[i], streams[i]), "join");
-            ck(cudaStreamWaitEvent(stream, evJoin[i], 0), "wait join");
+            ck(cudaStreamWaitEvent(captureStream, evJoin[i], 0), "wait join");
         }
     }
     catch (...) {
         cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(stream, &g);
+        cudaStreamEndCapture(captureStream, &g);
         if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
         throw;
     }
-    ck(cudaStreamEndCapture(stream, &graph), "end capture");
+    ck(cudaStreamEndCapture(captureStream, &graph), "end capture");
     ck(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
 }
 
@@ -819,6 +823,7 @@ RenderBatch::~RenderBatch() {
     for (auto e : evEnd) cudaEventDestroy(e);
     for (auto e : evJoin) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
+    if (captureStream) cudaStreamDestroy(captureStream);
 }
 
 void RenderBatch::launch(cudaStream_t stream) {

@@ -173,6 +173,7 @@ private:
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> evBegin, evEnd, evJoin;
     cudaEvent_t fork = nullptr;
+    cudaStream_t captureStream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };

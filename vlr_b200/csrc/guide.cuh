@@ -77,9 +77,13 @@ struct Sample {
 };
 
 // Per-query mixture: lobe k = (mu_k, kappa_k), mixture weight pi_k.
+// Per-query mixture: lobe k = (mu_k, kappa_k), mixture weight pi_k, and
+// scale_k = pi_k * kappa_k / (2 pi (1 - exp(-2 kappa_k))) so that
+// q(w) = sum_k scale_k exp(kappa_k (mu_k . w - 1)) costs one exp per lobe.
 struct Mixture {
     float4 lobe[kLobes];
     float weight[kLobes];
+    float scale[kLobes];
 };
 
 // ------------------------------------------------------------ encoding
@@ -154,7 +158,7 @@ __device__ __forceinline__ float mixturePdf(const Mixture &m, const V3 &w) {
     for (int k = 0; k < kLobes; ++k) {
         const float4 l = m.lobe[k];
         const float cosT = l.x * w.x + l.y * w.y + l.z * w.z;
-        q += m.weight[k] * expf(vmfLogNorm(l.w) + l.w * (cosT - 1.0f));
+        q += m.scale[k] * expf(l.w * (cosT - 1.0f));
     }
     return q;
 }
@@ -202,7 +206,10 @@ __device__ __forceinline__ void decodeMixture(const float raw[kRaw], Mixture &m)
     }
     const float inv = 1.0f / sum;
 #pragma unroll
-    for (int k = 0; k < kLobes; ++k) m.weight[k] *= inv;
+    for (int k = 0; k < kLobes; ++k) {
+        m.weight[k] *= inv;
+        m.scale[k] = m.weight[k] * expf(vmfLogNorm(m.lobe[k].w));
+    }
 }
 
 } // namespace guide

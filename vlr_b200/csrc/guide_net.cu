@@ -169,7 +169,7 @@ void GuideNet::inferArrays(const float* pos, const float* wo, const float* nrm, 
     ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmemBytes), "smem attr");
     const uint32_t tiles = (n + kRows - 1) / kRows;
     const uint32_t grid = tiles < uint32_t(numSMs) * 3 ? tiles : uint32_t(numSMs) * 3;
-    kern<<<grid, kRows, kInferSmemBytes, stream>>>(net, src, dst, err);
+    kern<<<grid, kInferThreads, kInferSmemBytes, stream>>>(net, src, dst, err);
     ck(cudaGetLastError(), "infer launch");
 }
 
@@ -182,7 +182,7 @@ void GuideNet::gradients(const Sample* samples, uint32_t n, cudaStream_t stream,
     const uint32_t tiles = (n + kRows - 1) / kRows;
     const uint32_t grid = tiles < uint32_t(numSMs) ? tiles : uint32_t(numSMs);
     TrainArgs a{ samples, n, countDev, scalars, dwSlabs, scalars + 1, err };
-    guideTrainKernel<<<grid, kRows, kTrainSmemBytes, stream>>>(net, a);
+    guideTrainKernel<<<grid, kTrainThreads, kTrainSmemBytes, stream>>>(net, a);
     reduceDwKernel<<<(kDwSlabFloats + 255) / 256, 256, 0, stream>>>(dwSlabs, grid, net.wGrad);
     ck(cudaGetLastError(), "train launch");
 }

@@ -3,7 +3,7 @@
 // gradients accumulated in TMEM across the CTA's tiles, hash-grid gradients
 // scattered with atomics.
 //
-// Per 128-sample tile (thread t = sample row t = TMEM lane t):
+// Per 128-sample tile (sample row t = TMEM lane t):
 //   forward   X -> A1 -> A2 -> A3 -> Y as in inference, keeping X and the
 //             three hidden activation tiles in shared memory;
 //   output    dY = d loss / d raw outputs per row (FP32 in registers, stored
@@ -23,10 +23,6 @@
 
 namespace vlrb {
 namespace guide {
-
-// TMEM lane holding row r (0..63) of an M = 64 accumulator: rows 16 q .. 16 q
-// + 15 sit in lanes 32 q .. 32 q + 15 of the four 32-lane sub-partitions.
-__device__ __forceinline__ uint32_t m64Lane(uint32_t r) { return (r >> 4) * 32u + (r & 15u); }
 
 constexpr uint32_t kTrainSmemBytes = kWeightTileBytes + 6 * kActTileBytes + 64;
 constexpr uint32_t kTrainTmemCols = 512;
@@ -92,7 +88,29 @@ __device__ __forceinline__ float mixtureLossGrad(const float raw[kOut], const V3
     return -w * logQ;
 }
 
-__global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) {
+// Row r of a chunk-major tile: `nchunks` 8-column chunks starting at c0.
+__device__ __forceinline__ void loadChunks(const uint8_t* tile, uint32_t R, uint32_t r, float* v, int c0,
+                                           int nchunks) {
+#pragma unroll
+    for (int c = 0; c < nchunks; ++c) {
+        uint4 q = *reinterpret_cast<const uint4*>(tile + (c0 + c) * R * 16u + r * 16u);
+        const uint32_t w[4] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[i]));
+            v[8 * c + 2 * i] = f.x;
+            v[8 * c + 2 * i + 1] = f.y;
+        }
+    }
+}
+
+// 256 threads per 128-row tile, as in inference: thread t works on row
+// t mod 128 and half h = t / 128.  Each half encodes 8 grid levels and one SH
+// block, handles 32 of the 64 columns after every product, and scatters the
+// hash-grid gradient of its 8 levels; half 0 computes the loss gradient.
+constexpr uint32_t kTrainThreads = 2 * kRows;
+
+__global__ void __launch_bounds__(kTrainThreads, 1) guideTrainKernel(Net net, TrainArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sW = smem;
     uint8_t* sX = smem + kWeightTileBytes;
@@ -102,6 +120,7 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
     uint64_t* mbar = reinterpret_cast<uint64_t*>(sX + 6 * kActTileBytes);
     uint32_t* slot = reinterpret_cast<uint32_t*>(mbar + 1);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t r = tid & (kRows - 1), half = tid / kRows, lane0 = 32 * (warp & 3);
 
     loadWeightTiles(net, sW);
     if (warp == 0) umma::tmemAlloc(slot, kTrainTmemCols);
@@ -121,7 +140,7 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
     uint32_t tilesDone = 0;
     float lossAcc = 0.0f;
 
-    // Issue (thread 0), commit, bounded wait by all; false on timeout.
+    // Bounded wait by all threads for the latest commit; false on timeout.
     auto sync = [&]() -> bool {
         const bool done = umma::mbarWait(mbar, phase);
         phase ^= 1u;
@@ -140,22 +159,29 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
 
     const uint32_t count = a.countDev ? min(*a.countDev, a.count) : a.count;
     for (uint32_t tile = blockIdx.x; ok && tile * kRows < count; tile += gridDim.x) {
-        const uint32_t row = tile * kRows + tid;
+        const uint32_t row = tile * kRows + r;
         const bool valid = row < count;
         Sample s;
         if (valid) s = a.samples[row];
         else s = Sample{ make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 1.f, 0.f),
                          make_float4(0.f, 0.f, 1.f, 0.f), make_float4(0.f, 0.f, 1.f, 0.f) };
         const float3 p = normalisedPosition(net, s.posWeight.x, s.posWeight.y, s.posWeight.z);
-        const V3 wo(s.wo.x, s.wo.y, s.wo.z), nrm(s.nrm.x, s.nrm.y, s.nrm.z), wi(s.wi.x, s.wi.y, s.wi.z);
+        const V3 wi(s.wi.x, s.wi.y, s.wi.z);
         {
-            float f[kIn];
-            if (valid) encode(net, p, wo, nrm, f);
+            float f[16];
+            if (valid) encodeLevels(net, p, 8 * half, f);
             else {
 #pragma unroll
-                for (int i = 0; i < kIn; ++i) f[i] = 0.0f;
+                for (int i = 0; i < 16; ++i) f[i] = 0.0f;
             }
-            storeRow(sX, kRows, tid, f, kIn);
+            storeChunks(sX, kRows, r, f, 2 * half, 2);
+            const float4 d = half ? s.nrm : s.wo;
+            sphericalHarmonics(d.x, d.y, d.z, f);
+            if (!valid) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) f[i] = 0.0f;
+            }
+            storeChunks(sX, kRows, r, f, 4 + 2 * half, 2);
         }
         // ---- forward
         uint32_t in = xAddr;
@@ -169,21 +195,21 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
             }
             if (!(ok = sync())) break;
             if (l < kNumLayers - 1) {
-                float h[kHidden];
+                float h[32];
+                umma::tmemLoad16(umma::tmemAt(tmem, lane0, 32 * half), h);
+                umma::tmemLoad16(umma::tmemAt(tmem, lane0, 32 * half + 16), h + 16);
 #pragma unroll
-                for (int c = 0; c < kHidden; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, 32 * warp, c), h + c);
-#pragma unroll
-                for (int i = 0; i < kHidden; ++i) h[i] = fmaxf(h[i], 0.0f);
-                storeRow(sA[l], kRows, tid, h, kHidden);
+                for (int i = 0; i < 32; ++i) h[i] = fmaxf(h[i], 0.0f);
+                storeChunks(sA[l], kRows, r, h, 4 * half, 4);
                 in = aAddr[l];
             }
         }
         if (!ok) break;
-        // ---- loss gradient at the outputs
-        {
+        // ---- loss gradient at the outputs (half 0)
+        if (half == 0) {
             float y[kOut], dy[kHidden];
 #pragma unroll
-            for (int c = 0; c < kOut; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, 32 * warp, c), y + c);
+            for (int c = 0; c < kOut; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, lane0, c), y + c);
             const float w = valid ? s.posWeight.w * invWeightSum : 0.0f;
             if (w > 0.0f) lossAcc += mixtureLossGrad(y, wi, w, dy);
             else {
@@ -192,7 +218,7 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
             }
 #pragma unroll
             for (int i = kOut; i < kHidden; ++i) dy[i] = 0.0f;
-            storeRow(sDY, kRows, tid, dy, kHidden);
+            storeRow(sDY, kRows, r, dy, kHidden);
         }
         // ---- backward, layer 3 .. 0
         const bool accumulate = tilesDone > 0;
@@ -213,23 +239,23 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
             }
             if (!(ok = sync())) break;
             if (l > 0) {
-                float g[kHidden], act[kHidden];
+                float g[32], act[32];
+                umma::tmemLoad16(umma::tmemAt(tmem, lane0, 32 * half), g);
+                umma::tmemLoad16(umma::tmemAt(tmem, lane0, 32 * half + 16), g + 16);
+                loadChunks(sA[l - 1], kRows, r, act, 4 * half, 4);
 #pragma unroll
-                for (int c = 0; c < kHidden; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, 32 * warp, c), g + c);
-                loadRow(sA[l - 1], kRows, tid, act, kHidden);
-#pragma unroll
-                for (int i = 0; i < kHidden; ++i) g[i] = act[i] > 0.0f ? g[i] : 0.0f;
-                storeRow(sDZ, kRows, tid, g, kHidden);
+                for (int i = 0; i < 32; ++i) g[i] = act[i] > 0.0f ? g[i] : 0.0f;
+                storeChunks(sDZ, kRows, r, g, 4 * half, 4);
                 dzTile = dzAddr;
             }
             else {
-                float g[kGridFeatures];
-#pragma unroll
-                for (int c = 0; c < kGridFeatures; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, 32 * warp, c), g + c);
+                float g[16];
+                umma::tmemLoad16(umma::tmemAt(tmem, lane0, 16 * half), g);
                 if (valid) {
 #pragma unroll 1
-                    for (int lv = 0; lv < kLevels; ++lv) {
-                        const float g0 = g[2 * lv], g1 = g[2 * lv + 1];
+                    for (int j = 0; j < 8; ++j) {
+                        const int lv = 8 * half + j;
+                        const float g0 = g[2 * j], g1 = g[2 * j + 1];
                         if (g0 == 0.0f && g1 == 0.0f) continue;
                         float* table = net.gridGrad + (static_cast<size_t>(lv) << net.log2Table) * kFeatPerLevel;
                         forEachCorner(net, lv, p.x, p.y, p.z, [&](uint32_t idx, float cw) {
@@ -243,35 +269,34 @@ __global__ void __launch_bounds__(kRows) guideTrainKernel(Net net, TrainArgs a) 
         if (!ok) break;
         ++tilesDone;
     }
-    // ---- weight-gradient partial sums of this CTA -> its slab
+    // ---- weight-gradient partial sums of this CTA -> its slab; the M = 64
+    // accumulator keeps row 16 q + i in lane 32 q + i (i < 16)
     umma::fenceBeforeSync();
     __syncthreads();
     umma::fenceAfterSync();
     float* slab = a.dwSlabs + static_cast<size_t>(blockIdx.x) * kDwSlabFloats;
-    const uint32_t lane = 32 * warp + (tid & 31);
     const bool holdsRow = (tid & 31) < 16;
-    const uint32_t r = warp * 16 + (tid & 31);           // row of the M = 64 result held by this lane
+    const uint32_t row64 = 16 * (warp & 3) + (tid & 31);
     for (int l = 0; l < kNumLayers; ++l) {
-        for (int c = 0; c < kHidden; c += 16) {
+        for (int c = 32 * half; c < 32 * half + 32; c += 16) {
             float v[16];
-            umma::tmemLoad16(umma::tmemAt(tmem, 32 * warp, 64 + 64 * l + c), v);
+            umma::tmemLoad16(umma::tmemAt(tmem, lane0, 64 + 64 * l + c), v);
             if (holdsRow) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
-                    slab[l * kHidden * kHidden + r * kHidden + c + i] = (tilesDone > 0 && ok) ? v[i] : 0.0f;
+                    slab[l * kHidden * kHidden + row64 * kHidden + c + i] = (tilesDone > 0 && ok) ? v[i] : 0.0f;
             }
         }
     }
-    (void)lane;
     // loss: block reduction then one atomic
     for (int off = 16; off > 0; off >>= 1) lossAcc += __shfl_xor_sync(0xFFFFFFFFu, lossAcc, off);
-    __shared__ float sLoss[kRows / 32];
+    __shared__ float sLoss[kTrainThreads / 32];
     if ((tid & 31) == 0) sLoss[warp] = lossAcc;
     umma::fenceBeforeSync();
     __syncthreads();
     if (tid == 0) {
         float t = 0.0f;
-        for (int i = 0; i < kRows / 32; ++i) t += sLoss[i];
+        for (uint32_t i = 0; i < kTrainThreads / 32; ++i) t += sLoss[i];
         atomicAdd(a.lossSum, t);
     }
     if (warp == 0) umma::tmemFree(tmem, kTrainTmemCols);

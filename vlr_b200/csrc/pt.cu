@@ -157,6 +157,9 @@ __device__ __forceinline__ void loadMixture(const GuideFrame &gf, uint32_t P, ui
     const float4 w0 = gf.lobeWeights[p], w1 = gf.lobeWeights[static_cast<size_t>(P) + p];
     m.weight[0] = w0.x; m.weight[1] = w0.y; m.weight[2] = w0.z; m.weight[3] = w0.w;
     m.weight[4] = w1.x; m.weight[5] = w1.y; m.weight[6] = w1.z; m.weight[7] = w1.w;
+    const float4 s0 = gf.lobeScales[p], s1 = gf.lobeScales[static_cast<size_t>(P) + p];
+    m.scale[0] = s0.x; m.scale[1] = s0.y; m.scale[2] = s0.z; m.scale[3] = s0.w;
+    m.scale[4] = s1.x; m.scale[5] = s1.y; m.scale[6] = s1.z; m.scale[7] = s1.w;
 }
 
 // Three resident 256-thread blocks per SM (85 registers): the kernel is
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         bool guided = false;
         guide::Mixture mix;
         if constexpr (kGuide) {
-            guided = gf.sample && isGuidedKind(k);
+            guided = gf.sample && isGuidedKind(k) && fp.bounce < gf.recBounces;
             if (guided) loadMixture(gf, P, p, mix);
         }
         // next-event estimation
@@ -438,6 +441,7 @@ struct MixtureDst {
     GuidedHitSrc src;
     float4* lobes;
     float4* lobeWeights;
+    float4* lobeScales;
     __device__ void store(uint32_t i, const float y[guide::kOut]) const {
         const uint32_t p = src.pathOf(i);
         const uint32_t P = src.fp.numPaths;
@@ -447,6 +451,8 @@ struct MixtureDst {
         for (int k = 0; k < guide::kLobes; ++k) lobes[static_cast<size_t>(k) * P + p] = m.lobe[k];
         lobeWeights[p] = make_float4(m.weight[0], m.weight[1], m.weight[2], m.weight[3]);
         lobeWeights[static_cast<size_t>(P) + p] = make_float4(m.weight[4], m.weight[5], m.weight[6], m.weight[7]);
+        lobeScales[p] = make_float4(m.scale[0], m.scale[1], m.scale[2], m.scale[3]);
+        lobeScales[static_cast<size_t>(P) + p] = make_float4(m.scale[4], m.scale[5], m.scale[6], m.scale[7]);
     }
 };
 
@@ -465,24 +471,38 @@ __global__ void __launch_bounds__(256) guideFinalizeKernel(PathBuffers pb, Frame
     const uint32_t last = gf.counts[2];
     const uint32_t stamp = gf.counts[kCountStamp];
     const float accept = last > gf.targetSamples ? static_cast<float>(gf.targetSamples) / last : 1.0f;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        const float4 cEnd = pb.contrib[p];
-        for (uint32_t b = 0; b < gf.recBounces; ++b) {
-            if (gf.recStamp[static_cast<size_t>(b) * P + p] != stamp) continue;
-            const float4 beta = recField(gf, P, b, 4)[p];
-            const float4 snap = recField(gf, P, b, 5)[p];
-            const float bt[4] = { beta.x, beta.y, beta.z, beta.w };
-            const float dc[4] = { cEnd.x - snap.x, cEnd.y - snap.y, cEnd.z - snap.z, cEnd.w - snap.w };
+    // one thread per (bounce, path) record: independent loads in flight
+    const size_t total = static_cast<size_t>(P) * gf.recBounces;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const uint32_t b = static_cast<uint32_t>(i / P), p = static_cast<uint32_t>(i % P);
+        {
             float w = 0.0f;
-            for (int i = 0; i < 4; ++i)
-                if (bt[i] > 0.0f) w += fmaxf(dc[i], 0.0f) / bt[i];
-            w *= 0.25f;
-            if (!(w > 0.0f) || !isfinite(w)) continue;
-            atomicAdd(gf.counts + 1, 1u);
-            const float u = (mixBits(p, b, stamp) >> 8) * (1.0f / 16777216.0f);
-            if (u >= accept) continue;
-            const uint32_t slot = atomicAdd(gf.counts, 1u);
-            if (slot >= gf.sampleCapacity) continue;
+            if (gf.recStamp[i] == stamp) {
+                const float4 cEnd = pb.contrib[p];
+                const float4 beta = recField(gf, P, b, 4)[p];
+                const float4 snap = recField(gf, P, b, 5)[p];
+                const float bt[4] = { beta.x, beta.y, beta.z, beta.w };
+                const float dc[4] = { cEnd.x - snap.x, cEnd.y - snap.y, cEnd.z - snap.z, cEnd.w - snap.w };
+                for (int i = 0; i < 4; ++i)
+                    if (bt[i] > 0.0f) w += fmaxf(dc[i], 0.0f) / bt[i];
+                w *= 0.25f;
+            }
+            const bool cand = w > 0.0f && isfinite(w);
+            const bool keep = cand && (mixBits(p, b, stamp) >> 8) * (1.0f / 16777216.0f) < accept;
+            // one atomic per warp for the candidate count and the slots
+            const uint32_t active = __activemask();
+            const int leader = __ffs(active) - 1;
+            const uint32_t lane = threadIdx.x & 31;
+            const uint32_t cm = __ballot_sync(active, cand), km = __ballot_sync(active, keep);
+            uint32_t base = 0;
+            if (static_cast<int>(lane) == leader) {
+                if (cm) atomicAdd(gf.counts + 1, static_cast<uint32_t>(__popc(cm)));
+                if (km) base = atomicAdd(gf.counts, static_cast<uint32_t>(__popc(km)));
+            }
+            base = __shfl_sync(active, base, leader);
+            const uint32_t slot = base + __popc(km & ((1u << lane) - 1u));
+            if (!keep || slot >= gf.sampleCapacity) continue;
             const float4 pos = recField(gf, P, b, 0)[p];
             guide::Sample smp;
             smp.posWeight = make_float4(pos.x, pos.y, pos.z, w);
@@ -611,7 +631,7 @@ void carvePathBuffers(void* base, uint32_t P, PathBuffers* pb) {
 size_t guideBufferBytes(uint32_t P, uint32_t recBounces, uint32_t sampleCapacity) {
     size_t b = 0;
     b += a256(size_t(P) * 16 * guide::kLobes);
-    b += a256(size_t(P) * 16 * 2);
+    b += a256(size_t(P) * 16 * 2) * 2;
     b += a256(size_t(P) * 16 * kRecFields * recBounces);
     b += a256(size_t(P) * 4 * recBounces);
     b += a256(size_t(sampleCapacity) * sizeof(guide::Sample));
@@ -624,6 +644,7 @@ void carveGuideBuffers(void* base, uint32_t P, uint32_t recBounces, uint32_t sam
     auto take = [&](size_t bytes) { char* r = s; s += a256(bytes); return r; };
     gf->lobes = reinterpret_cast<float4*>(take(size_t(P) * 16 * guide::kLobes));
     gf->lobeWeights = reinterpret_cast<float4*>(take(size_t(P) * 16 * 2));
+    gf->lobeScales = reinterpret_cast<float4*>(take(size_t(P) * 16 * 2));
     gf->rec = reinterpret_cast<float4*>(take(size_t(P) * 16 * kRecFields * recBounces));
     gf->recStamp = reinterpret_cast<uint32_t*>(take(size_t(P) * 4 * recBounces));
     gf->samples = reinterpret_cast<guide::Sample*>(take(size_t(sampleCapacity) * sizeof(guide::Sample)));
@@ -695,14 +716,14 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
         T.begin(kStageTrace, stream, pMain);
         traceKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);
         T.end(stream);
-        if (guiding && gfp->sample) {
+        if (guiding && gfp->sample && b < gfp->recBounces) {
             GuidedHitSrc src{ scene, pb, fp, gfp->net };
-            MixtureDst dst{ src, gfp->lobes, gfp->lobeWeights };
+            MixtureDst dst{ src, gfp->lobes, gfp->lobeWeights, gfp->lobeScales };
             auto kern = guide::guideInferKernel<GuidedHitSrc, MixtureDst>;
             ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, guide::kInferSmemBytes),
                "infer smem");
             T.begin(kStageGuide, stream, sizeof(guide::Net) + 2 * sizeof(GuidedHitSrc));
-            kern<<<numSMs * 3, guide::kRows, guide::kInferSmemBytes, stream>>>(gfp->net, src, dst, gfp->err);
+            kern<<<numSMs * 3, guide::kInferThreads, guide::kInferSmemBytes, stream>>>(gfp->net, src, dst, gfp->err);
             T.end(stream);
         }
         T.begin(kStageShade, stream, pMain + (guiding ? sizeof(GuideFrame) : 0));

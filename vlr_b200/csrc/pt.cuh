@@ -62,11 +62,11 @@ struct Film {
     uint32_t* frames;
 };
 
-// Learned guiding for one launch.  `sample`: guided kinds (Matte,
-// LambertianScattering, UE4) draw their next direction from the network's
-// vMF mixture or the BSDF with probability 1/2 each and weight by the
-// combined density (one-sample MIS).  `record`: every guided-kind vertex of
-// the first recBounces bounces stores a training record; after the launch
+// Learned guiding for one launch, at the first recBounces bounces.
+// `sample`: guided kinds (Matte, LambertianScattering, UE4) draw their next
+// direction from the network's vMF mixture or the BSDF with probability 1/2
+// each and weight by the combined density (one-sample MIS).  `record`: every
+// guided-kind vertex stores a training record; after the launch
 // each record becomes a training sample (position, directions, weight =
 // radiance carried back along wi x BSDF x cos / pdf, per path).
 constexpr uint32_t kMaxRecBounces = 8;
@@ -81,6 +81,7 @@ struct GuideFrame {
     guide::Net net;
     float4* lobes;             // [kLobes][P]  (mu, kappa)
     float4* lobeWeights;       // [2][P]       mixture weights
+    float4* lobeScales;        // [2][P]       weight x vMF normalisation
     float4* rec;               // [recBounces][kRecFields][P]
     uint32_t* recStamp;        // [recBounces][P] launch stamp once a record is complete
     guide::Sample* samples;    // training-sample buffer

@@ -250,6 +250,7 @@ bool kindAny(const Object*) { return true; }
 #define API_CATCH(name)                                               \
     }                                                                 \
     catch (const std::exception &ex) {                                \
+        cudaGetLastError(); /* a failed call must not leak into the next */ \
         std::fprintf(stderr, "%s: %s\n", name, ex.what());            \
         return VLRResult_InternalError;                               \
     }
