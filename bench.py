@@ -216,18 +216,28 @@ def time_to_rmse():
         y = f @ cy
         return y.view(H // b, b, W // b, b).mean(dim=(1, 3))
 
-    ctx, cam, keep = make(False, 0x9E3779B97F4A7C15)
-    ctx.render_samples(cam, True, RMSE_REF_SPP)
-    ref = blocks(ctx) / RMSE_REF_SPP
-    torch.cuda.synchronize()
-    ctx.close()
+    # the reference in two independent halves: their difference measures the
+    # reference's own noise, which is subtracted from every squared error
+    halves = []
+    for seed in (0x9E3779B97F4A7C15, 0xD1B54A32D192ED03):
+        ctx, cam, keep = make(False, seed)
+        ctx.render_samples(cam, True, RMSE_REF_SPP // 2)
+        halves.append(blocks(ctx) / (RMSE_REF_SPP // 2))
+        torch.cuda.synchronize()
+        ctx.close()
+    ref = 0.5 * (halves[0] + halves[1])
+    ref_var = (torch.mean((halves[0] - halves[1]) ** 2) / 4).item()
     ref_mean = ref.mean().item()
     out = {"scene": "Cornell box, 20,022-triangle GGX dielectric sphere (IOR 1.5, roughness 0.02), light 0.1x area",
            "resolution": [W, H], "max_path_length": MAX_PATH_LENGTH, "target": RMSE_TARGET,
            "error": f"RMSE of {b}x{b}-pixel block means of CIE Y / reference mean",
-           "reference": f"plain PT, {RMSE_REF_SPP} spp, FP64 film, independent seed",
+           "reference": f"plain PT, {RMSE_REF_SPP} spp in two independently seeded halves, FP64 film; "
+                        f"the reference's own variance (a quarter of the halves' mean squared difference) is "
+                        f"subtracted from each squared error",
+           "reference_noise": None,
            "dielectric_pdf": "consistent (the reference's MicrofacetScattering pdf is 0 for exits: "
                              "NEE double counting and fireflies)"}
+    out["reference_noise"] = math.sqrt(ref_var) / ref_mean
     for name, guided in (("plain", False), ("guided", True)):
         ctx, cam, keep = make(guided, 0)
         stream = torch.cuda.current_stream()
@@ -243,7 +253,8 @@ def time_to_rmse():
             e1.synchronize()
             t += e0.elapsed_time(e1) * 1e-3
             n += RMSE_CHUNK_SPP
-            err = (torch.sqrt(torch.mean((blocks(ctx) / n - ref) ** 2)) / ref_mean).item()
+            mse = torch.mean((blocks(ctx) / n - ref) ** 2).item()
+            err = math.sqrt(max(mse - ref_var, 0.0)) / ref_mean
             if n in (4, 16, 64, 256, 1024, 4096) or err <= RMSE_TARGET:
                 curve.append([n, round(t, 4), err])
             if err <= RMSE_TARGET:
@@ -404,18 +415,13 @@ def main():
 
     film_t = None
     if world > 1:
-        class _Film:
-            pass
-        # Wrap the library's FP64 film (W*H*16 doubles) for the all-reduce.
-        f = _Film()
-        f.__cuda_array_interface__ = {"shape": (H * W * 16,), "typestr": "<f8", "version": 3,
-                                      "data": (ctx.film_device_ptr(), False)}
-        film_t = torch.as_tensor(f, device="cuda")
+        from vlr_b200 import multigpu
+        film_t = multigpu.film_tensor(ctx)
 
     def step():
         ctx.render_samples(cam, True, SPP_PER_STEP, stream=stream)
         if film_t is not None:
-            dist.all_reduce(film_t)
+            multigpu.allreduce_film(film_t)
 
     for _ in range(args.warmup):
         step()
@@ -437,13 +443,8 @@ def main():
     seg = ctx.stats()["pathSegments"] - seg0
     _, launches = ctx.kernel_times()
     param_bytes = ctx.launch_param_bytes()
-    t = torch.tensor([ms, float(seg)], device="cuda", dtype=torch.float64)
     if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, seg_total = mx[0].item(), sm[1].item()
+        ms_max, seg_total = multigpu.combine(ms, seg)
     else:
         ms_max, seg_total = ms, float(seg)
     value = seg_total / (ms_max * 1e-3) / 1e9
@@ -459,13 +460,8 @@ def main():
         ctx.read_output(out_np)
     t_e2e = time.perf_counter() - t0
     seg_e2e = ctx.stats()["pathSegments"] - seg1
-    te = torch.tensor([t_e2e, float(seg_e2e)], device="cuda", dtype=torch.float64)
     if world > 1:
-        mx = te.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = te.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        t_e2e, seg_e2e = mx[0].item(), sm[1].item()
+        t_e2e, seg_e2e = multigpu.combine(t_e2e, seg_e2e)
     e2e = seg_e2e / t_e2e / 1e9
 
     # ---- per-stage device times (separate profiled pass; events add syncs)

@@ -125,7 +125,7 @@ typedef struct VLRBGuidingOptions {
     float learningRate;           /* default 1e-2 */
     uint32_t samplesPerStep;      /* default 2^18 */
     uint32_t stepsPerLaunch;      /* default 1 */
-    uint32_t recordBounces;       /* bounces that are guided and recorded, 1..8, default 4 */
+    uint32_t recordBounces;       /* bounces that are guided and recorded, 1..8, default 2 */
     uint32_t warmupLaunches;      /* default 4 */
 } VLRBGuidingOptions;
 
@@ -136,9 +136,15 @@ typedef struct VLRBGuidingStats {
     uint32_t lastSamples;         /* training samples the latest launch recorded */
 } VLRBGuidingStats;
 
+typedef struct VLRBGuideNet_API* VLRBGuideNet;
 VLRResult vlrbContextSetGuiding(VLRContext context, const VLRBGuidingOptions* options);
 VLRResult vlrbContextGetGuiding(VLRContext context, VLRBGuidingOptions* options);
 VLRResult vlrbContextGetGuidingStats(VLRContext context, VLRBGuidingStats* stats);
+/* A handle to the context's network (created by its first guided or
+ * training render) for the vlrbGuideNet* calls below; release it with
+ * vlrbGuideNetDestroy, which leaves the context's network alone.  The handle
+ * is valid while the context lives and keeps its guiding table size. */
+VLRResult vlrbContextGetGuideNet(VLRContext context, VLRBGuideNet* net);
 
 /* Copies the FP64 spectral film (width * height * 16 doubles, strata of
  * 29.375 nm over 360-830 nm, sum over accumulated samples) to host memory. */
@@ -258,7 +264,6 @@ VLRResult vlrbRenderBatchDestroy(VLRBRenderBatch batch);
  * outgoing direction (xyz, pad), shading normal (xyz, pad), incident
  * direction (xyz, pad).  The loss is sum_j (w_j / sum w) * -log q(wi_j).
  * ---------------------------------------------------------------------- */
-typedef struct VLRBGuideNet_API* VLRBGuideNet;
 VLRResult vlrbGuideNetCreate(uint32_t log2TableSize, uint64_t seed, VLRBGuideNet* net);
 VLRResult vlrbGuideNetDestroy(VLRBGuideNet net);
 VLRResult vlrbGuideNetSetBounds(VLRBGuideNet net, const float* lo, const float* hi);

@@ -852,7 +852,8 @@ void Context::readStats(RenderStats* out) {
     if (sg.bvh.errorFlag) {
         uint32_t e = 0;
         ck(cudaMemcpy(&e, sg.bvh.errorFlag, 4, cudaMemcpyDeviceToHost), "bvh flag");
-        if (e) throw std::runtime_error("BVH traversal met an out-of-range node reference");
+        if (e & 1u) throw std::runtime_error("BVH traversal met an out-of-range node reference");
+        if (e & 2u) throw std::runtime_error("BVH traversal stack overflowed (a hierarchy deeper than 64 levels)");
     }
     out->segments = t[0] + tl[0] + totalsBase[0];
     out->shadowRays = t[1] + tl[1] + totalsBase[1];

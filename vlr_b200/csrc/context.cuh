@@ -50,7 +50,7 @@ struct GuidingOptions {
     float learningRate = 1e-2f;
     uint32_t samplesPerStep = 1u << 18;
     uint32_t stepsPerLaunch = 1;
-    uint32_t recordBounces = 4;
+    uint32_t recordBounces = 2;
     uint32_t warmupLaunches = 4;      // launches that train on plain BSDF sampling first
 };
 

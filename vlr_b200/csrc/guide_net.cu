@@ -217,10 +217,6 @@ float GuideNet::lastLoss() const {
 // ------------------------------------------------------------ C entry points
 using vlrb::guide::GuideNet;
 
-struct VLRBGuideNet_API {
-    GuideNet* impl;
-};
-
 namespace {
 
 struct DevMem {
@@ -248,12 +244,12 @@ VLRResult guarded(const char* name, F f) {
 
 extern "C" VLRResult vlrbGuideNetCreate(uint32_t log2TableSize, uint64_t seed, VLRBGuideNet* net) {
     if (!net || log2TableSize < 8 || log2TableSize > 24) return VLRResult_InvalidArgument;
-    return guarded("vlrbGuideNetCreate", [&] { *net = new VLRBGuideNet_API{ new GuideNet(log2TableSize, seed) }; });
+    return guarded("vlrbGuideNetCreate", [&] { *net = new VLRBGuideNet_API{ new GuideNet(log2TableSize, seed), true }; });
 }
 
 extern "C" VLRResult vlrbGuideNetDestroy(VLRBGuideNet net) {
     if (!net) return VLRResult_InvalidInstance;
-    delete net->impl;
+    if (net->owned) delete net->impl;
     delete net;
     return VLRResult_NoError;
 }

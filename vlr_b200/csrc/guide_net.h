@@ -44,3 +44,10 @@ private:
 
 } // namespace guide
 } // namespace vlrb
+
+// Handle behind VLRBGuideNet: a network the handle owns, or a context's
+// network lent out by vlrbContextGetGuideNet.
+struct VLRBGuideNet_API {
+    vlrb::guide::GuideNet* impl;
+    bool owned;
+};

@@ -34,7 +34,7 @@ struct Bvh {
     const BvhNode* nodes;
     const BvhTri* tris;
     uint32_t numTris;
-    uint32_t* errorFlag;   // set to 1 when traversal meets an out-of-range node reference
+    uint32_t* errorFlag;   // bit 0: out-of-range node reference met; bit 1: traversal stack overflow
 };
 
 struct Hit {
@@ -110,6 +110,7 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
             if (hit0 && hit1) {
                 if (t1 < t0) { int tmp = c0; c0 = c1; c1 = tmp; }
                 if (sp < kTraversalStack) stack[sp++] = c1;
+                else if (bvh.errorFlag) atomicOr(bvh.errorFlag, 2u);
                 node = c0;
                 continue;
             }

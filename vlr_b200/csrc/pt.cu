@@ -142,7 +142,8 @@ __device__ __forceinline__ float4* recField(const GuideFrame &gf, uint32_t P, ui
 }
 
 // Completes the training record of the previous bounce with the path's
-// contribution before anything of this vertex is added.
+// contribution so far (everything gathered after the snapshot is the
+// indirect light the previous vertex received along its sampled direction).
 __device__ __forceinline__ void completeRecord(const GuideFrame &gf, uint32_t P, uint32_t bounce, uint32_t p,
                                                uint32_t flags, const S4 &contrib) {
     if (!(flags & kFlagRecordPending) || bounce == 0) return;
@@ -188,10 +189,11 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         uint32_t pathLength = ((flags >> 8) & 0xFFFFu) + 1;
         bool maxLengthTerminate = pathLength >= fp.maxPathLength;
         S4 contrib = toS4(pb.contrib[p]);
-        if constexpr (kGuide) completeRecord(gf, P, fp.bounce, p, flags, contrib);
+        const uint32_t flagsIn = flags;
         flags = (flags & 0x1Fu) | (pathLength << 8) | (maxLengthTerminate ? 0x20u : 0u);
         if (k == kNumBsdfKinds) {
             shadeMiss(S, pb, p, wls, pathLength, contrib);
+            if constexpr (kGuide) completeRecord(gf, P, fp.bounce, p, flagsIn, contrib);
             pb.contrib[p] = toF4(contrib);
             pb.flags[p] = flags;
             continue;
@@ -221,6 +223,10 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
             }
             contrib += alpha * Le * MIS;
         }
+        // The record of the previous vertex closes after this vertex's
+        // emission: light reached directly from there is NEE's job, and the
+        // network learns the indirect light NEE cannot sample.
+        if constexpr (kGuide) completeRecord(gf, P, fp.bounce, p, flagsIn, contrib);
         pb.contrib[p] = toF4(contrib);
         pb.flags[p] = flags;
         if (maxLengthTerminate) continue;

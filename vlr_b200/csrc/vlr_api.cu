@@ -1274,6 +1274,13 @@ VLRResult vlrbContextGetGuiding(VLRContext context, VLRBGuidingOptions* o) {
     return VLRResult_NoError;
 }
 
+VLRResult vlrbContextGetGuideNet(VLRContext context, VLRBGuideNet* net) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!net || !c->guideNet) return VLRResult_InvalidArgument;
+    *net = new VLRBGuideNet_API{ c->guideNet.get(), false };
+    return VLRResult_NoError;
+}
+
 VLRResult vlrbContextGetGuidingStats(VLRContext context, VLRBGuidingStats* st) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!st) return VLRResult_InvalidArgument;

@@ -44,6 +44,17 @@ class GuideNet:
         check(_api().vlrbGuideNetGetSizes(self.h, ctypes.byref(nw), ctypes.byref(ng)), "getSizes")
         self.n_weights, self.n_grid = nw.value, ng.value
 
+    @classmethod
+    def from_handle(cls, h, log2_table):
+        """Wrap an existing handle (e.g. vlrbContextGetGuideNet's)."""
+        self = cls.__new__(cls)
+        self.h = h
+        self.log2_table = log2_table
+        nw, ng = c_uint32(), c_uint64()
+        check(_api().vlrbGuideNetGetSizes(self.h, ctypes.byref(nw), ctypes.byref(ng)), "getSizes")
+        self.n_weights, self.n_grid = nw.value, ng.value
+        return self
+
     def close(self):
         if self.h:
             _api().vlrbGuideNetDestroy(self.h)

@@ -121,6 +121,7 @@ def _api():
                                 ctypes.POINTER(ctypes.c_uint32)],
         "vlrbContextGetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
         "vlrbContextGetGuidingStats": [v, ctypes.POINTER(VLRBGuidingStats)],
+        "vlrbContextGetGuideNet": [v, ctypes.POINTER(c_void_p)],
         "vlrbContextReadFilm": [v, v],
         "vlrbContextGetOutputDevicePointer": [v, ctypes.POINTER(v)],
         "vlrbContextSetProfiling": [v, ctypes.c_bool],
@@ -366,6 +367,15 @@ class Context:
                 raise TypeError(f"unknown guiding option {k}")
             setattr(o, k, val)
         check(_api().vlrbContextSetGuiding(self.h, ctypes.byref(o)), "setGuiding")
+
+    def guide_net(self):
+        """The context's guiding network as a vlr_b200.guide.GuideNet (borrowed)."""
+        from .guide import GuideNet
+        h = c_void_p()
+        check(_api().vlrbContextGetGuideNet(self.h, ctypes.byref(h)), "getGuideNet")
+        o = VLRBGuidingOptions()
+        check(_api().vlrbContextGetGuiding(self.h, ctypes.byref(o)), "getGuiding")
+        return GuideNet.from_handle(h, o.log2TableSize)
 
     def guiding_stats(self):
         st = VLRBGuidingStats()
