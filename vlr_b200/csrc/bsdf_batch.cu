@@ -1,6 +1,6 @@
-// BSDF shading batch: one thread per query, each query = Meng upsampling of
-// the query's RGB albedo and grey IOR, construction of one of the six BSDFs,
-// then sample + evaluate + evaluatePDF at the sampled direction.
+// BSDF shading batch: each query = Meng upsampling of the query's RGB albedo
+// and grey IOR, construction of one of the six BSDFs, then sample + evaluate
+// + evaluatePDF at the sampled direction.
 //
 // This translation unit is compiled with -fmad=false so every product and sum
 // is rounded exactly like the reference's host build (materials.cu classes
@@ -36,13 +36,16 @@ struct BsdfBatchArgs {
 // Builds the BSDF of material `kind` from the query's immediate parameters in
 // the way the reference's setupBSDF callables do (materials.cu:653-661,
 // 776-787, 1220-1240, 1516-1536, 1674-1684, 1959-1978).
+// K is the material id (ids above kUE4 build the UE4 BSDF, as the
+// reference's default branch does).
+template <uint32_t K>
 __device__ __forceinline__ Bsdf buildBatchBsdf(const BsdfBatchArgs &a, int64_t i, const WLS &wls) {
     Bsdf B;
     const ColorMatrices &M = *a.mats;
     const float r = __ldg(a.rgb + 3 * i + 0), g = __ldg(a.rgb + 3 * i + 1), b = __ldg(a.rgb + 3 * i + 2);
     const float eta = __ldg(a.ior + i);
     const float rx = __ldg(a.rough + 2 * i + 0), ry = __ldg(a.rough + 2 * i + 1);
-    const uint32_t kind = __ldg(a.mat + i);
+    constexpr uint32_t kind = K;
     B.kind = kind;
     B.flags = 0;
     B.f0 = B.f1 = B.f2 = 0.0f;
@@ -99,70 +102,77 @@ __device__ __forceinline__ Bsdf buildBatchBsdf(const BsdfBatchArgs &a, int64_t i
     return B;
 }
 
-// Queries arrive in random material order; shading them in that order makes
-// every warp execute all six BSDFs.  Each CTA therefore takes a tile of 256
-// queries, counting-sorts the tile's indices by material in shared memory,
-// and lets thread t shade the t-th query of the sorted tile, so warps run one
-// material each except at the few material boundaries.  Inputs and outputs
-// stay in their original slots.
-constexpr int kBatchTile = 256;
-
-__global__ void __launch_bounds__(kBatchTile) bsdfBatchKernel(BsdfBatchArgs a) {
-    __shared__ uint32_t sCount[8];
-    __shared__ uint32_t sOffset[8];
-    __shared__ uint16_t sOrder[kBatchTile];
-    const int64_t numTiles = (a.n + kBatchTile - 1) / kBatchTile;
-    for (int64_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x) {
-        const int64_t base = tile * kBatchTile;
-        if (threadIdx.x < 8) sCount[threadIdx.x] = 0;
-        __syncthreads();
-        const int64_t mine = base + threadIdx.x;
-        uint32_t key = 7;   // slots past the end of the batch sort last
-        if (mine < a.n) key = min(__ldg(a.mat + mine), 6u);
-        const uint32_t rank = atomicAdd(&sCount[key], 1u);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t run = 0;
-            for (int k = 0; k < 8; ++k) { sOffset[k] = run; run += sCount[k]; }
-        }
-        __syncthreads();
-        sOrder[sOffset[key] + rank] = static_cast<uint16_t>(threadIdx.x);
-        __syncthreads();
-        const int64_t i = base + sOrder[threadIdx.x];
-        __syncthreads();
-        if (i >= a.n) continue;
-        float wlPdf;
-        WLS wls = WLS::equalOffsets(__ldg(a.wl + 2 * i + 0), __ldg(a.wl + 2 * i + 1), &wlPdf);
-        Bsdf B = buildBatchBsdf(a, i, wls);
-        BsdfQuery q;
-        q.dirLocal = V3(__ldg(a.wo + 3 * i + 0), __ldg(a.wo + 3 * i + 1), __ldg(a.wo + 3 * i + 2));
-        q.wlHint = wls.selected;
-        q.filter = dir::All;
-        q.importanceMode = 0;
-        const float uc = __ldg(a.u + 3 * i + 0), u0 = __ldg(a.u + 3 * i + 1), u1 = __ldg(a.u + 3 * i + 2);
-        BsdfSample s;
-        s.dirPDF = 0.0f;
-        s.dirLocal = V3(0.0f, 0.0f, 0.0f);
-        S4 fs = bsdfSampleInternal(B, q, uc, u0, u1, &s, nullptr);
-        float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), e4 = v4;
-        float pdf = 0.0f, epdf = 0.0f;
-        V3 wi(0.0f, 0.0f, 0.0f);
-        if (s.dirPDF > 0.0f) {
-            v4 = make_float4(fs[0], fs[1], fs[2], fs[3]);
-            pdf = s.dirPDF;
-            wi = s.dirLocal;
-            S4 ev = bsdfEvalInternal(B, q, wi, nullptr);
-            e4 = make_float4(ev[0], ev[1], ev[2], ev[3]);
-            epdf = bsdfPDFInternal(B, q, wi, nullptr);
-        }
-        reinterpret_cast<float4*>(a.value)[i] = v4;
-        a.pdf[i] = pdf;
-        a.wi[3 * i + 0] = wi.x;
-        a.wi[3 * i + 1] = wi.y;
-        a.wi[3 * i + 2] = wi.z;
-        reinterpret_cast<float4*>(a.evalValue)[i] = e4;
-        a.evalPdf[i] = epdf;
+// One query: sample, then evaluate value and pdf at the sampled direction.
+template <uint32_t K>
+__device__ __forceinline__ void shadeQuery(const BsdfBatchArgs &a, int64_t i) {
+    float wlPdf;
+    WLS wls = WLS::equalOffsets(__ldg(a.wl + 2 * i + 0), __ldg(a.wl + 2 * i + 1), &wlPdf);
+    Bsdf B = buildBatchBsdf<K>(a, i, wls);
+    BsdfQuery q;
+    q.dirLocal = V3(__ldg(a.wo + 3 * i + 0), __ldg(a.wo + 3 * i + 1), __ldg(a.wo + 3 * i + 2));
+    q.wlHint = wls.selected;
+    q.filter = dir::All;
+    q.importanceMode = 0;
+    const float uc = __ldg(a.u + 3 * i + 0), u0 = __ldg(a.u + 3 * i + 1), u1 = __ldg(a.u + 3 * i + 2);
+    BsdfSample s;
+    s.dirPDF = 0.0f;
+    s.dirLocal = V3(0.0f, 0.0f, 0.0f);
+    S4 fs = bsdfSampleInternal(B, q, uc, u0, u1, &s, nullptr);
+    float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), e4 = v4;
+    float pdf = 0.0f, epdf = 0.0f;
+    V3 wi(0.0f, 0.0f, 0.0f);
+    if (s.dirPDF > 0.0f) {
+        v4 = make_float4(fs[0], fs[1], fs[2], fs[3]);
+        pdf = s.dirPDF;
+        wi = s.dirLocal;
+        S4 ev = bsdfEvalInternal(B, q, wi, nullptr);
+        e4 = make_float4(ev[0], ev[1], ev[2], ev[3]);
+        epdf = bsdfPDFInternal(B, q, wi, nullptr);
     }
+    reinterpret_cast<float4*>(a.value)[i] = v4;
+    a.pdf[i] = pdf;
+    a.wi[3 * i + 0] = wi.x;
+    a.wi[3 * i + 1] = wi.y;
+    a.wi[3 * i + 2] = wi.z;
+    reinterpret_cast<float4*>(a.evalValue)[i] = e4;
+    a.evalPdf[i] = epdf;
+}
+
+// Queries arrive in random material order.  One launch per material: each
+// warp scans the material ids 32 at a time, collects the indices of its
+// material in shared memory (ballot + popcount, no block barriers) and
+// shades them 32 at a time, so every warp runs one BSDF with full lanes and
+// each launch's code is one BSDF's, which keeps the instruction cache warm.
+// Inputs and outputs stay in their original slots.
+constexpr int kBatchThreads = 256;
+
+template <uint32_t K>
+__global__ void __launch_bounds__(kBatchThreads) bsdfBatchKernel(BsdfBatchArgs a) {
+    __shared__ uint32_t sIdx[kBatchThreads / 32][64];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t warpId = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t numWarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    uint32_t pending = 0;
+    for (int64_t base = warpId * 32; base < a.n; base += numWarps * 32) {
+        const int64_t i = base + lane;
+        bool match = false;
+        if (i < a.n) {
+            const uint32_t m = __ldg(a.mat + i);
+            match = K == kUE4 ? m >= kUE4 : m == K;
+        }
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, match);
+        if (match) sIdx[w][pending + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint32_t>(i);
+        pending += __popc(bal);
+        __syncwarp();
+        if (pending >= 32) {
+            shadeQuery<K>(a, sIdx[w][lane]);
+            __syncwarp();
+            pending -= 32;
+            if (lane < pending) sIdx[w][lane] = sIdx[w][32 + lane];
+            __syncwarp();
+        }
+    }
+    if (lane < pending) shadeQuery<K>(a, sIdx[w][lane]);
 }
 
 static int g_numSMs = 0;
@@ -188,7 +198,7 @@ cudaError_t launchBsdfBatch(const VLRBBsdfBatch &b, cudaStream_t stream, float* 
     a.zeroIOR = mengUpsample(ht, hm, SpType::IOR, ColorSp::Rec709, 0.0f, 0.0f, 0.0f);
     // Grid: enough resident 256-thread CTAs to fill every SM several times
     // over, grid-striding beyond that.
-    const int64_t blocksNeeded = (b.count + 255) / 256;
+    const int64_t blocksNeeded = (b.count + kBatchThreads - 1) / kBatchThreads;
     const int64_t maxBlocks = static_cast<int64_t>(g_numSMs) * 8;
     const int blocks = static_cast<int>(blocksNeeded < maxBlocks ? blocksNeeded : maxBlocks);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -197,7 +207,21 @@ cudaError_t launchBsdfBatch(const VLRBBsdfBatch &b, cudaStream_t stream, float* 
         cudaEventCreate(&e1);
         cudaEventRecord(e0, stream);
     }
-    bsdfBatchKernel<<<blocks, 256, 0, stream>>>(a);
+    // indices are kept as 32-bit in shared memory: chunks of at most 2^31 queries
+    const int64_t chunk = int64_t(1) << 31;
+    for (int64_t first = 0; first < b.count; first += chunk) {
+        BsdfBatchArgs c = a;
+        c.n = b.count - first < chunk ? b.count - first : chunk;
+        c.wo += 3 * first; c.mat += first; c.rough += 2 * first; c.ior += first; c.rgb += 3 * first;
+        c.metallic += first; c.u += 3 * first; c.wl += 2 * first;
+        c.value += 4 * first; c.pdf += first; c.wi += 3 * first; c.evalValue += 4 * first; c.evalPdf += first;
+        bsdfBatchKernel<kMatte><<<blocks, kBatchThreads, 0, stream>>>(c);
+        bsdfBatchKernel<kSpecularBRDF><<<blocks, kBatchThreads, 0, stream>>>(c);
+        bsdfBatchKernel<kMicrofacetBRDF><<<blocks, kBatchThreads, 0, stream>>>(c);
+        bsdfBatchKernel<kMicrofacetBSDF><<<blocks, kBatchThreads, 0, stream>>>(c);
+        bsdfBatchKernel<kLambertianBSDF><<<blocks, kBatchThreads, 0, stream>>>(c);
+        bsdfBatchKernel<kUE4><<<blocks, kBatchThreads, 0, stream>>>(c);
+    }
     cudaError_t err = cudaGetLastError();
     if (kernelMs) {
         cudaEventRecord(e1, stream);
