@@ -91,6 +91,7 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
     V3 invDir(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
     int stack[kTraversalStack];
     int sp = 0;
+    bool overflow = false;   // reported once after the loop: an atomic inside it halves the speed
     int node = bvh.numTris == 1 ? ~0 : 0;
     while (true) {
         // A malformed hierarchy must not send the traversal outside its
@@ -110,7 +111,7 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
             if (hit0 && hit1) {
                 if (t1 < t0) { int tmp = c0; c0 = c1; c1 = tmp; }
                 if (sp < kTraversalStack) stack[sp++] = c1;
-                else if (bvh.errorFlag) atomicOr(bvh.errorFlag, 2u);
+                else overflow = true;
                 node = c0;
                 continue;
             }
@@ -131,6 +132,7 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
         if (sp == 0) break;
         node = stack[--sp];
     }
+    if (overflow && bvh.errorFlag) atomicOr(bvh.errorFlag, 2u);
     return h;
 }
 
