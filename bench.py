@@ -368,6 +368,91 @@ def terrain_workloads():
     return out
 
 
+def batch_workload():
+    """32 seeded scenes of uneven size (triangles log-uniform in [1k, 2M]
+    from the terrain/instance generator; resolution from {256^2, 512^2,
+    1024x768, 1920x1080}; 1-64 spp; odd scenes guided with online training),
+    each context's paths in flight and blocks per SM chosen by the
+    autotuner.  Rendered once as plain per-scene launches one after another,
+    then as one CUDA graph of all scenes replayed (vlrbRenderBatch*); reports
+    aggregate segments/s and per-scene frame latency p50/p99 for both."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    rng = np.random.default_rng(2024)
+    resolutions = [(256, 256), (512, 512), (1024, 768), (1920, 1080)]
+    items = []
+    for k in range(32):
+        tris = float(np.exp(rng.uniform(np.log(1e3), np.log(2e6))))
+        n_spheres = max(1, int(0.3 * tris / 320))
+        cells = max(8, int(np.sqrt(0.7 * tris / 2)))
+        W, H = resolutions[int(rng.integers(0, 4))]
+        spp = int(np.exp(rng.uniform(0, np.log(64))))
+        desc = scenes.terrain_scene_desc(W, H, cells=cells, n_spheres=n_spheres, seed=100 + k, sky=(256, 128))
+        ctx = V.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = scenes.build_instanced(ctx, desc)
+        ctx.setScene(scene)
+        ctx.setOptions(max_path_length=8, max_paths_in_flight=min(1 << 22, W * H * spp))
+        if k % 2 == 1:
+            ctx.setGuiding(enabled=True, train=True, log2TableSize=16, samplesPerStep=1 << 16)
+        items.append((ctx, cam, keep, spp, W, H))
+    for ctx, cam, keep, spp, W, H in items:
+        ctx.autotune(cam, samples_per_trial=1)
+    stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # per-scene launches, one scene after another (after one warm-up pass)
+    for ctx, cam, keep, spp, W, H in items:
+        ctx.render_samples(cam, True, spp, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    seg0 = sum(c.stats()["pathSegments"] for c, *_ in items)
+    lat = []
+    t0 = ev()
+    t0.record(stream)
+    for ctx, cam, keep, spp, W, H in items:
+        a, b = ev(), ev()
+        a.record(stream)
+        ctx.render_samples(cam, True, spp, stream=stream.cuda_stream)
+        b.record(stream)
+        lat.append((a, b))
+    t1 = ev()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = t0.elapsed_time(t1)
+    seq_lat = [a.elapsed_time(b) for a, b in lat]
+    seq_seg = sum(c.stats()["pathSegments"] for c, *_ in items) - seg0
+    # one graph of all scenes
+    batch = V.RenderBatch([(ctx, cam, spp, True) for ctx, cam, keep, spp, W, H in items])
+    batch.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    reps = 3
+    seg0 = sum(c.stats()["pathSegments"] for c, *_ in items)
+    g_lat = []
+    t0 = ev()
+    t0.record(stream)
+    for _ in range(reps):
+        batch.launch(stream.cuda_stream)
+        g_lat += batch.item_times()
+    t1 = ev()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    g_ms = t0.elapsed_time(t1) / reps
+    g_seg = (sum(c.stats()["pathSegments"] for c, *_ in items) - seg0) / reps
+    batch.close()
+    out = {"workload": "32 seeded terrain/instance scenes, 1k-2M triangles (log-uniform), 256^2..1920x1080, "
+                       "1-64 spp, half guided, autotuned launch configuration",
+           "triangles": [int(c.stats()["numTriangles"]) for c, *_ in items],
+           "per_scene_launches": {"segments_per_s": seq_seg / (seq_ms * 1e-3) / 1e9, "ms": seq_ms,
+                                  "latency_ms_p50": float(np.percentile(seq_lat, 50)),
+                                  "latency_ms_p99": float(np.percentile(seq_lat, 99))},
+           "graph_batch": {"segments_per_s": g_seg / (g_ms * 1e-3) / 1e9, "ms": g_ms,
+                           "latency_ms_p50": float(np.percentile(g_lat, 50)),
+                           "latency_ms_p99": float(np.percentile(g_lat, 99))},
+           "unit": "G path segments/s"}
+    for ctx, *_ in items:
+        ctx.close()
+    return out
+
+
 # Algorithmic bytes per unit of work of each wavefront stage (SoA path state,
 # counted once per read or write; BVH traffic excluded):
 #   trace: queue index 4 + ray 32 + hit 16 + bucket append 4          = 56 B / ray
@@ -499,7 +584,8 @@ def main():
     workloads = None
     if rank == 0 and world == 1 and not args.no_workloads:
         workloads = {}
-        for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads):
+        for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads,
+                   lambda: {"multi_scene_batch": batch_workload()}):
             try:
                 workloads.update(fn())
             except Exception as ex:  # reported, never fatal for the GPU line

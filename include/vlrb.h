@@ -110,10 +110,10 @@ typedef struct VLRBRenderStats {
 VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);
 
 /* Learned path guiding of the path tracer (no counterpart in the reference).
- * With `train`, every launch records training samples at the Matte,
+ * With `train`, a launch records training samples at the Matte,
  * LambertianScattering and UE4 vertices of its first `recordBounces` bounces
  * and is followed by `stepsPerLaunch` Adam steps on about `samplesPerStep` of
- * them.  With `enabled`, those vertices sample the next direction from the
+ * them (every launch during the warm-up, then every `trainInterval`-th).  With `enabled`, those vertices sample the next direction from the
  * network's vMF mixture or the BSDF with probability 1/2 each and weight by
  * the combined density (one-sample MIS: unbiased whatever the network
  * learned); when training too, guided sampling starts after `warmupLaunches`
@@ -127,6 +127,10 @@ typedef struct VLRBGuidingOptions {
     uint32_t stepsPerLaunch;      /* default 1 */
     uint32_t recordBounces;       /* bounces that are guided and recorded, 1..8, default 2 */
     uint32_t warmupLaunches;      /* default 4 */
+    float weightClamp;            /* > 0: training weights above this multiple of the batch
+                                     mean are clipped (0 = off, the default) */
+    uint32_t trainInterval;       /* after the warm-up, record and train on every n-th launch
+                                     (0 or 1 = every launch) */
 } VLRBGuidingOptions;
 
 typedef struct VLRBGuidingStats {

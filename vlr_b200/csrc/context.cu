@@ -599,6 +599,7 @@ void Context::ensureGuiding(uint32_t paths) {
     const float lo[3] = { sg.bounds.lo.x, sg.bounds.lo.y, sg.bounds.lo.z };
     const float hi[3] = { sg.bounds.hi.x, sg.bounds.hi.y, sg.bounds.hi.z };
     guideNet->setBounds(lo, hi);
+    guideNet->weightClamp = g.weightClamp;
     const uint32_t rec = std::min<uint32_t>(std::max<uint32_t>(g.recordBounces, 1u), kMaxRecBounces);
     const uint32_t cap = 2 * g.samplesPerStep;
     if (paths > guideCapacityPaths || rec != guideRecBounces || cap != guideSampleCapacity) {
@@ -691,13 +692,17 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
             }
             else if (guiding.enabled || guiding.train) {
                 ensureGuiding(pathCapacity);
-                gframe.record = guiding.train;
+                // record and train on every trainInterval-th launch once
+                // the warm-up launches are done
+                const uint32_t interval = std::max<uint32_t>(guiding.trainInterval, 1u);
+                gframe.record = guiding.train &&
+                                (guideLaunches < guiding.warmupLaunches || guideLaunches % interval == 0);
                 gframe.sample = guiding.enabled && (!guiding.train || guideLaunches >= guiding.warmupLaunches);
                 gframe.net = guideNet->net;
                 gframe.targetSamples = guiding.samplesPerStep;
                 ptRenderLaunch(sg, pb, fl, fp, numSMs, stream, &timer, &gframe);
                 if (gframe.sample) ++guidingStats.guidedLaunches;
-                if (guiding.train) trainGuide(stream);
+                if (gframe.record) trainGuide(stream);
                 ++guideLaunches;
             }
             else {

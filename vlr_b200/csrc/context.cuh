@@ -52,6 +52,8 @@ struct GuidingOptions {
     uint32_t stepsPerLaunch = 1;
     uint32_t recordBounces = 2;
     uint32_t warmupLaunches = 4;      // launches that train on plain BSDF sampling first
+    float weightClamp = 0.0f;         // > 0: clip training weights above this multiple of the batch mean
+    uint32_t trainInterval = 1;       // after warm-up, record and train on every n-th launch
 };
 
 struct GuidingStats {

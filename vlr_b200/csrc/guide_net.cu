@@ -181,7 +181,7 @@ void GuideNet::gradients(const Sample* samples, uint32_t n, cudaStream_t stream,
        "smem attr");
     const uint32_t tiles = (n + kRows - 1) / kRows;
     const uint32_t grid = tiles < uint32_t(numSMs) ? tiles : uint32_t(numSMs);
-    TrainArgs a{ samples, n, countDev, scalars, dwSlabs, scalars + 1, err };
+    TrainArgs a{ samples, n, countDev, scalars, weightClamp, dwSlabs, scalars + 1, err };
     guideTrainKernel<<<grid, kTrainThreads, kTrainSmemBytes, stream>>>(net, a);
     reduceDwKernel<<<(kDwSlabFloats + 255) / 256, 256, 0, stream>>>(dwSlabs, grid, net.wGrad);
     ck(cudaGetLastError(), "train launch");

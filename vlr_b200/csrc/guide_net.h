@@ -34,6 +34,7 @@ public:
     int device = 0;
     int numSMs = 148;
     uint32_t adamStep = 0;
+    float weightClamp = 0.0f;   // > 0: clip training weights above this multiple of the batch mean
     float* dwSlabs = nullptr;
     float* scalars = nullptr;   // [0] batch weight sum, [1] batch loss
     uint32_t* err = nullptr;

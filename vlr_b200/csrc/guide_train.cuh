@@ -33,6 +33,7 @@ struct TrainArgs {
     uint32_t count;            // buffer capacity (or the exact count when countDev is null)
     const uint32_t* countDev;  // device sample count (clamped to count), or null
     const float* weightSum;    // device: sum of the batch's sample weights
+    float weightClamp;         // > 0: weights above this multiple of the batch mean are clipped
     float* dwSlabs;            // [gridDim.x][4][64][64]
     float* lossSum;            // device accumulator of the batch loss
     uint32_t* err;
@@ -210,7 +211,9 @@ __global__ void __launch_bounds__(kTrainThreads, 1) guideTrainKernel(Net net, Tr
             float y[kOut], dy[kHidden];
 #pragma unroll
             for (int c = 0; c < kOut; c += 16) umma::tmemLoad16(umma::tmemAt(tmem, lane0, c), y + c);
-            const float w = valid ? s.posWeight.w * invWeightSum : 0.0f;
+            float w = valid ? s.posWeight.w * invWeightSum : 0.0f;
+            // clipping the rare huge weights (sum-normalised: mean = 1/count)
+            if (a.weightClamp > 0.0f) w = fminf(w, a.weightClamp / fmaxf(static_cast<float>(count), 1.0f));
             if (w > 0.0f) lossAcc += mixtureLossGrad(y, wi, w, dy);
             else {
 #pragma unroll

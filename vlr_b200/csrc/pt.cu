@@ -16,6 +16,7 @@
 // Queue lengths live in device counters, so a launch never synchronises with
 // the host and its fixed kernel sequence can be captured in a CUDA graph.
 #include "pt.cuh"
+#include <cuda_fp16.h>
 #include "guide_mlp.cuh"
 #include "tables.cuh"
 #include "wavefront.cuh"
@@ -152,20 +153,35 @@ __device__ __forceinline__ void completeRecord(const GuideFrame &gf, uint32_t P,
     gf.recStamp[static_cast<size_t>(b) * P + p] = gf.counts[kCountStamp];
 }
 
+__device__ __forceinline__ uint32_t packHalf2(float a, float b) {
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ float2 unpackHalf2(uint32_t u) {
+    return __half22float2(*reinterpret_cast<const __half2*>(&u));
+}
+
+// The stored mixture (112 B per path): directions, concentrations and
+// weights in half precision, and per lobe the FP32 factor that turns
+// exp(kappa (mu.w - 1)) into density, computed from the rounded values the
+// sampler uses, so sampling and pdf stay one density.
 __device__ __forceinline__ void loadMixture(const GuideFrame &gf, uint32_t P, uint32_t p, guide::Mixture &m) {
 #pragma unroll
-    for (int k = 0; k < guide::kLobes; ++k) m.lobe[k] = gf.lobes[static_cast<size_t>(k) * P + p];
-    const float4 w0 = gf.lobeWeights[p], w1 = gf.lobeWeights[static_cast<size_t>(P) + p];
-    m.weight[0] = w0.x; m.weight[1] = w0.y; m.weight[2] = w0.z; m.weight[3] = w0.w;
-    m.weight[4] = w1.x; m.weight[5] = w1.y; m.weight[6] = w1.z; m.weight[7] = w1.w;
+    for (int k = 0; k < guide::kLobes; ++k) {
+        const uint2 q = gf.lobes[static_cast<size_t>(k) * P + p];
+        const float2 a = unpackHalf2(q.x), b = unpackHalf2(q.y);
+        const float inv = rsqrtf(a.x * a.x + a.y * a.y + b.x * b.x);
+        m.lobe[k] = make_float4(a.x * inv, a.y * inv, b.x * inv, b.y);
+    }
+    const uint2 w0 = gf.lobeWeights[p], w1 = gf.lobeWeights[static_cast<size_t>(P) + p];
+    const float2 a = unpackHalf2(w0.x), b = unpackHalf2(w0.y), c = unpackHalf2(w1.x), d = unpackHalf2(w1.y);
+    m.weight[0] = a.x; m.weight[1] = a.y; m.weight[2] = b.x; m.weight[3] = b.y;
+    m.weight[4] = c.x; m.weight[5] = c.y; m.weight[6] = d.x; m.weight[7] = d.y;
     const float4 s0 = gf.lobeScales[p], s1 = gf.lobeScales[static_cast<size_t>(P) + p];
     m.scale[0] = s0.x; m.scale[1] = s0.y; m.scale[2] = s0.z; m.scale[3] = s0.w;
     m.scale[4] = s1.x; m.scale[5] = s1.y; m.scale[6] = s1.z; m.scale[7] = s1.w;
 }
 
-// Three resident 256-thread blocks per SM (85 registers): the kernel is
-// bound by memory latency, and the extra warps hide more of it than the
-// few spilled registers cost.
 template <bool kGuide>
 __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb, FrameParams fp, GuideFrame gf) {
     uint32_t* ctr = bounceCounters(pb, fp.bounce);
@@ -445,20 +461,39 @@ struct GuidedHitSrc {
 
 struct MixtureDst {
     GuidedHitSrc src;
-    float4* lobes;
-    float4* lobeWeights;
+    uint2* lobes;
+    uint2* lobeWeights;
     float4* lobeScales;
     __device__ void store(uint32_t i, const float y[guide::kOut]) const {
         const uint32_t p = src.pathOf(i);
         const uint32_t P = src.fp.numPaths;
         guide::Mixture m;
         guide::decodeMixture(y, m);
+        // round to half, then derive the density factors from what the
+        // sampler will read back: lobe k is chosen with the probability its
+        // cumulative-weight test gives (the last lobe takes the remainder)
+        float w[guide::kLobes], kap[guide::kLobes];
+        float acc = 0.0f, prev = 0.0f;
 #pragma unroll
-        for (int k = 0; k < guide::kLobes; ++k) lobes[static_cast<size_t>(k) * P + p] = m.lobe[k];
-        lobeWeights[p] = make_float4(m.weight[0], m.weight[1], m.weight[2], m.weight[3]);
-        lobeWeights[static_cast<size_t>(P) + p] = make_float4(m.weight[4], m.weight[5], m.weight[6], m.weight[7]);
-        lobeScales[p] = make_float4(m.scale[0], m.scale[1], m.scale[2], m.scale[3]);
-        lobeScales[static_cast<size_t>(P) + p] = make_float4(m.scale[4], m.scale[5], m.scale[6], m.scale[7]);
+        for (int k = 0; k < guide::kLobes; ++k) {
+            const float4 l = m.lobe[k];
+            lobes[static_cast<size_t>(k) * P + p] = make_uint2(packHalf2(l.x, l.y), packHalf2(l.z, l.w));
+            kap[k] = unpackHalf2(packHalf2(l.w, 0.0f)).x;
+            w[k] = unpackHalf2(packHalf2(m.weight[k], 0.0f)).x;
+        }
+        lobeWeights[p] = make_uint2(packHalf2(w[0], w[1]), packHalf2(w[2], w[3]));
+        lobeWeights[static_cast<size_t>(P) + p] = make_uint2(packHalf2(w[4], w[5]), packHalf2(w[6], w[7]));
+        float sc[guide::kLobes];
+#pragma unroll
+        for (int k = 0; k < guide::kLobes; ++k) {
+            acc += w[k];
+            const float cum = k == guide::kLobes - 1 ? 1.0f : fminf(acc, 1.0f);
+            const float prob = fmaxf(cum - prev, 0.0f);
+            prev = fmaxf(prev, cum);
+            sc[k] = prob * expf(guide::vmfLogNorm(kap[k]));
+        }
+        lobeScales[p] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+        lobeScales[static_cast<size_t>(P) + p] = make_float4(sc[4], sc[5], sc[6], sc[7]);
     }
 };
 
@@ -636,8 +671,8 @@ void carvePathBuffers(void* base, uint32_t P, PathBuffers* pb) {
 
 size_t guideBufferBytes(uint32_t P, uint32_t recBounces, uint32_t sampleCapacity) {
     size_t b = 0;
-    b += a256(size_t(P) * 16 * guide::kLobes);
-    b += a256(size_t(P) * 16 * 2) * 2;
+    b += a256(size_t(P) * 8 * guide::kLobes);
+    b += a256(size_t(P) * 8 * 2) + a256(size_t(P) * 16 * 2);
     b += a256(size_t(P) * 16 * kRecFields * recBounces);
     b += a256(size_t(P) * 4 * recBounces);
     b += a256(size_t(sampleCapacity) * sizeof(guide::Sample));
@@ -648,8 +683,8 @@ size_t guideBufferBytes(uint32_t P, uint32_t recBounces, uint32_t sampleCapacity
 void carveGuideBuffers(void* base, uint32_t P, uint32_t recBounces, uint32_t sampleCapacity, GuideFrame* gf) {
     char* s = static_cast<char*>(base);
     auto take = [&](size_t bytes) { char* r = s; s += a256(bytes); return r; };
-    gf->lobes = reinterpret_cast<float4*>(take(size_t(P) * 16 * guide::kLobes));
-    gf->lobeWeights = reinterpret_cast<float4*>(take(size_t(P) * 16 * 2));
+    gf->lobes = reinterpret_cast<uint2*>(take(size_t(P) * 8 * guide::kLobes));
+    gf->lobeWeights = reinterpret_cast<uint2*>(take(size_t(P) * 8 * 2));
     gf->lobeScales = reinterpret_cast<float4*>(take(size_t(P) * 16 * 2));
     gf->rec = reinterpret_cast<float4*>(take(size_t(P) * 16 * kRecFields * recBounces));
     gf->recStamp = reinterpret_cast<uint32_t*>(take(size_t(P) * 4 * recBounces));

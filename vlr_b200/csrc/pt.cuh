@@ -79,9 +79,9 @@ struct GuideFrame {
     bool record;
     uint32_t recBounces;
     guide::Net net;
-    float4* lobes;             // [kLobes][P]  (mu, kappa)
-    float4* lobeWeights;       // [2][P]       mixture weights
-    float4* lobeScales;        // [2][P]       weight x vMF normalisation
+    uint2* lobes;              // [kLobes][P]  (mu, kappa) as 4 halves
+    uint2* lobeWeights;        // [2][P]       mixture weights, 4 halves each
+    float4* lobeScales;        // [2][P]       sampling probability x vMF normalisation (FP32)
     float4* rec;               // [recBounces][kRecFields][P]
     uint32_t* recStamp;        // [recBounces][P] launch stamp once a record is complete
     guide::Sample* samples;    // training-sample buffer

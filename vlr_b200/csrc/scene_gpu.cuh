@@ -122,12 +122,16 @@ struct SurfPt {
 
 // Instantiate the BSDF of material m at the given wavelengths (the setupBSDF
 // callables of materials.cu with immediate values).
+// K >= 0: the material is known to be of that kind (the shade kernels
+// specialised per material queue), which lets every BSDF dispatch fold.
+template <int K = -1>
 VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
     Bsdf B;
-    B.kind = m.bsdfKind;
+    const uint32_t kind = K >= 0 ? static_cast<uint32_t>(K) : m.bsdfKind;
+    B.kind = kind;
     B.flags = 0;
     B.f0 = m.f[0]; B.f1 = m.f[1]; B.f2 = m.f[2];
-    switch (m.bsdfKind) {
+    switch (kind) {
     case kMatte:
     case kLambertianBSDF:
         B.a = mengEvaluate(T, m.sp[0], wls);
@@ -138,8 +142,8 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
         B.a = mengEvaluate(T, m.sp[0], wls);
         B.b = mengEvaluate(T, m.sp[1], wls);
         B.c = mengEvaluate(T, m.sp[2], wls);
-        if (m.bsdfKind == kSpecularBSDF) B.flags = wls.single ? 0u : 1u;
-        if (m.bsdfKind == kMicrofacetBSDF) B.flags = m.bsdfFlags & kBsdfConsistentPdf;
+        if (kind == kSpecularBSDF) B.flags = wls.single ? 0u : 1u;
+        if (kind == kMicrofacetBSDF) B.flags = m.bsdfFlags & kBsdfConsistentPdf;
         break;
     case kMicrofacetBRDF:
         B.b = mengEvaluate(T, m.sp[1], wls);

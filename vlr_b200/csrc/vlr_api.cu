@@ -1262,6 +1262,8 @@ VLRResult vlrbContextSetGuiding(VLRContext context, const VLRBGuidingOptions* o)
     g.stepsPerLaunch = o->stepsPerLaunch;
     g.recordBounces = o->recordBounces;
     g.warmupLaunches = o->warmupLaunches;
+    g.weightClamp = o->weightClamp;
+    g.trainInterval = o->trainInterval;
     return VLRResult_NoError;
 }
 
@@ -1270,7 +1272,8 @@ VLRResult vlrbContextGetGuiding(VLRContext context, VLRBGuidingOptions* o) {
     if (!o) return VLRResult_InvalidArgument;
     const GuidingOptions &g = c->guiding;
     *o = VLRBGuidingOptions{ g.enabled, g.train, g.log2TableSize, g.learningRate, g.samplesPerStep,
-                             g.stepsPerLaunch, g.recordBounces, g.warmupLaunches };
+                             g.stepsPerLaunch, g.recordBounces, g.warmupLaunches, g.weightClamp,
+                             g.trainInterval };
     return VLRResult_NoError;
 }
 

@@ -87,8 +87,11 @@ FLOAT_SLOTS = {"MicrofacetReflection": ("roughness", "anisotropy", "rotation"),
 FLOAT_DEFAULTS = {"roughness": 0.1, "anisotropy": 0.0, "rotation": 0.0, "f0": 0.04, "metallic": 0.0}
 
 
-def cornell_box_desc(width=512, height=512, glass="box", light_scale=1.0, emittance=15.0):
-    """Plain description of the Cornell box workload (see module doc)."""
+def cornell_box_desc(width=512, height=512, glass="box", light_scale=1.0, emittance=15.0, light_up=False):
+    """Plain description of the Cornell box workload (see module doc).
+    light_up: the light hangs at 2.4 facing the ceiling, so the room is lit
+    only by the bright ceiling patch above it (indirect light that next-event
+    estimation cannot reach)."""
     srgb = "Rec709(D65) sRGB Gamma"
     lin = "Rec709(D65)"
     mats = {
@@ -109,7 +112,10 @@ def cornell_box_desc(width=512, height=512, glass="box", light_scale=1.0, emitta
     v += _quad((-1.5, 0, 1.5), (-1.5, 0, -1.5), (-1.5, 3, -1.5), (-1.5, 3, 1.5), (1, 0, 0), (0, 0, -1))   # left
     v += _quad((1.5, 0, -1.5), (1.5, 0, 1.5), (1.5, 3, 1.5), (1.5, 3, -1.5), (-1, 0, 0), (0, 0, 1))       # right
     hl = 0.5 * math.sqrt(light_scale)
-    v += _quad((-hl, 2.9, -hl), (hl, 2.9, -hl), (hl, 2.9, hl), (-hl, 2.9, hl), (0, -1, 0), (1, 0, 0))     # light
+    if light_up:
+        v += _quad((-hl, 2.4, -hl), (-hl, 2.4, hl), (hl, 2.4, hl), (hl, 2.4, -hl), (0, 1, 0), (1, 0, 0))  # light, up
+    else:
+        v += _quad((-hl, 2.9, -hl), (hl, 2.9, -hl), (hl, 2.9, hl), (-hl, 2.9, hl), (0, -1, 0), (1, 0, 0))  # light
     meshes = [{"name": "CornellBox", "verts": np.array(v, np.float32), "groups": [
         (np.array([0, 1, 2, 0, 2, 3, 4, 5, 6, 4, 6, 7, 8, 9, 10, 8, 10, 11], np.uint32), "white"),
         (np.array([12, 13, 14, 12, 14, 15], np.uint32), "red"),
@@ -154,8 +160,8 @@ def build(ctx, desc):
     return scene, cam, keep
 
 
-def cornell_box(ctx, width=512, height=512, glass="box", light_scale=1.0, emittance=15.0):
-    return build(ctx, cornell_box_desc(width, height, glass, light_scale, emittance))
+def cornell_box(ctx, width=512, height=512, glass="box", light_scale=1.0, emittance=15.0, light_up=False):
+    return build(ctx, cornell_box_desc(width, height, glass, light_scale, emittance, light_up))
 
 
 MAT_DTYPE = np.dtype([("type", "<i4"), ("colorSpace", "<i4", 3), ("spectra", "<f4", (3, 3)),

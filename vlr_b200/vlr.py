@@ -49,7 +49,8 @@ class VLRBGuidingOptions(ctypes.Structure):
     _fields_ = [("enabled", ctypes.c_bool), ("train", ctypes.c_bool), ("log2TableSize", ctypes.c_uint32),
                 ("learningRate", ctypes.c_float), ("samplesPerStep", ctypes.c_uint32),
                 ("stepsPerLaunch", ctypes.c_uint32), ("recordBounces", ctypes.c_uint32),
-                ("warmupLaunches", ctypes.c_uint32)]
+                ("warmupLaunches", ctypes.c_uint32), ("weightClamp", ctypes.c_float),
+                ("trainInterval", ctypes.c_uint32)]
 
 
 class VLRBGuidingStats(ctypes.Structure):
@@ -355,7 +356,7 @@ class Context:
     def setGuiding(self, enabled=None, train=None, **kw):
         """vlrbContextSetGuiding; keyword names are the C struct's fields
         (log2TableSize, learningRate, samplesPerStep, stepsPerLaunch,
-        recordBounces, warmupLaunches)."""
+        recordBounces, warmupLaunches, weightClamp, trainInterval)."""
         o = VLRBGuidingOptions()
         check(_api().vlrbContextGetGuiding(self.h, ctypes.byref(o)), "getGuiding")
         if enabled is not None:
