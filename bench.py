@@ -336,7 +336,7 @@ def bsdf_batch_workload(hbm_peak):
     return out
 
 
-def terrain_workloads():
+def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt")):
     """Path tracing and LVC-BPT on the 2,097,152-triangle terrain with 4096
     instanced icospheres under the 2048x1024 sky (FP64 CDF), 1920x1080,
     max depth 12; device-timed segments/s after warm-up."""
@@ -346,6 +346,8 @@ def terrain_workloads():
     desc = scenes.terrain_scene_desc(W, H)
     out = {}
     for name, renderer, spp in (("terrain_pt", V.RENDERER_PATH_TRACING, 8), ("terrain_lvc_bpt", V.RENDERER_BPT, 4)):
+        if name not in names:
+            continue
         ctx = V.Context()
         ctx.bindOutputBuffer(W, H)
         scene, cam, keep = scenes.build_instanced(ctx, desc)
@@ -372,6 +374,50 @@ def terrain_workloads():
             out[name]["light_vertex_overflow"] = st["lightVertexOverflow"]
         ctx.close()
     return out
+
+
+def glossy_guided_workload():
+    """Guided path tracing with online training on the Cornell box with the
+    20,022-triangle GGX dielectric sphere and the light at 0.1x area,
+    1024x1024, max path length 8, consistent dielectric pdf: 16 spp of
+    warm-up training, then 16 spp in 4 launches timed per stage (the
+    workload of the guiding-kernel profiles)."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    W = H = 1024
+    ctx = V.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = scenes.cornell_box(ctx, W, H, glass="sphere", light_scale=0.1)
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=8, max_paths_in_flight=1 << 22, consistent_dielectric_pdf=True)
+    ctx.setGuiding(enabled=True, train=True)
+    ctx.render_samples(cam, True, 16)
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.kernel_times(reset=True)
+    s0 = ctx.stats()
+    ctx.render_samples(cam, False, 16)
+    torch.cuda.synchronize()
+    stages, _ = ctx.kernel_times(reset=True)
+    s1 = ctx.stats()
+    ctx.set_profiling(False)
+    seg = s1["pathSegments"] - s0["pathSegments"]
+    total_ms = sum(v["ms"] for v in stages.values())
+    out = {"workload": "guided PT with online training, Cornell box with GGX dielectric sphere, light 0.1x, "
+                       "1024x1024, 16 spp, max path length 8",
+           "segments_per_s": seg / (total_ms * 1e-3) / 1e9, "unit": "G path segments/s",
+           "stage_ms": {k: v["ms"] for k, v in stages.items()}, "guiding": ctx.guiding_stats()}
+    ctx.close()
+    return out
+
+
+WORKLOADS = {
+    "bsdf_batch": lambda: {"bsdf_batch": bsdf_batch_workload(measured_peaks()[0])},
+    "terrain_pt": lambda: terrain_workloads(("terrain_pt",)),
+    "terrain_lvc_bpt": lambda: terrain_workloads(("terrain_lvc_bpt",)),
+    "multi_scene_batch": lambda: {"multi_scene_batch": batch_workload()},
+    "glossy_guided": lambda: {"glossy_guided": glossy_guided_workload()},
+}
 
 
 def batch_workload():
@@ -468,6 +514,11 @@ def batch_workload():
 #          + next-queue append 4 + shadow ray 48                      = 412 B / hit
 #   shadow: shadow ray 48 + contribution read-modify-write 32        = 80 B / shadow ray
 STAGE_BYTES = {"trace": 56, "shade": 412, "shadow": 80}
+# DRAM bytes per unit measured on this workload: dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the 128 launches of each stage in one
+# 256-spp step (ncu, one pass), divided by that step's 149,342,553 segments
+# (trace, shade) or per segment as well for shadow.
+STAGE_DRAM_BYTES_PER_SEGMENT = {"trace": 68.33, "shade": 369.95, "shadow": 38.22}
 
 
 def main():
@@ -479,11 +530,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-1%%-error measurement")
     ap.add_argument("--no-workloads", action="store_true", help="skip the BSDF-batch and terrain workloads")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS),
+                    help="run only this secondary workload and print its JSON line (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(WORKLOADS[args.workload]()), flush=True)
+        return
 
     import torch
     import torch.distributed as dist
@@ -578,14 +636,8 @@ def main():
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
                 "peak_source": peak_kind,
                 "stage_ms_per_step": {k: v["ms"] / 2 for k, v in stages.items()}}
-    prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(prof):
-        try:
-            tr = json.load(open(prof)).get(dominant)
-            if tr:
-                roofline["traffic"] = tr["bytes_per_unit"] * units[dominant] / max(st["launches"], 1)
-        except Exception:
-            pass
+    roofline["traffic"] = STAGE_DRAM_BYTES_PER_SEGMENT[dominant] * rays / max(st["launches"], 1)
+    roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum per segment on this workload"
 
     workloads = None
     if rank == 0 and world == 1 and not args.no_workloads:
