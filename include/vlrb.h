@@ -81,6 +81,8 @@ typedef struct VLRBRenderOptions {
                                      through exits; 1: pdf consistent with the sampled
                                      density and the value (unbiased MIS) */
     uint32_t blocksPerSM;         /* grid of the wavefront kernels = SMs x this (0 = 8) */
+    uint32_t bvhTreeletRounds;    /* treelet restructuring rounds after the LBVH build
+                                     (vlrbBvhBuildOptimizedHost), 0..8; default 3 */
 } VLRBRenderOptions;
 
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options);
@@ -170,6 +172,16 @@ VLRResult vlrbContextGetOutputDevicePointer(VLRContext context, void** devicePtr
  * ---------------------------------------------------------------------- */
 VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
                            int32_t* children, float* nodeBoxes, float* buildMs);
+
+/* The LBVH build followed by `treeletRounds` rounds of treelet restructuring
+ * (7-leaf treelets, least-SAH topology by dynamic programming; the hierarchy
+ * the renderer traverses, VLRBRenderOptions::bvhTreeletRounds).  Same outputs
+ * as vlrbBvhBuildHost, children and nodeBoxes after restructuring;
+ * restructured (may be NULL) receives the number of treelets rebuilt.
+ * treeletRounds = 0 is vlrbBvhBuildHost. */
+VLRResult vlrbBvhBuildOptimizedHost(const float* triVerts, uint32_t n, uint32_t treeletRounds,
+                                    uint32_t* sortedCodes, uint32_t* sortedPrims, int32_t* children,
+                                    float* nodeBoxes, uint32_t* restructured, float* buildMs);
 
 /* ------------------------------------------------------------------------
  * The same LBVH build with caller-owned DEVICE buffers that allocates no

@@ -152,3 +152,191 @@ int oracle_lbvh_build(const float* verts, uint32_t n, uint32_t* sortedCodes, uin
     free(parent);
     return 0;
 }
+
+/* ---- treelet restructuring (Karras and Aila, "Fast Parallel Construction
+ * of High-Quality Bounding Volume Hierarchies", HPG 2013), restated
+ * sequentially for the GPU pass in vlr_b200/csrc/lbvh.cu: per round
+ * (gamma = 7, 14, 28, ...), every internal node in post-order gets its SAH
+ * cost (1.2 x area for a node, 1.0 x area for a triangle) and triangle count
+ * from its children; a node with >= gamma triangles roots a treelet of up to
+ * 7 leaves, grown by opening the leaf of largest area (first of equals), and
+ * the treelet is rebuilt with the least-cost topology from a dynamic program
+ * over its leaf subsets when that is below 0.9999 x its current cost.  The
+ * new inner nodes take the treelet's node indices in breadth-first order of
+ * their subsets, the root keeping its own. */
+typedef struct { int ref; float lo[3], hi[3]; float cost; uint32_t count; } TLeaf;
+
+static float boxArea(const float lo[3], const float hi[3]) {
+    float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    float s = dx * dy + dy * dz;
+    s = s + dz * dx;
+    return 2.0f * s;
+}
+
+static void refBox(const float* verts, const uint32_t* prims, const float* nodeBoxes, int ref, float lo[3],
+                   float hi[3]) {
+    if (ref >= 0) {
+        for (int a = 0; a < 3; ++a) { lo[a] = nodeBoxes[6 * ref + a]; hi[a] = nodeBoxes[6 * ref + 3 + a]; }
+        return;
+    }
+    const float* p = verts + 9 * (size_t)prims[~ref];
+    for (int a = 0; a < 3; ++a) {
+        float m0 = p[a] < p[3 + a] ? p[a] : p[3 + a];
+        float M0 = p[a] > p[3 + a] ? p[a] : p[3 + a];
+        lo[a] = m0 < p[6 + a] ? m0 : p[6 + a];
+        hi[a] = M0 > p[6 + a] ? M0 : p[6 + a];
+    }
+}
+
+static TLeaf makeLeaf(const float* verts, const uint32_t* prims, const float* nodeBoxes, const float* cost,
+                      const uint32_t* count, int ref) {
+    TLeaf t;
+    t.ref = ref;
+    refBox(verts, prims, nodeBoxes, ref, t.lo, t.hi);
+    if (ref >= 0) { t.cost = cost[ref]; t.count = count[ref]; }
+    else { t.cost = 1.0f * boxArea(t.lo, t.hi); t.count = 1; }
+    return t;
+}
+
+static void unionBox(const TLeaf* L, int nl, int s, float lo[3], float hi[3]) {
+    int first = 1;
+    for (int i = 0; i < nl; ++i) {
+        if (!((s >> i) & 1)) continue;
+        for (int a = 0; a < 3; ++a) {
+            if (first) { lo[a] = L[i].lo[a]; hi[a] = L[i].hi[a]; }
+            else {
+                lo[a] = L[i].lo[a] < lo[a] ? L[i].lo[a] : lo[a];
+                hi[a] = L[i].hi[a] > hi[a] ? L[i].hi[a] : hi[a];
+            }
+        }
+        first = 0;
+    }
+}
+
+static float treelet(const float* verts, const uint32_t* prims, int32_t* children, float* nodeBoxes, float* cost,
+                     uint32_t* count, int root, float rootCost, uint32_t* restructured) {
+    TLeaf L[7];
+    int inner[6];
+    int nl = 2, ni = 0;
+    inner[ni++] = root;
+    L[0] = makeLeaf(verts, prims, nodeBoxes, cost, count, children[2 * root]);
+    L[1] = makeLeaf(verts, prims, nodeBoxes, cost, count, children[2 * root + 1]);
+    while (nl < 7) {
+        int best = -1;
+        float bestArea = -1.0f;
+        for (int j = 0; j < nl; ++j) {
+            if (L[j].ref < 0) continue;
+            float a = boxArea(L[j].lo, L[j].hi);
+            if (a > bestArea) { bestArea = a; best = j; }
+        }
+        if (best < 0) break;
+        int x = L[best].ref;
+        inner[ni++] = x;
+        L[best] = makeLeaf(verts, prims, nodeBoxes, cost, count, children[2 * x]);
+        L[nl++] = makeLeaf(verts, prims, nodeBoxes, cost, count, children[2 * x + 1]);
+    }
+    const int full = (1 << nl) - 1;
+    float A[128], C[128];
+    uint8_t P[128];
+    for (int s = 1; s <= full; ++s) {
+        float lo[3], hi[3];
+        unionBox(L, nl, s, lo, hi);
+        A[s] = boxArea(lo, hi);
+    }
+    for (int i = 0; i < nl; ++i) C[1 << i] = L[i].cost;
+    for (int s = 1; s <= full; ++s) {
+        if ((s & (s - 1)) == 0) continue;
+        int low = s & -s;
+        float best = 3.402823466e+38f;
+        int bp = 0;
+        for (int p = (s - 1) & s; p; p = (p - 1) & s) {
+            if (!(p & low)) continue;
+            float c = C[p] + C[s ^ p];
+            if (c < best) { best = c; bp = p; }
+        }
+        C[s] = 1.2f * A[s] + best;
+        P[s] = (uint8_t)bp;
+    }
+    if (!(C[full] < rootCost * 0.9999f)) return rootCost;
+    int qs[6], qn[6], qh = 0, qt = 0, next = 1;
+    qs[qt] = full; qn[qt] = root; ++qt;
+    while (qh < qt) {
+        int s = qs[qh], x = qn[qh];
+        ++qh;
+        int part[2] = { P[s], s ^ P[s] };
+        float lo[2][3], hi[2][3];
+        uint32_t cnt = 0;
+        for (int k = 0; k < 2; ++k) {
+            int q = part[k], ref;
+            unionBox(L, nl, q, lo[k], hi[k]);
+            if ((q & (q - 1)) == 0) {
+                int i = __builtin_ctz((unsigned)q);
+                ref = L[i].ref;
+                cnt += L[i].count;
+            }
+            else {
+                ref = inner[next++];
+                qs[qt] = q; qn[qt] = ref; ++qt;
+                for (int i = 0; i < nl; ++i) if ((q >> i) & 1) cnt += L[i].count;
+            }
+            children[2 * x + k] = ref;
+        }
+        for (int a = 0; a < 3; ++a) {
+            nodeBoxes[6 * x + a] = lo[0][a] < lo[1][a] ? lo[0][a] : lo[1][a];
+            nodeBoxes[6 * x + 3 + a] = hi[0][a] > hi[1][a] ? hi[0][a] : hi[1][a];
+        }
+        cost[x] = C[s];
+        count[x] = cnt;
+    }
+    ++*restructured;
+    return C[full];
+}
+
+/* children/nodeBoxes: an LBVH from oracle_lbvh_build, modified in place.
+ * Returns the number of treelets rebuilt, or -1. */
+int oracle_lbvh_optimize(const float* verts, uint32_t n, const uint32_t* sortedPrims, int32_t* children,
+                         float* nodeBoxes, uint32_t rounds) {
+    if (n < 3 || rounds == 0) return 0;
+    const int N = (int)n;
+    float* cost = (float*)malloc(sizeof(float) * (size_t)N);
+    uint32_t* count = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)N);
+    int32_t* order = (int32_t*)malloc(sizeof(int32_t) * (size_t)N);
+    int32_t* stack = (int32_t*)malloc(sizeof(int32_t) * (size_t)N * 2);
+    uint8_t* seen = (uint8_t*)malloc((size_t)N);
+    if (!cost || !count || !order || !stack || !seen) return -1;
+    uint32_t restructured = 0, gamma = 7;
+    for (uint32_t r = 0; r < rounds; ++r, gamma *= 2) {
+        memset(seen, 0, (size_t)N);
+        int sp = 0, no = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            int x = stack[sp - 1];
+            if (!seen[x]) {
+                seen[x] = 1;
+                for (int k = 0; k < 2; ++k) if (children[2 * x + k] >= 0) stack[sp++] = children[2 * x + k];
+                continue;
+            }
+            --sp;
+            order[no++] = x;
+        }
+        for (int k = 0; k < no; ++k) {
+            int x = order[k];
+            TLeaf a = makeLeaf(verts, sortedPrims, nodeBoxes, cost, count, children[2 * x]);
+            TLeaf b = makeLeaf(verts, sortedPrims, nodeBoxes, cost, count, children[2 * x + 1]);
+            float lo[3], hi[3];
+            for (int q = 0; q < 3; ++q) {
+                lo[q] = a.lo[q] < b.lo[q] ? a.lo[q] : b.lo[q];
+                hi[q] = a.hi[q] > b.hi[q] ? a.hi[q] : b.hi[q];
+            }
+            float c = 1.2f * boxArea(lo, hi) + a.cost;
+            c = c + b.cost;
+            uint32_t cnt = a.count + b.count;
+            if (cnt >= gamma)
+                c = treelet(verts, sortedPrims, children, nodeBoxes, cost, count, x, c, &restructured);
+            cost[x] = c;
+            count[x] = cnt;
+        }
+    }
+    free(cost); free(count); free(order); free(stack); free(seen);
+    return (int)restructured;
+}

@@ -141,3 +141,83 @@ def test_lbvh_oracle_structure():
     # root box contains every triangle
     tri = v.reshape(n, 3, 3)
     assert np.all(boxes[0:3] <= tri.min(axis=(0, 1))) and np.all(boxes[3:6] >= tri.max(axis=(0, 1)))
+
+
+def _sah(ch, boxes, v, prims):
+    """SAH cost (1.2 per node area, 1.0 per triangle box area) over the root area."""
+    n = len(prims)
+    tri = v.reshape(n, 3, 3)[prims]
+    tlo, thi = tri.min(axis=1), tri.max(axis=1)
+    area = lambda lo, hi: 2 * ((hi - lo)[..., 0] * (hi - lo)[..., 1] + (hi - lo)[..., 1] * (hi - lo)[..., 2]
+                               + (hi - lo)[..., 2] * (hi - lo)[..., 0])
+    b = boxes.reshape(-1, 6).astype(np.float64)
+    return (1.2 * area(b[:, :3], b[:, 3:]).sum() + area(tlo, thi).sum()) / area(b[0, :3], b[0, 3:])
+
+
+def _closest_hits(v, prims, ch, boxes, rays):
+    """Closest hit per ray by walking every box the ray meets (no ordering)."""
+    n = len(prims)
+    tri = v.reshape(n, 3, 3).astype(np.float64)
+    b = boxes.reshape(-1, 6).astype(np.float64)
+    out = []
+    for o, d in rays:
+        inv = 1.0 / d
+        best, hit = np.inf, -1
+        stack = [0]
+        while stack:
+            x = stack.pop()
+            for c in (ch[2 * x], ch[2 * x + 1]):
+                if c >= 0:
+                    t0, t1 = (b[c, :3] - o) * inv, (b[c, 3:] - o) * inv
+                    if max(np.minimum(t0, t1).max(), 0.0) <= min(np.maximum(t0, t1).min(), best):
+                        stack.append(c)
+                else:
+                    a, p1, p2 = tri[prims[~c]]
+                    e1, e2 = p1 - a, p2 - a
+                    p = np.cross(d, e2)
+                    det = e1 @ p
+                    if det == 0:
+                        continue
+                    s = o - a
+                    u = (s @ p) / det
+                    q = np.cross(s, e1)
+                    w = (d @ q) / det
+                    t = (e2 @ q) / det
+                    if u >= 0 and w >= 0 and u + w <= 1 and 0 < t < best:
+                        best, hit = t, int(prims[~c])
+        out.append(hit)
+    return out
+
+
+def test_treelet_oracle_keeps_the_tree_valid_and_lowers_its_sah_cost():
+    """Treelet restructuring (host restatement): still a binary tree over the
+    same leaves, every node box the union of its children's, a lower SAH cost,
+    and the same closest hits as the LBVH it started from."""
+    rng = np.random.default_rng(5)
+    n = 3000
+    scale = np.exp(rng.uniform(-4, 0, (n, 1, 1)))
+    v = (rng.uniform(-1, 1, (n, 1, 3)) + 0.1 * scale * rng.normal(0, 1, (n, 3, 3))).astype(np.float32).reshape(n, 9)
+    codes, prims, ch, boxes = lbvh.build_lbvh(v)
+    och, obx, nr = lbvh.optimize_lbvh(v, prims, ch, boxes, 3)
+    assert nr > 0
+    assert sorted((~c) for c in och if c < 0) == list(range(n))
+    assert sorted(c for c in och if c >= 0) == list(range(1, n - 1))
+    tri = v.reshape(n, 3, 3)[prims]
+    cb = lambda c: (obx[6 * c:6 * c + 3], obx[6 * c + 3:6 * c + 6]) if c >= 0 else \
+        (tri[~c].min(axis=0), tri[~c].max(axis=0))
+    for x in range(n - 1):
+        (l0, h0), (l1, h1) = cb(och[2 * x]), cb(och[2 * x + 1])
+        assert np.array_equal(obx[6 * x:6 * x + 3], np.minimum(l0, l1))
+        assert np.array_equal(obx[6 * x + 3:6 * x + 6], np.maximum(h0, h1))
+    assert np.array_equal(obx[:6], boxes[:6])
+    before, after = _sah(ch, boxes, v, prims), _sah(och, obx, v, prims)
+    assert after < 0.95 * before, (before, after)
+    rays = []
+    for _ in range(150):
+        o = rng.uniform(-1.5, 1.5, 3)
+        d = rng.normal(size=3)
+        rays.append((o, d / np.linalg.norm(d)))
+    assert _closest_hits(v, prims, ch, boxes, rays) == _closest_hits(v, prims, och, obx, rays)
+    # a second call on the same input gives the same tree
+    och2, obx2, nr2 = lbvh.optimize_lbvh(v, prims, ch, boxes, 3)
+    assert np.array_equal(och, och2) and np.array_equal(obx, obx2) and nr == nr2

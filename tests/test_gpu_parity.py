@@ -101,6 +101,36 @@ def test_lbvh_bit_exact_against_host_build(n):
     assert np.array_equal(bx[: 6 * (n - 1)], hbx)
 
 
+@pytest.mark.parametrize("n,rounds", [(3, 1), (8, 3), (37, 3), (4096, 3), (100000, 3), (1 << 20, 3), (4096, 6)])
+def test_treelet_restructuring_bit_exact_against_host(n, rounds):
+    """The GPU treelet pass (one thread per treelet, bottom-up with arrival
+    counters) against its sequential host restatement: same hierarchy and
+    boxes bit for bit, same number of rebuilt treelets."""
+    L = V.lib()
+    L.vlrbBvhBuildOptimizedHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 6
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rng = np.random.default_rng(1000 + n)
+    scale = np.exp(rng.uniform(-4, 0, (n, 1, 1))).astype(np.float32)      # mixed triangle sizes
+    c = rng.uniform(-10, 10, (n, 1, 3)).astype(np.float32)
+    v = (c + scale * rng.normal(0, 1.0, (n, 3, 3))).astype(np.float32).reshape(n, 9)
+    if n >= 4096:
+        v[: n // 50] = v[0]
+    codes = np.zeros(n, np.uint32)
+    prims = np.zeros(n, np.uint32)
+    ch = np.zeros(max(2 * (n - 1), 1), np.int32)
+    bx = np.zeros(max(6 * (n - 1), 1), np.float32)
+    nr = np.zeros(1, np.uint32)
+    assert L.vlrbBvhBuildOptimizedHost(P(v), n, rounds, P(codes), P(prims), P(ch), P(bx), P(nr), None) == 0
+    hc, hp, hch, hbx = lbvh.build_lbvh(v)
+    och, obx, onr = lbvh.optimize_lbvh(v, hp, hch, hbx, rounds)
+    assert np.array_equal(prims, hp)
+    assert int(nr[0]) == onr
+    assert np.array_equal(ch[: 2 * (n - 1)], och)
+    assert np.array_equal(bx[: 6 * (n - 1)], obx)
+    if n >= 4096:
+        assert onr > 0
+
+
 def _film_xyz(film, cmf):
     return np.einsum("hwk,ck->hwc", film, cmf.astype(np.float64))
 

@@ -97,10 +97,12 @@ extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernel
     }
 }
 
-extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
-                                      int32_t* children, float* nodeBoxes, float* buildMs) {
+static VLRResult bvhBuildHost(const float* triVerts, uint32_t n, uint32_t treeletRounds, uint32_t* sortedCodes,
+                              uint32_t* sortedPrims, int32_t* children, float* nodeBoxes, uint32_t* restructured,
+                              float* buildMs) {
     if (!triVerts || !sortedCodes || !sortedPrims || (n > 1 && (!children || !nodeBoxes)))
         return VLRResult_InvalidArgument;
+    if (restructured) *restructured = 0;
     if (n == 0) return VLRResult_NoError;
     try {
         const size_t N = n;
@@ -108,9 +110,12 @@ extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_
         const size_t sizes[7] = { N * 36, N * 4, N * 4, N * 8, N * 24, N * sizeof(vlrb::BvhNode), N * sizeof(vlrb::BvhTri) };
         size_t off[7], total = 0;
         for (int i = 0; i < 7; ++i) { off[i] = total; total += a256(sizes[i]); }
-        DevBuf out, scratch;
-        if (out.alloc(total) != cudaSuccess || scratch.alloc(vlrb::lbvhScratchBytes(n)) != cudaSuccess)
+        DevBuf out, scratch, optScratch;
+        if (out.alloc(total) != cudaSuccess || scratch.alloc(vlrb::lbvhScratchBytes(n)) != cudaSuccess ||
+            optScratch.alloc(vlrb::lbvhOptimizeScratchBytes(n) + 256) != cudaSuccess)
             return VLRResult_InternalError;
+        uint32_t* dRestructured = reinterpret_cast<uint32_t*>(static_cast<char*>(optScratch.p) +
+                                                              vlrb::lbvhOptimizeScratchBytes(n));
         char* b = static_cast<char*>(out.p);
         cudaMemcpy(b + off[0], triVerts, N * 36, cudaMemcpyHostToDevice);
         vlrb::LbvhOutput lo{ reinterpret_cast<uint32_t*>(b + off[1]), reinterpret_cast<uint32_t*>(b + off[2]),
@@ -121,6 +126,7 @@ extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_
         cudaEventCreate(&e1);
         cudaEventRecord(e0, nullptr);
         vlrb::lbvhBuild(reinterpret_cast<const float*>(b + off[0]), n, scratch.p, &lo, nullptr);
+        if (treeletRounds > 0) vlrb::lbvhOptimize(n, treeletRounds, optScratch.p, &lo, dRestructured, nullptr);
         cudaEventRecord(e1, nullptr);
         cudaEventSynchronize(e1);
         float ms = 0.0f;
@@ -134,10 +140,24 @@ extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_
             cudaMemcpy(children, lo.children, (N - 1) * 8, cudaMemcpyDeviceToHost);
             cudaMemcpy(nodeBoxes, lo.nodeBoxes, (N - 1) * 24, cudaMemcpyDeviceToHost);
         }
+        if (restructured && treeletRounds > 0 && n >= 3)
+            cudaMemcpy(restructured, dRestructured, 4, cudaMemcpyDeviceToHost);
         return cudaGetLastError() == cudaSuccess ? VLRResult_NoError : VLRResult_InternalError;
     }
     catch (const std::exception &ex) {
         std::fprintf(stderr, "vlrbBvhBuildHost: %s\n", ex.what());
         return VLRResult_InternalError;
     }
+}
+
+extern "C" VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCodes, uint32_t* sortedPrims,
+                                      int32_t* children, float* nodeBoxes, float* buildMs) {
+    return bvhBuildHost(triVerts, n, 0, sortedCodes, sortedPrims, children, nodeBoxes, nullptr, buildMs);
+}
+
+extern "C" VLRResult vlrbBvhBuildOptimizedHost(const float* triVerts, uint32_t n, uint32_t treeletRounds,
+                                               uint32_t* sortedCodes, uint32_t* sortedPrims, int32_t* children,
+                                               float* nodeBoxes, uint32_t* restructured, float* buildMs) {
+    return bvhBuildHost(triVerts, n, treeletRounds, sortedCodes, sortedPrims, children, nodeBoxes, restructured,
+                        buildMs);
 }

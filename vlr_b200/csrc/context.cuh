@@ -35,6 +35,7 @@ struct RenderOptions {
     uint64_t rngSeed = 0;             // 0: 591842031321323413 (context.cpp:1176-1190)
     bool consistentDielectricPdf = false;   // see mfBsdfPDF; false = the reference's pdf
     uint32_t blocksPerSM = 8;         // wavefront kernel grid = SMs x blocksPerSM
+    uint32_t bvhTreeletRounds = 3;    // treelet restructuring rounds after the LBVH build
 };
 
 struct AutotuneTrial {

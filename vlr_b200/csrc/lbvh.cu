@@ -12,6 +12,7 @@
 #include "lbvh_build.h"
 
 #include <cuda_runtime.h>
+#include <cfloat>
 #include <stdexcept>
 #include <string>
 
@@ -277,6 +278,250 @@ __global__ void packTrisKernel(const float* verts, const uint32_t* sortedPrims, 
     tris[i] = t;
 }
 
+// ---- treelet restructuring (Karras and Aila, "Fast Parallel Construction of
+// High-Quality Bounding Volume Hierarchies", HPG 2013), one warp per
+// treelet: every internal node with at least gamma triangles below it becomes
+// the root of a treelet of up to 7 leaves (grown by opening the leaf of
+// largest surface area), and the treelet's topology is replaced by the one of
+// least SAH cost found by dynamic programming over the 127 leaf subsets.  The
+// pass runs bottom up with one arrival counter per node, so a treelet is
+// optimised after everything below it.  The result depends only on the
+// subtree below each root, not on the order the threads run in, and every
+// float operation is rounded explicitly, so the host restatement reproduces
+// it bit for bit.
+constexpr int kTreeletLeaves = 7;
+constexpr int kTreeletSubsets = 1 << kTreeletLeaves;
+constexpr float kSahNodeCost = 1.2f, kSahTriCost = 1.0f;
+
+__device__ __forceinline__ float surfaceArea(const V3 &lo, const V3 &hi) {
+    const float dx = __fsub_rn(hi.x, lo.x), dy = __fsub_rn(hi.y, lo.y), dz = __fsub_rn(hi.z, lo.z);
+    return __fmul_rn(2.0f, __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx)));
+}
+
+__device__ __forceinline__ BvhNode loadNodeCg(const BvhNode* p) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    BvhNode nd;
+    nd.lo0 = __ldcg(q + 0); nd.hi0 = __ldcg(q + 1); nd.lo1 = __ldcg(q + 2); nd.hi1 = __ldcg(q + 3);
+    return nd;
+}
+
+__global__ void parentsKernel(const int32_t* children, int n, int32_t* parentOfNode, int32_t* parentOfLeaf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    for (int k = 0; k < 2; ++k) {
+        int c = children[2 * i + k];
+        if (c >= 0 && c < n - 1) parentOfNode[c] = i;
+        else if (c < 0 && ~c < n) parentOfLeaf[~c] = i;
+    }
+    if (i == 0) parentOfNode[0] = -1;
+}
+
+struct TreeletLeaf {
+    int ref;
+    V3 lo, hi;
+    float cost;
+    uint32_t count;
+};
+
+__device__ __forceinline__ TreeletLeaf treeletLeaf(int ref, const float4 &lo, const float4 &hi, const float* cost,
+                                                   const uint32_t* count) {
+    TreeletLeaf t;
+    t.ref = ref;
+    t.lo = V3(lo.x, lo.y, lo.z);
+    t.hi = V3(hi.x, hi.y, hi.z);
+    if (ref >= 0) { t.cost = __ldcg(cost + ref); t.count = __ldcg(count + ref); }
+    else { t.cost = __fmul_rn(kSahTriCost, surfaceArea(t.lo, t.hi)); t.count = 1u; }
+    return t;
+}
+
+__device__ __forceinline__ void subsetBox(const TreeletLeaf* L, int nl, int s, V3* lo, V3* hi) {
+    bool first = true;
+    for (int i = 0; i < nl; ++i) {
+        if (!((s >> i) & 1)) continue;
+        if (first) { *lo = L[i].lo; *hi = L[i].hi; first = false; }
+        else { *lo = vmin3(*lo, L[i].lo); *hi = vmax3(*hi, L[i].hi); }
+    }
+}
+
+// Per-warp dynamic-programming tables in shared memory.
+struct TreeletTables {
+    float area[kTreeletSubsets];
+    float cost[kTreeletSubsets];
+    uint8_t split[kTreeletSubsets];
+};
+
+// Optimises the treelet rooted at `root` (cost `rootCost` with its current
+// topology) with the whole warp: every lane forms the same treelet, the lanes
+// share the subsets of each size of the dynamic program, and lane `owner`
+// writes the new topology.  Returns the root's cost afterwards (the same in
+// every lane).  All control flow is warp-uniform.
+__device__ float warpTreelet(int root, float rootCost, int owner, int n, int32_t* children, float* nodeBox,
+                             BvhNode* nodes, float* cost, uint32_t* count, uint32_t* restructured,
+                             TreeletTables &T) {
+    const int lane = threadIdx.x & 31;
+    const BvhNode rootNode = loadNodeCg(nodes + root);
+    TreeletLeaf L[kTreeletLeaves];
+    int inner[kTreeletLeaves - 1];
+    int nl = 2, ni = 0;
+    inner[ni++] = root;
+    L[0] = treeletLeaf(__float_as_int(rootNode.lo0.w), rootNode.lo0, rootNode.hi0, cost, count);
+    L[1] = treeletLeaf(__float_as_int(rootNode.lo1.w), rootNode.lo1, rootNode.hi1, cost, count);
+    while (nl < kTreeletLeaves) {
+        int best = -1;
+        float bestArea = -1.0f;
+        for (int j = 0; j < nl; ++j) {
+            if (L[j].ref < 0) continue;
+            const float a = surfaceArea(L[j].lo, L[j].hi);
+            if (a > bestArea) { bestArea = a; best = j; }
+        }
+        if (best < 0) break;
+        const int x = L[best].ref;
+        if (x >= n - 1) return rootCost;
+        const BvhNode xn = loadNodeCg(nodes + x);
+        const int x0 = __float_as_int(xn.lo0.w), x1 = __float_as_int(xn.lo1.w);
+        if (x0 >= n - 1 || x1 >= n - 1 || ~x0 >= n || ~x1 >= n) return rootCost;
+        inner[ni++] = x;
+        L[best] = treeletLeaf(x0, xn.lo0, xn.hi0, cost, count);
+        L[nl++] = treeletLeaf(x1, xn.lo1, xn.hi1, cost, count);
+    }
+    const int full = (1 << nl) - 1;
+    for (int s = lane + 1; s <= full; s += 32) {
+        V3 lo, hi;
+        subsetBox(L, nl, s, &lo, &hi);
+        T.area[s] = surfaceArea(lo, hi);
+    }
+    for (int i = 0; i < nl; ++i)
+        if (lane == i) T.cost[1 << i] = L[i].cost;
+    __syncwarp();
+    for (int size = 2; size <= nl; ++size) {
+        for (int s = lane + 1; s <= full; s += 32) {
+            if (__popc(s) != size) continue;
+            const int low = s & -s;
+            float best = FLT_MAX;
+            int bp = 0;
+            for (int p = (s - 1) & s; p; p = (p - 1) & s) {
+                if (!(p & low)) continue;
+                const float c = __fadd_rn(T.cost[p], T.cost[s ^ p]);
+                if (c < best) { best = c; bp = p; }
+            }
+            T.cost[s] = __fadd_rn(__fmul_rn(kSahNodeCost, T.area[s]), best);
+            T.split[s] = static_cast<uint8_t>(bp);
+        }
+        __syncwarp();
+    }
+    const float newCost = T.cost[full];
+    if (!(newCost < __fmul_rn(rootCost, 0.9999f))) { __syncwarp(); return rootCost; }
+    if (lane == owner) {
+        // New topology: subsets in breadth-first order onto the treelet's
+        // inner nodes (the root keeps its index, so its parent's reference
+        // stays valid).
+        int qs[kTreeletLeaves - 1], qn[kTreeletLeaves - 1];
+        int qh = 0, qt = 0, next = 1;
+        qs[qt] = full; qn[qt] = root; ++qt;
+        while (qh < qt) {
+            const int s = qs[qh], x = qn[qh];
+            ++qh;
+            const int part[2] = { T.split[s], s ^ T.split[s] };
+            int ref[2];
+            V3 lo[2], hi[2];
+            uint32_t cnt = 0;
+            for (int k = 0; k < 2; ++k) {
+                const int q = part[k];
+                subsetBox(L, nl, q, &lo[k], &hi[k]);
+                if ((q & (q - 1)) == 0) {
+                    const int i = __ffs(q) - 1;
+                    ref[k] = L[i].ref;
+                    cnt += L[i].count;
+                }
+                else {
+                    ref[k] = inner[next++];
+                    qs[qt] = q; qn[qt] = ref[k]; ++qt;
+                    for (int i = 0; i < nl; ++i) if ((q >> i) & 1) cnt += L[i].count;
+                }
+            }
+            children[2 * x + 0] = ref[0];
+            children[2 * x + 1] = ref[1];
+            BvhNode nd;
+            nd.lo0 = make_float4(lo[0].x, lo[0].y, lo[0].z, __int_as_float(ref[0]));
+            nd.hi0 = make_float4(hi[0].x, hi[0].y, hi[0].z, 0.0f);
+            nd.lo1 = make_float4(lo[1].x, lo[1].y, lo[1].z, __int_as_float(ref[1]));
+            nd.hi1 = make_float4(hi[1].x, hi[1].y, hi[1].z, 0.0f);
+            float4* np = reinterpret_cast<float4*>(nodes + x);
+            __stcg(np + 0, nd.lo0); __stcg(np + 1, nd.hi0); __stcg(np + 2, nd.lo1); __stcg(np + 3, nd.hi1);
+            const V3 ulo = vmin3(lo[0], lo[1]), uhi = vmax3(hi[0], hi[1]);
+            float* ob = nodeBox + 6 * x;
+            __stcg(ob + 0, ulo.x); __stcg(ob + 1, ulo.y); __stcg(ob + 2, ulo.z);
+            __stcg(ob + 3, uhi.x); __stcg(ob + 4, uhi.y); __stcg(ob + 5, uhi.z);
+            __stcg(cost + x, T.cost[s]);
+            __stcg(count + x, cnt);
+        }
+        atomicAdd(restructured, 1u);
+    }
+    __syncwarp();
+    return newCost;
+}
+
+constexpr int kTreeletThreads = 256;
+
+// One bottom-up pass, one thread per leaf climbing while it is the second
+// arrival at a node: each node's SAH cost and triangle count from its
+// children, then, for every node over >= gamma triangles, the warp optimises
+// the treelet rooted there.  The warp stays converged: lanes that have
+// stopped climbing keep helping with the others' treelets.
+__global__ void __launch_bounds__(kTreeletThreads) treeletKernel(int n, uint32_t gamma, int32_t* children,
+                                                                 float* nodeBox, BvhNode* nodes,
+                                                                 const int32_t* parentOfNode,
+                                                                 const int32_t* parentOfLeaf, uint32_t* arrivals,
+                                                                 float* cost, uint32_t* count,
+                                                                 uint32_t* restructured) {
+    __shared__ TreeletTables tables[kTreeletThreads / 32];
+    TreeletTables &T = tables[threadIdx.x >> 5];
+    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = leaf < n;
+    int node = active ? parentOfLeaf[leaf] : -1;
+    int guard = 0;
+    while (__any_sync(0xFFFFFFFFu, active)) {
+        bool work = false;
+        if (active) {
+            if (node < 0 || node >= n - 1 || guard++ >= n) active = false;
+            else {
+                __threadfence();
+                if (atomicAdd(&arrivals[node], 1u) == 0u) active = false;
+                else { __threadfence(); work = true; }
+            }
+        }
+        float c = 0.0f;
+        uint32_t cnt = 0;
+        if (work) {
+            const BvhNode nd = loadNodeCg(nodes + node);
+            const int c0 = __float_as_int(nd.lo0.w), c1 = __float_as_int(nd.lo1.w);
+            if (c0 >= n - 1 || c1 >= n - 1 || ~c0 >= n || ~c1 >= n) { work = false; active = false; }
+            else {
+                const TreeletLeaf a = treeletLeaf(c0, nd.lo0, nd.hi0, cost, count);
+                const TreeletLeaf b = treeletLeaf(c1, nd.lo1, nd.hi1, cost, count);
+                const V3 ulo = vmin3(a.lo, b.lo), uhi = vmax3(a.hi, b.hi);
+                c = __fadd_rn(__fadd_rn(__fmul_rn(kSahNodeCost, surfaceArea(ulo, uhi)), a.cost), b.cost);
+                cnt = a.count + b.count;
+            }
+        }
+        uint32_t pending = __ballot_sync(0xFFFFFFFFu, work && cnt >= gamma);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const int root = __shfl_sync(0xFFFFFFFFu, node, src);
+            const float rootCost = __shfl_sync(0xFFFFFFFFu, c, src);
+            const float nc = warpTreelet(root, rootCost, src, n, children, nodeBox, nodes, cost, count,
+                                         restructured, T);
+            if ((threadIdx.x & 31) == src) c = nc;
+        }
+        if (work) {
+            __stcg(cost + node, c);
+            __stcg(count + node, cnt);
+            node = parentOfNode[node];
+        }
+    }
+}
+
 inline void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string("lbvh ") + what + ": " + cudaGetErrorString(e));
 }
@@ -343,6 +588,38 @@ void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, c
     }
     packTrisKernel<<<blocks, tb, 0, stream>>>(verts, out->sortedPrims, n, out->tris);
     ck(cudaGetLastError(), "launch");
+}
+
+size_t lbvhOptimizeScratchBytes(uint32_t n) {
+    return 5 * align256(size_t(n) * 4) + 256;
+}
+
+void lbvhOptimize(uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out, uint32_t* restructuredDev,
+                  cudaStream_t stream) {
+    if (n < 3 || rounds == 0) return;
+    char* s = static_cast<char*>(scratch);
+    auto take = [&](size_t bytes) { char* p = s; s += align256(bytes); return p; };
+    int32_t* parentOfNode = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    int32_t* parentOfLeaf = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    uint32_t* arrivals = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    float* cost = reinterpret_cast<float*>(take(size_t(n) * 4));
+    uint32_t* count = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
+    uint32_t* restructured = restructuredDev ? restructuredDev : reinterpret_cast<uint32_t*>(take(4));
+    ck(cudaMemsetAsync(restructured, 0, 4, stream), "treelet counter");
+    const uint32_t tb = 256;
+    uint32_t gamma = kTreeletLeaves;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        ck(cudaMemsetAsync(arrivals, 0, size_t(n) * 4, stream), "arrivals");
+        ck(cudaMemsetAsync(parentOfLeaf, 0xFF, size_t(n) * 4, stream), "leaf parents");
+        ck(cudaMemsetAsync(parentOfNode, 0xFF, size_t(n) * 4, stream), "node parents");
+        parentsKernel<<<(n - 1 + tb - 1) / tb, tb, 0, stream>>>(out->children, static_cast<int>(n), parentOfNode,
+                                                                 parentOfLeaf);
+        treeletKernel<<<(n + kTreeletThreads - 1) / kTreeletThreads, kTreeletThreads, 0, stream>>>(
+            static_cast<int>(n), gamma, out->children, out->nodeBoxes, out->nodes, parentOfNode, parentOfLeaf,
+            arrivals, cost, count, restructured);
+        gamma *= 2;
+    }
+    ck(cudaGetLastError(), "treelet launch");
 }
 
 } // namespace vlrb

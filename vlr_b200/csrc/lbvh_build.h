@@ -22,4 +22,12 @@ size_t lbvhScratchBytes(uint32_t n);
 // verts: n triangles x 3 vertices x xyz, device memory.  Enqueued on stream.
 void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, cudaStream_t stream);
 
+// Treelet restructuring of a built hierarchy in place (children, nodeBoxes and
+// nodes change; codes, prims and tris do not): `rounds` bottom-up passes with
+// treelets of 7 leaves rooted at nodes over >= 7, 14, 28, ... triangles.
+// restructuredDev (device, optional) receives the number of treelets changed.
+size_t lbvhOptimizeScratchBytes(uint32_t n);
+void lbvhOptimize(uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out, uint32_t* restructuredDev,
+                  cudaStream_t stream);
+
 } // namespace vlrb

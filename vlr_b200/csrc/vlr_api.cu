@@ -1157,7 +1157,7 @@ VLRResult vlrbContextRenderSamples(VLRContext context, CUstream stream, VLRCamer
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!options || options->maxPathLength == 0 || options->maxPathLength > kMaxBounces ||
-        options->maxPathsInFlight == 0 || options->blocksPerSM > 64)
+        options->maxPathsInFlight == 0 || options->blocksPerSM > 64 || options->bvhTreeletRounds > 8)
         return VLRResult_InvalidArgument;
     c->options.blocksPerSM = options->blocksPerSM ? options->blocksPerSM : 8;
     c->options.maxPathLength = options->maxPathLength;
@@ -1166,6 +1166,10 @@ VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOption
     c->options.rngSeed = options->rngSeed;
     if (c->options.consistentDielectricPdf != (options->consistentDielectricPdf != 0)) {
         c->options.consistentDielectricPdf = options->consistentDielectricPdf != 0;
+        c->markDirty();
+    }
+    if (c->options.bvhTreeletRounds != options->bvhTreeletRounds) {
+        c->options.bvhTreeletRounds = options->bvhTreeletRounds;
         c->markDirty();
     }
     return VLRResult_NoError;
@@ -1180,6 +1184,7 @@ VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* opt
     options->rngSeed = c->options.rngSeed;
     options->consistentDielectricPdf = c->options.consistentDielectricPdf ? 1u : 0u;
     options->blocksPerSM = c->options.blocksPerSM;
+    options->bvhTreeletRounds = c->options.bvhTreeletRounds;
     return VLRResult_NoError;
 }
 

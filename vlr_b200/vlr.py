@@ -32,7 +32,8 @@ class VLRShaderNodePlug(ctypes.Structure):
 class VLRBRenderOptions(ctypes.Structure):
     _fields_ = [("maxPathLength", ctypes.c_uint32), ("maxPathsInFlight", ctypes.c_uint32),
                 ("lightPathsPerFrame", ctypes.c_uint32), ("rngSeed", ctypes.c_uint64),
-                ("consistentDielectricPdf", ctypes.c_uint32), ("blocksPerSM", ctypes.c_uint32)]
+                ("consistentDielectricPdf", ctypes.c_uint32), ("blocksPerSM", ctypes.c_uint32),
+                ("bvhTreeletRounds", ctypes.c_uint32)]
 
 
 class VLRBAutotuneTrial(ctypes.Structure):
@@ -322,7 +323,7 @@ class Context:
         check(_api().vlrContextSetRenderer(self.h, renderer), "setRenderer")
 
     def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None, rng_seed=None,
-                   consistent_dielectric_pdf=None, blocks_per_sm=None):
+                   consistent_dielectric_pdf=None, blocks_per_sm=None, bvh_treelet_rounds=None):
         o = VLRBRenderOptions()
         check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
         if max_path_length is not None:
@@ -337,6 +338,8 @@ class Context:
             o.consistentDielectricPdf = int(bool(consistent_dielectric_pdf))
         if blocks_per_sm is not None:
             o.blocksPerSM = blocks_per_sm
+        if bvh_treelet_rounds is not None:
+            o.bvhTreeletRounds = bvh_treelet_rounds
         check(_api().vlrbContextSetRenderOptions(self.h, ctypes.byref(o)), "setOptions")
 
     def autotune(self, camera, samples_per_trial=4, stream=0):
