@@ -179,6 +179,17 @@ VLRResult vlrbBvhBuildHost(const float* triVerts, uint32_t n, uint32_t* sortedCo
  * as vlrbBvhBuildHost, children and nodeBoxes after restructuring;
  * restructured (may be NULL) receives the number of treelets rebuilt.
  * treeletRounds = 0 is vlrbBvhBuildHost. */
+/* Ray queries against a hierarchy built here (the traversal the renderers
+ * use; replaces optixTrace, path_tracing.cu:89-93 and
+ * light_transport_common.h:169-172, for callers with rays of their own).
+ * triVerts as above (host); the hierarchy is the LBVH after `treeletRounds`
+ * rounds of restructuring.  rays: count x 8 floats (origin xyz, tmax,
+ * direction xyz, unused); hits: count x 4 floats (t, b1, b2, primitive index
+ * bits; 0xFFFFFFFF and t = tmax for a miss).  anyHit: stop at the first hit
+ * found.  kernelMs (may be NULL) receives the trace kernel's device time. */
+VLRResult vlrbTraceRaysHost(const float* triVerts, uint32_t n, uint32_t treeletRounds, const float* rays,
+                            uint32_t count, uint32_t anyHit, float* hits, float* kernelMs);
+
 VLRResult vlrbBvhBuildOptimizedHost(const float* triVerts, uint32_t n, uint32_t treeletRounds,
                                     uint32_t* sortedCodes, uint32_t* sortedPrims, int32_t* children,
                                     float* nodeBoxes, uint32_t* restructured, float* buildMs);

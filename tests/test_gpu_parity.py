@@ -283,3 +283,74 @@ def test_environment_lighting_bpt_matches_pt():
         means.append(y.mean())
         ctx.close()
     assert abs(means[1] / means[0] - 1) < 0.03, means
+
+
+def _trace(v, rays, rounds, any_hit):
+    L = V.lib()
+    L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                    ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    hits = np.zeros((len(rays), 4), np.float32)
+    rc = L.vlrbTraceRaysHost(P(v), len(v), rounds, P(rays), len(rays), int(any_hit), P(hits), None)
+    assert rc == 0
+    return hits[:, 0], hits[:, 3].view(np.uint32)
+
+
+def _brute_force(v, rays):
+    """Closest hit per ray over every triangle (float64 Moller-Trumbore)."""
+    tri = v.reshape(-1, 3, 3).astype(np.float64)
+    a, e1, e2 = tri[:, 0], tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
+    best_t = np.full(len(rays), np.inf)
+    best = np.full(len(rays), 0xFFFFFFFF, np.uint32)
+    for i, r in enumerate(rays.astype(np.float64)):
+        o, tmax, d = r[0:3], r[3], r[4:7]
+        p = np.cross(d, e2)
+        det = np.einsum("ij,ij->i", e1, p)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv = 1.0 / det
+            s = o - a
+            u = np.einsum("ij,ij->i", s, p) * inv
+            q = np.cross(s, e1)
+            w = (q @ d) * inv
+            t = np.einsum("ij,ij->i", e2, q) * inv
+        ok = (det != 0) & (u >= 0) & (u <= 1) & (w >= 0) & (u + w <= 1) & (t > 0) & (t < tmax)
+        if ok.any():
+            j = np.argmin(np.where(ok, t, np.inf))
+            best_t[i], best[i] = t[j], j
+    return best_t, best
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 37, 3000, 40000])
+def test_traversal_matches_brute_force(n):
+    """Closest and first hits through the plain LBVH and the restructured
+    hierarchy (vlrbTraceRaysHost) against a brute-force search over every
+    triangle: no hit lost, the same closest triangle for every ray the brute
+    force resolves away from float ties, the same hit/miss answer for the
+    any-hit query, and both hierarchies agree."""
+    rng = np.random.default_rng(500 + n)
+    scale = np.exp(rng.uniform(-3, 0, (n, 1, 1)))
+    v = (rng.uniform(-1, 1, (n, 1, 3)) + 0.2 * scale * rng.normal(0, 1, (n, 3, 3))).astype(np.float32).reshape(n, 9)
+    m = 1500
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-1.5, 1.5, (m, 3))
+    d = rng.normal(size=(m, 3))
+    aim = rng.integers(0, n, m // 2)                       # half the rays aimed at a triangle
+    d[m // 2:] = v.reshape(n, 3, 3)[aim].mean(axis=1) - rays[m // 2:, 0:3]
+    d[: m // 10, 1] = 0.0                                  # axis-parallel components
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3] = np.where(np.arange(m) % 3 == 0, 0.8, 3.4e38)   # some short rays
+    t0, p0 = _trace(v, rays, 0, False)
+    t3, p3 = _trace(v, rays, 3, False)
+    ref_t, ref_p = _brute_force(v, rays)
+    hit = ref_p != 0xFFFFFFFF
+    assert hit.sum() >= m // 4
+    for t, p in ((t0, p0), (t3, p3)):
+        assert np.sum(hit & (p == 0xFFFFFFFF)) <= 1
+        assert np.mean((p != 0xFFFFFFFF) == hit) >= 0.999
+        resolved = hit & (np.abs(t - ref_t) <= 1e-4 * np.maximum(ref_t, 1e-3))
+        assert np.mean(resolved[hit]) >= 0.995
+    same = p0 == p3
+    assert np.mean(same) >= 0.999
+    assert np.array_equal(t0[same], t3[same])
+    _, a3 = _trace(v, rays, 3, True)
+    assert np.mean((a3 != 0xFFFFFFFF) == hit) >= 0.999

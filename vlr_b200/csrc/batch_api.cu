@@ -2,6 +2,7 @@
 #include "vlrb_internal.h"
 #include "lbvh_build.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <exception>
 
@@ -146,6 +147,73 @@ static VLRResult bvhBuildHost(const float* triVerts, uint32_t n, uint32_t treele
     }
     catch (const std::exception &ex) {
         std::fprintf(stderr, "vlrbBvhBuildHost: %s\n", ex.what());
+        return VLRResult_InternalError;
+    }
+}
+
+namespace {
+__global__ void traceRaysKernel(vlrb::Bvh bvh, const float4* rays, uint32_t count, bool anyHit, float4* hits) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4 o = rays[2 * i], d = rays[2 * i + 1];
+        const vlrb::V3 org(o.x, o.y, o.z), dir(d.x, d.y, d.z);
+        const vlrb::Hit h = anyHit ? vlrb::traceBvh<true>(bvh, org, dir, o.w) : vlrb::traceBvh<false>(bvh, org, dir, o.w);
+        hits[i] = make_float4(h.t, h.b1, h.b2, __uint_as_float(h.prim));
+    }
+}
+} // namespace
+
+extern "C" VLRResult vlrbTraceRaysHost(const float* triVerts, uint32_t n, uint32_t treeletRounds, const float* rays,
+                                       uint32_t count, uint32_t anyHit, float* hits, float* kernelMs) {
+    if (!triVerts || n == 0 || (count > 0 && (!rays || !hits)) || treeletRounds > 8) return VLRResult_InvalidArgument;
+    try {
+        const size_t N = n;
+        auto a256 = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const size_t sizes[9] = { N * 36, N * 4, N * 4, N * 8, N * 24, N * sizeof(vlrb::BvhNode),
+                                  N * sizeof(vlrb::BvhTri), size_t(count) * 32 + 16, size_t(count) * 16 + 16 };
+        size_t off[10], total = 0;
+        for (int i = 0; i < 9; ++i) { off[i] = total; total += a256(sizes[i]); }
+        off[9] = total;
+        total += 256;
+        const size_t scratchBytes = std::max(vlrb::lbvhScratchBytes(n), vlrb::lbvhOptimizeScratchBytes(n));
+        DevBuf out, scratch;
+        if (out.alloc(total) != cudaSuccess || scratch.alloc(scratchBytes) != cudaSuccess)
+            return VLRResult_InternalError;
+        char* b = static_cast<char*>(out.p);
+        cudaMemset(b + off[9], 0, 256);
+        cudaMemcpy(b + off[0], triVerts, N * 36, cudaMemcpyHostToDevice);
+        if (count) cudaMemcpy(b + off[7], rays, size_t(count) * 32, cudaMemcpyHostToDevice);
+        vlrb::LbvhOutput lo{ reinterpret_cast<uint32_t*>(b + off[1]), reinterpret_cast<uint32_t*>(b + off[2]),
+                             reinterpret_cast<int32_t*>(b + off[3]), reinterpret_cast<float*>(b + off[4]),
+                             reinterpret_cast<vlrb::BvhNode*>(b + off[5]), reinterpret_cast<vlrb::BvhTri*>(b + off[6]) };
+        uint32_t* flags = reinterpret_cast<uint32_t*>(b + off[9]);
+        vlrb::lbvhBuild(reinterpret_cast<const float*>(b + off[0]), n, scratch.p, &lo, nullptr);
+        vlrb::lbvhOptimize(n, treeletRounds, scratch.p, &lo, nullptr, nullptr);
+        const vlrb::Bvh bvh{ lo.nodes, lo.tris, n, flags };
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, nullptr);
+        if (count) {
+            const uint32_t blocks = std::min<uint32_t>((count + 255) / 256, 148u * 16u);
+            traceRaysKernel<<<blocks, 256>>>(bvh, reinterpret_cast<const float4*>(b + off[7]), count, anyHit != 0,
+                                             reinterpret_cast<float4*>(b + off[8]));
+        }
+        cudaEventRecord(e1, nullptr);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (kernelMs) *kernelMs = ms;
+        if (count) cudaMemcpy(hits, b + off[8], size_t(count) * 16, cudaMemcpyDeviceToHost);
+        uint32_t err = 0;
+        cudaMemcpy(&err, flags, 4, cudaMemcpyDeviceToHost);
+        if (cudaGetLastError() != cudaSuccess || err != 0) return VLRResult_InternalError;
+        return VLRResult_NoError;
+    }
+    catch (const std::exception &ex) {
+        cudaGetLastError();
+        std::fprintf(stderr, "vlrbTraceRaysHost: %s\n", ex.what());
         return VLRResult_InternalError;
     }
 }
