@@ -227,6 +227,12 @@ VLRResult vlrbUpsampleSpectrum(uint32_t spectrumType, uint32_t colorSpace, float
  * (spectrum_types.cpp:273-322). */
 VLRResult vlrbEvaluateSpectrum(const uint32_t packed[3], const float lambdas[4], float values[4]);
 
+/* The same spectrum evaluated the way the renderers evaluate material
+ * colours: tabulated once on the 95-sample wavelength grid with its point
+ * weights and scale applied, then interpolated (equal to
+ * vlrbEvaluateSpectrum up to float rounding). */
+VLRResult vlrbEvaluateSpectrumTabulated(const uint32_t packed[3], const float lambdas[4], float values[4]);
+
 /* The CIE 1931 colour-matching functions integrated over the 16 film strata
  * (xyz[0..15] = xbar, [16..31] = ybar, [32..47] = zbar) and the Y integral
  * (spectrum_types.cpp:634-680). */

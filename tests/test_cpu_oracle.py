@@ -107,6 +107,33 @@ def test_upsampling_bit_exact_against_reference():
         assert np.array_equal(vals, rv)
 
 
+def test_tabulated_material_spectra_match_evaluate():
+    """Material colours as the renderers evaluate them (tabulated once on the
+    95-sample grid, then interpolated) against the reference's evaluate
+    order (interpolate each table point, then weight): equal to float
+    rounding, at random wavelengths including the grid ends."""
+    L = _lib()
+    L.vlrbEvaluateSpectrumTabulated.argtypes = [ctypes.c_void_p] * 3
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rng = np.random.default_rng(9)
+    packed = np.zeros(3, np.uint32)
+    a = np.zeros(4, np.float32)
+    b = np.zeros(4, np.float32)
+    worst = 0.0
+    for k in range(400):
+        st = (0, 1, 2)[k % 3]
+        rgb = rng.uniform(0, 1, 3) if st == 0 else (rng.uniform(0, 20, 3) if st == 1 else np.full(3, rng.uniform(1, 2)))
+        assert L.vlrbUpsampleSpectrum(st, 1, *map(float, rgb), P(packed)) == 0
+        lam = rng.uniform(360.0, 830.0, 4).astype(np.float32)
+        if k % 50 == 0:
+            lam[:2] = (360.0, 830.0)
+        assert L.vlrbEvaluateSpectrum(P(packed), P(lam), P(a)) == 0
+        assert L.vlrbEvaluateSpectrumTabulated(P(packed), P(lam), P(b)) == 0
+        scale = max(np.abs(a).max(), 1e-30)
+        worst = max(worst, float(np.abs(a - b).max() / scale))
+    assert worst < 1e-5, worst
+
+
 @needs_ref
 def test_oracle_bsdf_self_consistency():
     """The reference BSDFs: evaluatePDF at the sampled direction reproduces

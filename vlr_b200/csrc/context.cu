@@ -192,7 +192,7 @@ namespace {
 // material's setupMaterialDescriptor / setupBSDF pair in the reference
 // (libVLR/materials.cpp and GPU_kernels/materials.cu).
 MatDesc describeMaterial(const SurfaceMaterial* m) {
-    MatDesc d;
+    MatDesc d{};
     std::memset(&d, 0, sizeof(d));
     d.bsdfKind = kNullBSDF;
     d.emitScale = 1.0f;
@@ -441,6 +441,18 @@ void Context::buildScene(cudaStream_t stream) {
     sg.tri = upload(f.tri, stream);
     sg.triMaterial = upload(f.triMaterial, stream);
     for (MatDesc &md : f.mats) md.bsdfFlags = options.consistentDielectricPdf ? kBsdfConsistentPdf : 0u;
+    // Material spectra are immediate colours: each is tabulated once here on
+    // the 95-sample grid, so a hit interpolates one table per spectrum.
+    {
+        std::vector<float> blended(f.mats.size() * 4 * kMengSamples);
+        const MengTables hostT = hostMengTables();
+        for (size_t i = 0; i < f.mats.size(); ++i)
+            for (int k = 0; k < 4; ++k) {
+                mengBlend(hostT, k < 3 ? f.mats[i].sp[k] : f.mats[i].emit, blended.data() + (i * 4 + k) * kMengSamples);
+                f.mats[i].table[k] = static_cast<int32_t>(i * 4 + k);
+            }
+        sg.meng.blended = upload(blended, stream);
+    }
     sg.mats = upload(f.mats, stream);
     if (f.pos.empty()) { f.lo = V3(0.0f); f.hi = V3(0.0f); }
     sg.bounds.lo = f.lo;

@@ -264,8 +264,10 @@ VLRB_HD bool isDispersive(uint32_t t) { return (t & Dispersive) != 0; }
 struct MengTables {
     const uint8_t* grid;
     const float* points;
+    const float* blended;   // optional: per-material spectra on the 95-sample grid (mengBlend)
 };
 constexpr uint32_t kMengGridW = 12, kMengGridH = 14, kMengSamples = 95, kMengPointStride = 99;
+constexpr uint32_t kMengNumPoints = 186;
 constexpr float kMengEqualEnergy = 0.009355121400914532f; // spectrum_types.h:373-375
 
 enum class SpType : uint32_t { Reflectance = 0, LightSource = 1, IOR = 2, NA = 3 };
@@ -436,6 +438,63 @@ VLRB_HD S4 mengEvaluate(const MengTables &T, const UpSpec &sp, const WLS &wls) {
         }
     }
     return ret * sp.scale;
+}
+
+// The spectrum an UpSpec evaluates to, tabulated on the table's 95-sample
+// wavelength grid with the point weights and the scale applied.  For a
+// spectrum that is the same at every hit (an immediate material colour) this
+// is computed once per scene, and evaluating it at a wavelength is one
+// linear interpolation (blendedEvaluate) instead of evaluate's 3-4 table
+// points.  Equal to evaluate up to float rounding (the weighted sum is taken
+// before the interpolation instead of after).
+VLRB_HD void mengBlend(const MengTables &T, const UpSpec &sp, float* out) {
+    uint32_t a[4] = { sp.adj & 0xFF, (sp.adj >> 8) & 0xFF, (sp.adj >> 16) & 0xFF, (sp.adj >> 24) & 0xFF };
+    for (uint32_t b = 0; b < kMengSamples; ++b) out[b] = 0.0f;
+    if (a[0] == 0xFF) return;
+    for (int j = 0; j < 4; ++j)
+        if (a[j] >= kMengNumPoints && !(j == 3 && a[j] == 0xFF)) return;   // not a table point: no spectrum
+    float sf = static_cast<float>(sp.s) / (65535 - 1);
+    float tf = static_cast<float>(sp.t) / (65535 - 1);
+    int n;
+    float w[4];
+    if (a[3] != 0xFF) {
+        w[0] = (1 - sf) * (1 - tf);
+        w[1] = sf * (1 - tf);
+        w[2] = (1 - sf) * tf;
+        w[3] = sf * tf;
+        n = 4;
+    }
+    else {
+        w[0] = sf;
+        w[1] = tf;
+        w[2] = 1.0f - sf - tf;
+        w[3] = 0.0f;
+        n = 3;
+    }
+    for (uint32_t b = 0; b < kMengSamples; ++b) {
+        float v = 0.0f;
+        for (int j = 0; j < n; ++j) v += w[j] * T.points[kMengPointStride * a[j] + 4 + b];
+        out[b] = v * sp.scale;
+    }
+}
+
+VLRB_HD S4 blendedEvaluate(const float* tab, const WLS &wls) {
+    S4 ret(0.0f);
+    for (int i = 0; i < 4; ++i) {
+        float p = (wls.lambda[i] - 360.0f) / (830.0f - 360.0f);
+        p = vclamp<float>(p, 0.0f, 1.0f);
+        float binF = p * (kMengSamples - 1);
+        uint32_t bin = vmin<uint32_t>(static_cast<uint32_t>(binF), kMengSamples - 1);
+        uint32_t binNext = vmin<uint32_t>(bin + 1, kMengSamples - 1);
+        float t = binF - bin;
+#if defined(__CUDA_ARCH__)
+        const float s0 = __ldg(tab + bin), s1 = __ldg(tab + binNext);
+#else
+        const float s0 = tab[bin], s1 = tab[binNext];
+#endif
+        ret.v[i] = s0 * (1 - t) + s1 * t;
+    }
+    return ret;
 }
 
 // ---------------------------------------------------------------- Fresnel

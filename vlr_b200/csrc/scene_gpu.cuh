@@ -24,7 +24,16 @@ struct MatDesc {
     UpSpec emit;            // emittance
     float emitScale;
     uint32_t bsdfFlags;     // Bsdf::flags bits chosen at scene build (kBsdfConsistentPdf)
+    int32_t table[4] = { -1, -1, -1, -1 };   // sp[0..2], emit: index of the blended spectrum
+                                             // in MengTables::blended (-1: evaluate the UpSpec)
 };
+
+// Spectrum slot 0-2 (sp) or 3 (emit) of material m at the path's wavelengths:
+// the scene's blended table when it has one, else the UpSpec.
+VLRB_HD S4 matSpectrum(const MengTables &T, const MatDesc &m, int slot, const WLS &wls) {
+    if (T.blended && m.table[slot] >= 0) return blendedEvaluate(T.blended + m.table[slot] * kMengSamples, wls);
+    return mengEvaluate(T, slot < 3 ? m.sp[slot] : m.emit, wls);
+}
 
 // A discrete distribution in the reference's layout (shared/shared.h:182-231):
 // PMF[n], CDF[n + 1] with CDF[n] = 1, integral = sum of the raw weights.
@@ -134,24 +143,24 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
     switch (kind) {
     case kMatte:
     case kLambertianBSDF:
-        B.a = mengEvaluate(T, m.sp[0], wls);
+        B.a = matSpectrum(T, m, 0, wls);
         break;
     case kSpecularBRDF:
     case kSpecularBSDF:
     case kMicrofacetBSDF:
-        B.a = mengEvaluate(T, m.sp[0], wls);
-        B.b = mengEvaluate(T, m.sp[1], wls);
-        B.c = mengEvaluate(T, m.sp[2], wls);
+        B.a = matSpectrum(T, m, 0, wls);
+        B.b = matSpectrum(T, m, 1, wls);
+        B.c = matSpectrum(T, m, 2, wls);
         if (kind == kSpecularBSDF) B.flags = wls.single ? 0u : 1u;
         if (kind == kMicrofacetBSDF) B.flags = m.bsdfFlags & kBsdfConsistentPdf;
         break;
     case kMicrofacetBRDF:
-        B.b = mengEvaluate(T, m.sp[1], wls);
-        B.c = mengEvaluate(T, m.sp[2], wls);
+        B.b = matSpectrum(T, m, 1, wls);
+        B.c = matSpectrum(T, m, 2, wls);
         break;
     case kUE4: {
         // UE4SurfaceMaterial_setupBSDF (materials.cu:1959-1978); f[1] = metallic.
-        S4 base = mengEvaluate(T, m.sp[0], wls);
+        S4 base = matSpectrum(T, m, 0, wls);
         const float metallic = m.f[1];
         const float specular = 0.5f;
         B.a = base * (1 - metallic);
@@ -167,7 +176,7 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
 
 VLRB_HD S4 emittance(const MengTables &T, const MatDesc &m, const WLS &wls) {
     if (m.emitter == 0) return S4::zero();
-    return mengEvaluate(T, m.emit, wls) * m.emitScale;
+    return matSpectrum(T, m, 3, wls) * m.emitScale;
 }
 
 #if defined(__CUDACC__)

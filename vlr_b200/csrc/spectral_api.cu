@@ -32,6 +32,24 @@ extern "C" VLRResult vlrbEvaluateSpectrum(const uint32_t packed[3], const float 
     return VLRResult_NoError;
 }
 
+extern "C" VLRResult vlrbEvaluateSpectrumTabulated(const uint32_t packed[3], const float lambdas[4], float values[4]) {
+    if (!packed || !lambdas || !values) return VLRResult_InvalidArgument;
+    UpSpec s;
+    std::memcpy(&s, packed, 12);
+    const uint32_t b[4] = { s.adj & 0xFF, (s.adj >> 8) & 0xFF, (s.adj >> 16) & 0xFF, (s.adj >> 24) & 0xFF };
+    if (b[0] != 0xFF && (b[0] >= 186 || b[1] >= 186 || b[2] >= 186 || (b[3] != 0xFF && b[3] >= 186)))
+        return VLRResult_InvalidArgument;
+    float tab[kMengSamples];
+    mengBlend(hostMengTables(), s, tab);
+    WLS w;
+    for (int i = 0; i < 4; ++i) w.lambda[i] = lambdas[i];
+    w.selected = 0;
+    w.single = 0;
+    S4 v = blendedEvaluate(tab, w);
+    for (int i = 0; i < 4; ++i) values[i] = v[i];
+    return VLRResult_NoError;
+}
+
 extern "C" VLRResult vlrbCmfStrata(float xyz[48], float* integralCMF) {
     if (!xyz || !integralCMF) return VLRResult_InvalidArgument;
     const CmfStrata &c = hostCmfStrata();
