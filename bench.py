@@ -166,7 +166,7 @@ RMSE_W = RMSE_H = 1024
 RMSE_BLOCK = 8
 RMSE_TARGET = 0.01
 RMSE_REF_SPP = 4096
-RMSE_CHUNK_SPP = 4
+RMSE_CHUNK_SPP = 16
 RMSE_CAP_S = 40.0
 
 
@@ -205,13 +205,14 @@ def time_to_rmse():
         ctx.bindOutputBuffer(W, H)
         scene, cam, keep = scenes.cornell_box(ctx, W, H, glass="sphere", light_scale=0.1)
         ctx.setScene(scene)
-        ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 22, rng_seed=seed,
+        ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 24, rng_seed=seed,
                        consistent_dielectric_pdf=True)
         if guided:
-            # guided and trained at the first bounce; after the 4 warm-up
-            # launches one training step every 16 launches (the fastest of the
-            # measured configurations: 1-2 guided bounces x interval 1-16)
-            ctx.setGuiding(enabled=True, train=True, recordBounces=1, trainInterval=16)
+            # guided and trained at the first bounce; after one warm-up
+            # launch (16 spp) one training step every 4 launches (64 spp: the
+            # fastest of the measured schedules, 1-2 guided bounces x a step
+            # every 4-64 spp)
+            ctx.setGuiding(enabled=True, train=True, recordBounces=1, warmupLaunches=1, trainInterval=4)
         return ctx, cam, keep
 
     def blocks(ctx):
@@ -242,7 +243,8 @@ def time_to_rmse():
                              "NEE double counting and fireflies)",
            "guided_config": "hash grid 16x2x2^19, 3x64 BF16 MLP, 8 vMF lobes, Adam lr 1e-2, 2^18 samples per "
                             "step, one-sample MIS 0.5 with the BSDF; guided and trained at the first bounce, "
-                            "4 warm-up launches, then one step every 16 launches (training time included)"}
+                            "one warm-up launch of 16 spp, then one step every 4 launches (64 spp); training time "
+                            "included"}
     out["reference_noise"] = math.sqrt(ref_var) / ref_mean
     for name, guided in (("plain", False), ("guided", True)):
         ctx, cam, keep = make(guided, 0)
@@ -261,7 +263,7 @@ def time_to_rmse():
             n += RMSE_CHUNK_SPP
             mse = torch.mean((blocks(ctx) / n - ref) ** 2).item()
             err = math.sqrt(max(mse - ref_var, 0.0)) / ref_mean
-            if n in (4, 16, 64, 256, 1024, 4096) or err <= RMSE_TARGET:
+            if n in (16, 64, 256, 1024, 4096, 8192) or err <= RMSE_TARGET:
                 curve.append([n, round(t, 4), err])
             if err <= RMSE_TARGET:
                 reached = t
@@ -354,6 +356,8 @@ def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt")):
         ctx.setScene(scene)
         ctx.setRenderer(renderer)
         ctx.setOptions(max_path_length=12, max_paths_in_flight=1 << 22)
+        if renderer == V.RENDERER_PATH_TRACING:
+            ctx.autotune(cam, spp)      # launch configuration for this workload's frame
         ctx.render_samples(cam, True, 2)
         torch.cuda.synchronize()
         s0 = ctx.stats()["pathSegments"]
@@ -449,7 +453,7 @@ def batch_workload():
             ctx.setGuiding(enabled=True, train=True, log2TableSize=16, samplesPerStep=1 << 16)
         items.append((ctx, cam, keep, spp, W, H))
     for ctx, cam, keep, spp, W, H in items:
-        ctx.autotune(cam, samples_per_trial=1)
+        ctx.autotune(cam, samples_per_trial=min(spp, 4))
     stream = torch.cuda.current_stream()
     ev = lambda: torch.cuda.Event(enable_timing=True)
     # per-scene launches, one scene after another (after one warm-up pass)
@@ -514,11 +518,12 @@ def batch_workload():
 #          + next-queue append 4 + shadow ray 48                      = 412 B / hit
 #   shadow: shadow ray 48 + contribution read-modify-write 32        = 80 B / shadow ray
 STAGE_BYTES = {"trace": 56, "shade": 412, "shadow": 80}
-# DRAM bytes per unit measured on this workload: dram__bytes_read.sum +
-# dram__bytes_write.sum summed over the 128 launches of each stage in one
-# 256-spp step (ncu, one pass), divided by that step's 149,342,553 segments
-# (trace, shade) or per segment as well for shadow.
-STAGE_DRAM_BYTES_PER_SEGMENT = {"trace": 68.33, "shade": 369.95, "shadow": 38.22}
+# DRAM bytes per path segment measured on this workload at the autotuned
+# launch configuration (2^25 paths in flight, 32 blocks per SM):
+# dram__bytes_read.sum + dram__bytes_write.sum summed over the 16 launches of
+# each stage in one 256-spp step (ncu, one pass), divided by that step's
+# 149,354,856 segments.
+STAGE_DRAM_BYTES_PER_SEGMENT = {"trace": 82.6, "shade": 426.9, "shadow": 44.3}
 
 
 def main():
@@ -530,6 +535,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-1%%-error measurement")
     ap.add_argument("--no-workloads", action="store_true", help="skip the BSDF-batch and terrain workloads")
+    ap.add_argument("--paths-in-flight", type=int, default=0,
+                    help="pin the launch configuration instead of autotuning it (profiling runs)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS),
                     help="run only this secondary workload and print its JSON line (profiling runs)")
     args = ap.parse_args()
@@ -561,6 +569,15 @@ def main():
     ctx.setScene(scene)
     ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 22)
     stream = torch.cuda.current_stream().cuda_stream
+    # launch configuration (paths in flight x blocks per SM) chosen by the
+    # library's autotuner, one full step per candidate, before any timing
+    if args.paths_in_flight:
+        ctx.setOptions(max_paths_in_flight=args.paths_in_flight, blocks_per_sm=args.blocks_per_sm or 8)
+        chosen = "pinned on the command line"
+    else:
+        ctx.autotune(cam, SPP_PER_STEP, stream=stream)
+        chosen = "vlrbContextAutotune, 2^20..2^25 paths x 4..32 blocks per SM, one step per candidate"
+    launch_opts = ctx.options()
 
     film_t = None
     if world > 1:
@@ -671,7 +688,11 @@ def main():
             "config": {"workload": f"Cornell box PT {W}x{H}, {SPP_PER_STEP} spp per step, max path length "
                                    f"{MAX_PATH_LENGTH}, 4 hero wavelengths, MIS NEE, FP64 film",
                        "scene_triangles": ctx.stats()["numTriangles"],
-                       "l2": "working set > L2: 4M path slots x ~200 B of SoA path state per launch",
+                       "l2": f"working set > L2: {launch_opts['maxPathsInFlight']} path slots x ~200 B of SoA "
+                             f"path state per launch",
+                       "launch": {"paths_in_flight": launch_opts["maxPathsInFlight"],
+                                  "blocks_per_sm": launch_opts["blocksPerSM"],
+                                  "chosen_by": chosen},
                        "parallelism": f"replica render per GPU + NCCL film all-reduce" if world > 1 else "1 GPU"},
             "segments_per_step": seg_total / args.steps,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(param_bytes / args.steps),

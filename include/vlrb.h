@@ -89,10 +89,13 @@ VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOption
 VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* options);
 
 /* Autotuner: times `samplesPerTrial`-spp renders of the bound scene and camera
- * over paths in flight {2^20 .. 2^23} x blocks per SM {4, 8, 16, 32}, keeps
+ * over paths in flight {2^20 .. 2^25} x blocks per SM {4, 8, 16, 32}, keeps
  * the fastest pair in the render options and writes up to maxTrials trials
- * (paths in flight, blocks per SM, segments/s).  The film holds the last
- * trial afterwards; the next render with firstFrame clears it. */
+ * (paths in flight, blocks per SM, segments/s).  Path counts above what one
+ * trial renders (pixels x samplesPerTrial) or above half the free device
+ * memory (~256 bytes a path) are not tried: give the trial the samples per
+ * call the application renders.  The film holds the last trial afterwards;
+ * the next render with firstFrame clears it. */
 typedef struct VLRBAutotuneTrial {
     uint32_t maxPathsInFlight;
     uint32_t blocksPerSM;

@@ -742,10 +742,18 @@ std::vector<AutotuneTrial> Context::autotune(cudaStream_t stream, const Camera* 
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
     uint32_t frames = 0;
-    for (uint32_t paths : { 1u << 20, 1u << 21, 1u << 22, 1u << 23 }) {
+    // Path slots cost ~250 bytes each; candidates stay within half the free
+    // device memory, and above the paths one trial renders (pixels x
+    // samplesPerTrial) a candidate behaves like the one that holds them all.
+    size_t freeBytes = 0, totalBytes = 0;
+    ck(cudaMemGetInfo(&freeBytes, &totalBytes), "memory info");
+    const uint64_t trialPaths = uint64_t(pixels) * samplesPerTrial;
+    for (uint32_t paths : { 1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25 }) {
         // below one sample per pixel per launch the candidate equals the
         // smallest one that holds a full frame
         if (paths < pixels && !trials.empty() && trials.back().maxPathsInFlight >= pixels) continue;
+        if (!trials.empty() && uint64_t(trials.back().maxPathsInFlight) >= trialPaths) break;
+        if (!trials.empty() && uint64_t(std::max(paths, pixels)) * 256 > freeBytes / 2) break;
         for (uint32_t bps : { 4u, 8u, 16u, 32u }) {
             options.maxPathsInFlight = std::max(paths, pixels);
             options.blocksPerSM = bps;
