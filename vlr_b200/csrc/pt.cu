@@ -39,10 +39,20 @@ __device__ __forceinline__ WLS loadWls(const PathBuffers &pb, uint32_t p) {
     return w;
 }
 
+// Pixel of path slot p: the slots of one sample cover the image in 8x4-pixel
+// tiles, one warp per tile, when it divides into them (row-major otherwise),
+// so a warp's camera rays leave neighbouring pixels in both directions.
+__device__ __forceinline__ uint32_t pixelOfPath(uint32_t p, uint32_t W, uint32_t H) {
+    const uint32_t i = p % (W * H);
+    if ((W & 7u) || (H & 3u)) return i;
+    const uint32_t tile = i >> 5, lane = i & 31u, tilesX = W >> 3;
+    return ((tile / tilesX) * 4 + (lane >> 3)) * W + (tile % tilesX) * 8 + (lane & 7u);
+}
+
 __global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
     const uint32_t P = fp.numPaths;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-        const uint32_t pixel = p % (fp.width * fp.height);
+        const uint32_t pixel = pixelOfPath(p, fp.width, fp.height);
         const uint32_t px = pixel % fp.width, py = pixel / fp.width;
         PCG32 rng{ pb.rng[p] };
         float jx = rng.uniform(), jy = rng.uniform();
@@ -572,7 +582,7 @@ __global__ void __launch_bounds__(256) filmKernel(PathBuffers pb, Film film, Fra
         if (!c.allFinite()) continue;
         float4 l = pb.lambda[p];
         float lam[4] = { l.x, l.y, l.z, l.w };
-        const uint32_t pixel = p % (fp.width * fp.height);
+        const uint32_t pixel = pixelOfPath(p, fp.width, fp.height);
         double* dst = film.strata + static_cast<size_t>(pixel) * kNumStrata;
         for (int i = 0; i < 4; ++i) {
             uint32_t bin = vmin<uint32_t>(static_cast<uint32_t>((lam[i] - kWavelengthLow) /
