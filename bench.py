@@ -415,12 +415,45 @@ def glossy_guided_workload():
     return out
 
 
+def light_tracing_workload():
+    """The light tracer (light subpaths with lens connections splatted to the
+    film) on the Cornell box workload's scene, 512x512, one light subpath per
+    pixel per frame, 64 frames, max path length 8; device-timed segments/s."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    ctx = V.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = scenes.build(ctx, scenes.cornell_box_desc(W, H))
+    ctx.setScene(scene)
+    ctx.setRenderer(V.RENDERER_LIGHT_TRACING)
+    ctx.setOptions(max_path_length=MAX_PATH_LENGTH)
+    stream = torch.cuda.current_stream()
+    ctx.render_samples(cam, True, 8, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    s0 = ctx.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.render_samples(cam, False, 64, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s1 = ctx.stats()
+    out = {"workload": f"light tracing, Cornell box {W}x{H}, {W * H} light subpaths per frame, 64 frames, "
+                       f"max path length {MAX_PATH_LENGTH}",
+           "segments_per_s": (s1["pathSegments"] - s0["pathSegments"]) / (ms * 1e-3) / 1e9,
+           "lens_connections_per_s": (s1["shadowRays"] - s0["shadowRays"]) / (ms * 1e-3) / 1e9,
+           "unit": "G path segments/s", "ms": ms}
+    ctx.close()
+    return out
+
+
 WORKLOADS = {
     "bsdf_batch": lambda: {"bsdf_batch": bsdf_batch_workload(measured_peaks()[0])},
     "terrain_pt": lambda: terrain_workloads(("terrain_pt",)),
     "terrain_lvc_bpt": lambda: terrain_workloads(("terrain_lvc_bpt",)),
     "multi_scene_batch": lambda: {"multi_scene_batch": batch_workload()},
     "glossy_guided": lambda: {"glossy_guided": glossy_guided_workload()},
+    "light_tracing": lambda: {"light_tracing": light_tracing_workload()},
 }
 
 
@@ -660,7 +693,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_workloads:
         workloads = {}
         for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads,
-                   lambda: {"multi_scene_batch": batch_workload()}):
+                   lambda: {"multi_scene_batch": batch_workload()},
+                   lambda: {"light_tracing": light_tracing_workload()}):
             try:
                 workloads.update(fn())
             except Exception as ex:  # reported, never fatal for the GPU line

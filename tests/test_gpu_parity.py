@@ -285,6 +285,69 @@ def test_environment_lighting_bpt_matches_pt():
     assert abs(means[1] / means[0] - 1) < 0.03, means
 
 
+def test_light_tracing_mean_matches_path_tracing_oracle():
+    """Light tracing (light subpaths splatted through lens connections) and
+    path tracing estimate the same image: on the Cornell box with every
+    surface diffuse (a light tracer cannot reach a pixel that sees a glossy
+    surface in reasonable time), the GPU light tracer must converge to the
+    CPU path-tracing oracle's mean: whole image within 2%, lit 8x8 blocks
+    within 6 combined standard errors.  A wrong density in the light sample,
+    the emission direction, the lens connection or the importance-mode BSDF
+    biases the mean."""
+    from vlr_b200 import vlr as VV, scenes
+    W = H = 64
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = scenes.build(ctx, desc)
+    ctx.setScene(scene)
+    ctx.setRenderer(VV.RENDERER_LIGHT_TRACING)
+    ctx.setOptions(max_path_length=8)
+    ctx.render_samples(cam, True, 1024)
+    st = ctx.stats()
+    assert st["pathSegments"] > W * H * 1024
+    g = _y_of(ctx.read_film())
+    assert np.isfinite(g).all()
+    flat = scenes.flatten_desc(desc)
+    cfilm, _, _ = ref.pt_render(flat, desc["camera"], W, H, 1024, 8)
+    c = _y_of(cfilm)
+    assert abs(g.sum() / c.sum() - 1) < 0.02, g.sum() / c.sum()
+    gb = g.reshape(8, 8, 8, 8).sum(axis=(1, 3))
+    cb = c.reshape(8, 8, 8, 8).sum(axis=(1, 3))
+    sg = g.reshape(8, 8, 8, 8).std(axis=(1, 3)) * 8
+    sc = c.reshape(8, 8, 8, 8).std(axis=(1, 3)) * 8
+    lit = cb > 1e-3 * cb.max()
+    z = np.abs(gb - cb)[lit] / np.sqrt(sg[lit] ** 2 + sc[lit] ** 2 + (1e-3 * cb[lit]) ** 2)
+    assert np.all(z < 6), z.max()
+    ctx.close()
+
+
+def test_environment_lighting_light_tracing_matches_pt():
+    """Light subpaths starting on the environment (FP64 importance map, the
+    disc that covers the scene, lens connections of points at infinity):
+    the light tracer and PT agree on the small terrain under the sky (whole
+    image within 3%)."""
+    from vlr_b200 import vlr as VV, scenes
+    W, H = 64, 36
+    desc = _small_env_desc(W, H)
+    means = []
+    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = scenes.build_instanced(ctx, desc)
+        ctx.setScene(scene)
+        ctx.setRenderer(renderer)
+        ctx.setOptions(max_path_length=6)
+        ctx.render_samples(cam, True, 2048)
+        y = _y_of(ctx.read_film())
+        assert np.isfinite(y).all()
+        means.append(y.mean())
+        ctx.close()
+    assert abs(means[1] / means[0] - 1) < 0.03, means
+
+
 def _trace(v, rays, rounds, any_hit):
     L = V.lib()
     L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

@@ -48,6 +48,7 @@ struct BptArgs {
     uint32_t width, height;
     uint32_t maxPathLength;
     uint32_t bounce;
+    struct LtConnection* conn;   // light tracing: lens connections of the current stage
 };
 
 __device__ __forceinline__ uint32_t pathLengthOf(uint32_t f) { return (f >> 8) & 0xFFFFu; }
@@ -396,6 +397,23 @@ __device__ __forceinline__ bool idfProject(const Camera &C, const Lens &L, const
     if (*u0 < 0.0f || *u0 >= 1.0f || *u1 < 0.0f || *u1 >= 1.0f) return false;
     *pdf = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
     return true;
+}
+
+// PerspectiveCamera_sample (cameras.cu:40-74): a point on the lens, its frame
+// and area density.
+__device__ __forceinline__ Lens sampleLens(const Camera &C, float ul0, float ul1, float* areaPDF) {
+    float lx, ly;
+    concentricDisk(ul0, ul1, &lx, &ly);
+    Lens L;
+    const V3 orgLocal(C.lensRadius * lx, C.lensRadius * ly, 0.0f);
+    L.frame.z = normalize(C.forward);
+    L.frame.x = normalize(C.right);
+    L.frame.y = cross(L.frame.z, L.frame.x);
+    L.position = C.right * orgLocal.x + C.up * orgLocal.y + C.forward * orgLocal.z + C.position;
+    L.xOnLens = C.lensRadius * lx;
+    L.yOnLens = C.lensRadius * ly;
+    *areaPDF = C.lensRadius > 0.0f ? 1.0f / (kPi * C.lensRadius * C.lensRadius) : 1.0f;
+    return L;
 }
 
 __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
@@ -767,6 +785,234 @@ __global__ void __launch_bounds__(256) eyeFilmKernel(BptArgs a) {
     }
 }
 
+// ----------------------------------------------------------------- light tracing
+// One light subpath per slot with wavelength samples of its own; the light
+// point and every scattering vertex connect to a lens sample and splat what
+// they send there to the pixel it projects to (light_tracing.cu:49-263).
+// Connections of one stage are traced and splatted before the next stage.
+struct LtConnection {
+    float4 org;       // xyz, tmax
+    float4 dir;       // xyz, pixel (bits)
+    float4 contrib;
+    float4 lambda;    // the path's wavelengths
+};
+
+// Connection from lens sample L to vertex sp (testVisibility from the lens,
+// light_transport_common.h:147-177): false when the direction misses the
+// frame; else the ray, the pixel, the vertex-side direction in its shading
+// frame and G / lensPDF with G = cos(vertex, geometric) cos(lens) / d^2.
+__device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, float lensAreaPDF, const SurfPt &sp,
+                                               uint32_t W, uint32_t H, V3* dir, V3* org, float* tmax,
+                                               uint32_t* pixel, V3* dirAtVertex, float* scalar) {
+    SurfPt spE;
+    spE.position = L.position;
+    spE.gn = L.frame.z;
+    spE.frame = L.frame;
+    spE.atInfinity = false;
+    float dist2;
+    visibilityRay(spE, sp, dir, &dist2, org, tmax);
+    const V3 dLens = L.frame.toLocal(*dir);
+    float u0, u1, pdf;
+    if (!idfProject(C, L, dLens, &u0, &u1, &pdf)) return false;
+    const uint32_t ipx = static_cast<uint32_t>(u0 * W), ipy = static_cast<uint32_t>(u1 * H);
+    if (ipx >= W || ipy >= H) return false;
+    *pixel = ipy * W + ipx;
+    *dirAtVertex = sp.frame.toLocal(-*dir);
+    *scalar = absDot(*dir, sp.gn) * absDot(*dir, L.frame.z) / dist2 / lensAreaPDF;
+    return true;
+}
+
+__device__ __forceinline__ void emitLensConnection(const BptArgs &a, uint32_t stage, const V3 &org, const V3 &dir,
+                                                   float tmax, uint32_t pixel, const S4 &c, const WLS &wls) {
+    const uint32_t slot = appendSlot(bounceCounters(a.pb, stage) + kCntShadow, 0u);
+    if (slot >= a.numPaths) return;
+    LtConnection k;
+    k.org = make_float4(org.x, org.y, org.z, tmax);
+    k.dir = make_float4(dir.x, dir.y, dir.z, __uint_as_float(pixel));
+    k.contrib = toF4(c);
+    k.lambda = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
+    a.conn[slot] = k;
+}
+
+__global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
+    const SceneGPU &S = a.S;
+    const Camera &C = S.cam;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.numPaths; p += gridDim.x * blockDim.x) {
+        PCG32 rng{ a.pb.rng[p] };
+        float selectWLPDF;
+        const float wo = rng.uniform(), ws = rng.uniform();
+        const WLS wls = WLS::equalOffsets(wo, ws, &selectWLPDF);
+        float uLight = rng.uniform();
+        float instProb, uInst;
+        uint32_t li = S.lightInsts.sample(uLight, &instProb, &uInst);
+        float groupProb, uPrim;
+        uint32_t g = S.instGroups[li].sample(uInst, &groupProb, &uPrim);
+        const float lightProb = instProb * groupProb;
+        float ue0 = rng.uniform(), ue1 = rng.uniform();
+        LightSample ls;
+        S4 Le0;
+        const bool env = static_cast<int32_t>(li) == S.envInst;
+        if (env) {
+            float uu, vv, uvPDF;
+            envSampleUV(S.env, ue0, ue1, &uu, &vv, &uvPDF);
+            float phi = 2 * kPi * uu, theta = kPi * vv;
+            float posPhi = phi - S.envRotation;
+            posPhi = posPhi - floorf(posPhi / (2 * kPi)) * 2 * kPi;
+            envSurfPt(dirFromPolarYUp(posPhi, theta), posPhi, &ls.sp);
+            ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
+            ls.material = S.envMaterial;
+            ls.delta = false;
+            Le0 = kPi * envRadiance(S, uu, vv, wls) * S.mats[S.envMaterial].emitScale;
+        }
+        else {
+            uint32_t grp = __ldg(S.instFirstGroup + li) + g;
+            sampleTriangleGroup(S, grp, uPrim, ue0, ue1, &ls);
+            Le0 = emittance(S.meng, S.mats[ls.material], wls);
+        }
+        S4 alpha = Le0 / (a.numLightPaths * lightProb * ls.areaPDF * selectWLPDF);
+        // explicit lens sampling from the light point (light_tracing.cu:70-106)
+        {
+            float lensPDF;
+            const Lens L = sampleLens(C, rng.uniform(), rng.uniform(), &lensPDF);
+            V3 dir, org, dv;
+            float tmax, scalar;
+            uint32_t pixel;
+            if (lensConnection(C, L, lensPDF, ls.sp, a.width, a.height, &dir, &org, &tmax, &pixel, &dv, &scalar)) {
+                const S4 Le1(dv.z > 0.0f ? 1.0f / kPi : 0.0f);      // DiffuseEDF / EnvironmentEDF evaluate
+                const S4 c = alpha * S4(C.sensitivity) * Le1 * scalar;
+                if (c.allFinite() && c.hasNonZero()) emitLensConnection(a, 0, org, dir, tmax, pixel, c, wls);
+            }
+        }
+        // emission direction (as the LVC light subpaths)
+        float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
+        (void)uc;
+        V3 dirLocal;
+        float dirPDF;
+        if (env) {
+            float dx, dy;
+            concentricDisk(ud0, ud1, &dx, &dy);
+            dirLocal = V3(S.bounds.worldRadius * dx, S.bounds.worldRadius * dy, 1.0f);
+            dirPDF = 1.0f / S.bounds.worldDiscArea;
+        }
+        else {
+            dirLocal = cosineHemisphere(ud0, ud1);
+            dirPDF = dirLocal.z / kPi;
+        }
+        V3 rayOrg = offsetRayOrigin(ls.sp.position, ls.sp.gn);
+        if (ls.sp.atInfinity) {
+            rayOrg = S.bounds.center + 1.1f * S.bounds.worldRadius * ls.sp.position + ls.sp.frame.x * dirLocal.x +
+                     ls.sp.frame.y * dirLocal.y;
+            dirLocal.x = 0;
+            dirLocal.y = 0;
+        }
+        const V3 rayDir = ls.sp.frame.fromLocal(dirLocal);
+        alpha *= S4(1.0f / kPi) * (absDot(rayDir, ls.sp.gn) / dirPDF);
+        a.pb.rng[p] = rng.state;
+        a.pb.alpha[p] = toF4(alpha);
+        a.pb.lambda[p] = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
+        a.pb.flags[p] = wls.selected;
+        a.pb.initImportance[p] = alpha.importance(wls.selected);
+        a.pb.rayOrg[p] = make_float4(rayOrg.x, rayOrg.y, rayOrg.z, FLT_MAX);
+        a.pb.rayDir[p] = make_float4(rayDir.x, rayDir.y, rayDir.z, 0.0f);
+        a.pb.active[0][p] = p;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) bounceCounters(a.pb, 0)[kCntActive] = a.numPaths;
+}
+
+// One scattering vertex of every live light subpath (lightTracingIteration,
+// light_tracing.cu:186-263, and the Russian roulette of its caller, :159-163).
+__global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
+    const SceneGPU &S = a.S;
+    const Camera &C = S.cam;
+    uint32_t* ctr = bounceCounters(a.pb, a.bounce);
+    uint32_t* next = bounceCounters(a.pb, a.bounce + 1);
+    __shared__ uint32_t sOff[kNumShadeBuckets + 1];
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < kNumShadeBuckets; ++k) { sOff[k] = run; run += ctr[kCntBucket0 + k]; }
+        sOff[kNumShadeBuckets] = run;
+    }
+    __syncthreads();
+    const uint32_t total = sOff[kNumBsdfKinds];   // misses end light subpaths
+    uint32_t* nextQueue = a.pb.active[(a.bounce + 1) & 1];
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        uint32_t k = 0;
+        while (j >= sOff[k + 1]) ++k;
+        const uint32_t p = a.pb.buckets[k * a.numPaths + (j - sOff[k])];
+        uint32_t flags = a.pb.flags[p];
+        const uint32_t traced = ((flags >> 8) & 0xFFFFu) + 1;
+        const float4 l4 = a.pb.lambda[p];
+        WLS wls;
+        wls.lambda[0] = l4.x; wls.lambda[1] = l4.y; wls.lambda[2] = l4.z; wls.lambda[3] = l4.w;
+        wls.selected = flags & 0xFu;
+        wls.single = (flags >> 4) & 1u;
+        const float4 h = a.pb.hit[p];
+        SurfPt sp;
+        decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, nullptr);
+        const uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
+        const Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls);
+        const float4 d4 = a.pb.rayDir[p];
+        BsdfQuery q;
+        q.dirLocal = sp.frame.toLocal(-V3(d4.x, d4.y, d4.z));
+        q.wlHint = wls.selected;
+        q.filter = dir::All;
+        q.importanceMode = 1;
+        const V3 gnLocal = sp.frame.toLocal(sp.gn);
+        S4 alpha = toS4(a.pb.alpha[p]);
+        PCG32 rng{ a.pb.rng[p] };
+        if (bsdfHasNonDelta(bsdf)) {
+            float lensPDF;
+            const Lens L = sampleLens(C, rng.uniform(), rng.uniform(), &lensPDF);
+            V3 dir, org, dv;
+            float tmax, scalar;
+            uint32_t pixel;
+            if (lensConnection(C, L, lensPDF, sp, a.width, a.height, &dir, &org, &tmax, &pixel, &dv, &scalar)) {
+                const S4 fs = bsdfEval(bsdf, q, gnLocal, dv, nullptr);
+                const S4 c = alpha * S4(C.sensitivity) * fs * scalar;
+                if (c.allFinite() && c.hasNonZero())
+                    emitLensConnection(a, a.bounce + 1, org, dir, tmax, pixel, c, wls);
+            }
+        }
+        float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
+        BsdfSample bs;
+        const S4 fs = bsdfSample(bsdf, q, gnLocal, uc, ud0, ud1, &bs, nullptr);
+        if (fs.isZero() || !(bs.dirPDF > 0.0f)) { a.pb.rng[p] = rng.state; continue; }
+        if (dir::isDispersive(bs.sampledType) && !wls.single) {
+            bs.dirPDF /= kNumLambdas;
+            flags |= 0x10u;
+        }
+        const float cosFactor = dot(bs.dirLocal, gnLocal);
+        alpha *= fs * (fabsf(cosFactor) / bs.dirPDF);
+        const float continueProb = fminf(alpha.importance(wls.selected) / a.pb.initImportance[p], 1.0f);
+        const bool survive = rng.uniform() < continueProb;
+        a.pb.rng[p] = rng.state;
+        if (!survive || traced + 1 >= a.maxPathLength) continue;
+        alpha /= continueProb;
+        const V3 dirOut = sp.frame.fromLocal(bs.dirLocal);
+        const V3 org = offsetRayOrigin(sp.position, cosFactor > 0.0f ? sp.gn : -sp.gn);
+        a.pb.flags[p] = (flags & 0xFFu) | (traced << 8);
+        a.pb.alpha[p] = toF4(alpha);
+        a.pb.rayOrg[p] = make_float4(org.x, org.y, org.z, FLT_MAX);
+        a.pb.rayDir[p] = make_float4(dirOut.x, dirOut.y, dirOut.z, 0.0f);
+        const uint32_t slot = appendSlot(next + kCntActive, 0u);
+        nextQueue[slot] = p;
+    }
+}
+
+// Traces one stage's lens connections and splats the unoccluded ones.
+__global__ void __launch_bounds__(256) ltSplatKernel(BptArgs a, uint32_t stage) {
+    const uint32_t n = min(bounceCounters(a.pb, stage)[kCntShadow], a.numPaths);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const LtConnection k = a.conn[i];
+        const Hit h = traceBvh<true>(a.S.bvh, V3(k.org.x, k.org.y, k.org.z), V3(k.dir.x, k.dir.y, k.dir.z), k.org.w);
+        if (h.prim != 0xFFFFFFFFu) continue;
+        const uint32_t pixel = __float_as_uint(k.dir.w);
+        if (pixel >= a.width * a.height) continue;
+        const float lam[4] = { k.lambda.x, k.lambda.y, k.lambda.z, k.lambda.w };
+        filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, toS4(k.contrib));
+    }
+}
+
 __global__ void bptStatsKernel(PathBuffers pb, uint32_t bounces) {
     unsigned long long seg = 0, sh = 0;
     for (uint32_t b = threadIdx.x; b <= bounces; b += 32) {
@@ -893,6 +1139,60 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
     T.end(stream);
     T.begin(kStageFilm, stream, sizeof(PathBuffers) + 4);
     bptStatsKernel<<<1, 32, 0, stream>>>(eyePaths, fp.maxPathLength);
+    T.end(stream);
+    ck(cudaGetLastError(), "launch");
+    T.collect();
+}
+
+size_t ltConnectionBytes(uint32_t numPaths) { return a256(size_t(numPaths) * sizeof(LtConnection)); }
+
+void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* connections, const Film &film,
+                    const FrameParams &fp, uint32_t numLightPaths, int numSMs, cudaStream_t stream,
+                    StageTimer* timer) {
+    if (fp.maxPathLength == 0 || fp.maxPathLength >= kMaxBounces)
+        throw std::runtime_error("maxPathLength out of range");
+    if (scene.lightInsts.n == 0)
+        throw std::runtime_error("light tracing needs at least one light");
+    StageTimer dummy;
+    StageTimer &T = timer ? *timer : dummy;
+    const int grid = numSMs * static_cast<int>(fp.blocksPerSM ? fp.blocksPerSM : 8);
+    const size_t pBytes = sizeof(BptArgs);
+    BptArgs a{};
+    a.S = scene;
+    a.pb = lightPaths;
+    a.film = film;
+    a.numLightPaths = numLightPaths;
+    a.numPaths = numLightPaths;
+    a.width = fp.width;
+    a.height = fp.height;
+    a.maxPathLength = fp.maxPathLength;
+    a.conn = static_cast<LtConnection*>(connections);
+    ck(cudaMemsetAsync(lightPaths.counters, 0, size_t(kMaxBounces + 1) * kCountersPerBounce * 4, stream), "counters");
+    T.begin(kStageCamera, stream, pBytes);
+    ltStartKernel<<<grid, 256, 0, stream>>>(a);
+    T.end(stream);
+    T.begin(kStageShadow, stream, pBytes + 4);
+    ltSplatKernel<<<grid, 256, 0, stream>>>(a, 0u);
+    T.end(stream);
+    FrameParams lf = fp;
+    lf.numPaths = numLightPaths;
+    // at most maxPathLength - 1 traced segments before the lens connection
+    // (the loop of light_tracing.cu:145-171 with MaxPathLength)
+    for (uint32_t b = 0; b + 1 < fp.maxPathLength; ++b) {
+        lf.bounce = b;
+        a.bounce = b;
+        T.begin(kStageTrace, stream, sizeof(SceneGPU) + sizeof(PathBuffers) + sizeof(FrameParams));
+        launchTraceSorted(scene, lightPaths, lf, grid, stream);
+        T.end(stream);
+        T.begin(kStageShade, stream, pBytes);
+        ltShadeKernel<<<grid, 256, 0, stream>>>(a);
+        T.end(stream);
+        T.begin(kStageShadow, stream, pBytes + 4);
+        ltSplatKernel<<<grid, 256, 0, stream>>>(a, b + 1);
+        T.end(stream);
+    }
+    T.begin(kStageFilm, stream, sizeof(PathBuffers) + 4);
+    bptStatsKernel<<<1, 32, 0, stream>>>(lightPaths, fp.maxPathLength);
     T.end(stream);
     ck(cudaGetLastError(), "launch");
     T.collect();

@@ -44,6 +44,14 @@ void carveBptBuffers(void* base, uint32_t numLightPaths, uint32_t numEyePaths, u
 
 // One LVC-BPT frame: light subpaths fill the cache, then one eye subpath per
 // pixel connects to it.  All paths share the frame's wavelength samples.
+// Light tracing (light_tracing.cu:49-263): numLightPaths light subpaths with
+// wavelength samples of their own, each vertex connected to a lens sample and
+// splatted to the film.  `connections` holds ltConnectionBytes(numLightPaths).
+size_t ltConnectionBytes(uint32_t numPaths);
+void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* connections, const Film &film,
+                    const FrameParams &fp, uint32_t numLightPaths, int numSMs, cudaStream_t stream,
+                    StageTimer* timer);
+
 void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const PathBuffers &lightPaths,
                      const BptBuffers &bb, const Film &film, const FrameParams &fp, uint32_t numLightPaths,
                      const WLS &commonWls, float wlPdf, int numSMs, cudaStream_t stream, StageTimer* timer);

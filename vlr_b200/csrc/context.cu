@@ -703,6 +703,28 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 bptRenderLaunch(sg, pb, lightPb, bb, fl, bf, lightPaths, wls, wlPdf, numSMs, stream, &timer);
                 k = 1;
             }
+            else if (renderer == VLRRenderer_LightTracing) {
+                // One frame per launch: light subpaths per frame default to
+                // the pixel count (the reference launches a fixed 500,000,
+                // context.h:303); each carries its own wavelength samples.
+                const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame : pixels;
+                if (ltCapacity < lightPaths) {
+                    ltCapacity = lightPaths;
+                    const size_t pathBytes = pathBufferBytes(lightPaths);
+                    ltMem.resize(pathBytes + ltConnectionBytes(lightPaths));
+                    carvePathBuffers(ltMem.ptr, lightPaths, &ltPb);
+                    ltConn = ltMem.as<char>() + pathBytes;
+                    std::vector<uint64_t> seeds(lightPaths);
+                    seedPathRngs(seeds.data(), lightPaths, 459182033132123413ull);
+                    ck(cudaMemcpy(ltPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
+                    ck(cudaMemset(ltPb.totals, 0, 16), "totals");
+                }
+                FrameParams lf = fp;
+                lf.sppPerLaunch = 1;
+                lf.numPaths = lightPaths;
+                ltRenderLaunch(sg, ltPb, ltConn, fl, lf, lightPaths, numSMs, stream, &timer);
+                k = 1;
+            }
             else if (guiding.enabled || guiding.train) {
                 ensureGuiding(pathCapacity);
                 // record and train on every trainInterval-th launch once
@@ -874,6 +896,10 @@ void Context::readStats(RenderStats* out) {
     if (pathCapacity > 0) ck(cudaMemcpy(t, pb.totals, 16, cudaMemcpyDeviceToHost), "stats");
     unsigned long long tl[2] = { 0, 0 };
     if (bptCapacityPaths > 0) ck(cudaMemcpy(tl, lightPb.totals, 16, cudaMemcpyDeviceToHost), "light stats");
+    unsigned long long tt[2] = { 0, 0 };
+    if (ltCapacity > 0) ck(cudaMemcpy(tt, ltPb.totals, 16, cudaMemcpyDeviceToHost), "light tracing stats");
+    tl[0] += tt[0];
+    tl[1] += tt[1];
     *out = stats;
     if (sg.bvh.errorFlag) {
         uint32_t e = 0;

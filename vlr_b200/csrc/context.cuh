@@ -142,6 +142,11 @@ private:
     uint64_t pathSeed = 0;
     unsigned long long totalsBase[2] = { 0, 0 };
     uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0, bptEyeCapacity = 0;
+    // light tracing: light subpaths of one frame and their lens connections
+    DeviceBuffer ltMem;
+    PathBuffers ltPb{};
+    void* ltConn = nullptr;
+    uint32_t ltCapacity = 0;
     CUarray outArray = nullptr;
     uint32_t* hostCounters = nullptr;
     std::vector<float> envPixelsCache;

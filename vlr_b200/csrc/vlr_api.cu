@@ -358,7 +358,8 @@ VLRResult vlrContextSetScene(VLRContext context, VLRScene scene) {
 
 VLRResult vlrContextSetRenderer(VLRContext context, enum VLRRenderer renderer) {
     CHECK_HANDLE(c, Context, kindContext, context);
-    if (renderer != VLRRenderer_PathTracing && renderer != VLRRenderer_BPT) return VLRResult_InvalidArgument;
+    if (renderer != VLRRenderer_PathTracing && renderer != VLRRenderer_BPT && renderer != VLRRenderer_LightTracing)
+        return VLRResult_InvalidArgument;
     c->renderer = renderer;
     return VLRResult_NoError;
 }

@@ -65,6 +65,7 @@ class VLRBBatchItem(ctypes.Structure):
 
 
 RENDERER_PATH_TRACING = 0
+RENDERER_LIGHT_TRACING = 1
 RENDERER_BPT = 2
 PLUG_SPECTRUM = 7
 
@@ -482,4 +483,4 @@ def quat_rotate_y(angle):
 
 
 __all__ = ["Context", "RenderBatch", "rgb", "Spectrum", "VLRError", "quat_rotate_y", "RENDERER_PATH_TRACING",
-           "RENDERER_BPT"]
+           "RENDERER_LIGHT_TRACING", "RENDERER_BPT"]
