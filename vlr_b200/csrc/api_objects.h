@@ -87,6 +87,7 @@ struct SurfaceMaterial : Queryable {
 };
 
 struct Camera : Queryable {
+    std::string type;    // "perspective" or "equirectangular"
     Camera() : Queryable(Kind::Camera) {}
 };
 

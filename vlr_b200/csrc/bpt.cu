@@ -388,15 +388,7 @@ struct Lens {
 
 __device__ __forceinline__ bool idfProject(const Camera &C, const Lens &L, const V3 &dirLocal, float* u0, float* u1,
                                            float* pdf) {
-    if (dirLocal.z <= 0.0f) return false;
-    V3 org(L.xOnLens, L.yOnLens, 0.0f);
-    float objZ = C.objPlaneDistance / dirLocal.z;
-    V3 pFocus = dirLocal * objZ + org;
-    *u0 = -pFocus.x / C.opWidth + 0.5f;
-    *u1 = -pFocus.y / C.opHeight + 0.5f;
-    if (*u0 < 0.0f || *u0 >= 1.0f || *u1 < 0.0f || *u1 >= 1.0f) return false;
-    *pdf = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
-    return true;
+    return cameraProject(C, L.xOnLens, L.yOnLens, dirLocal, u0, u1, pdf);
 }
 
 // PerspectiveCamera_sample (cameras.cu:40-74): a point on the lens, its frame
@@ -473,7 +465,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
                 V3 conLocalL = v.sp.frame.toLocal(-conDir);
                 V3 conLocalE = L.frame.toLocal(conDir);
                 float cosL = absDot(conDir, v.sp.gn);
-                float cosE = absDot(conDir, gn);
+                float cosE = lensCos(C, conDir, gn);
                 float G = cosL * cosE * recSq;
                 float scalarConTerm = G / vertexProb;
                 if (v.flags & 1u) scalarConTerm *= kNumLambdas;
@@ -510,11 +502,10 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
         }
         // camera ray (lvc_bpt.cu:481-503)
         float u0 = fx / a.width, u1 = fy / a.height;
-        V3 pFocus(C.opWidth * (0.5f - u0), C.opHeight * (0.5f - u1), C.objPlaneDistance);
-        V3 dirLocal = normalize(pFocus - orgLocal);
-        float dirPDF = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
+        float dirPDF;
+        V3 dirLocal = cameraSampleDir(C, orgLocal.x, orgLocal.y, u0, u1, &dirPDF);
         V3 rayDir = L.frame.fromLocal(dirLocal);
-        float cosTerm = absDot(rayDir, gn);
+        float cosTerm = lensCos(C, rayDir, gn);
         alpha *= S4::one() * (cosTerm / dirPDF);
         a.pb.rng[p] = rng.state;
         a.pb.alpha[p] = toF4(alpha);
@@ -818,7 +809,7 @@ __device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, f
     if (ipx >= W || ipy >= H) return false;
     *pixel = ipy * W + ipx;
     *dirAtVertex = sp.frame.toLocal(-*dir);
-    *scalar = absDot(*dir, sp.gn) * absDot(*dir, L.frame.z) / dist2 / lensAreaPDF;
+    *scalar = absDot(*dir, sp.gn) * lensCos(C, *dir, L.frame.z) / dist2 / lensAreaPDF;
     return true;
 }
 

@@ -575,6 +575,17 @@ void Context::setupCamera(const Camera* cam) {
     C.opWidth = C.opHeight * aspect;
     C.imgPlaneDistance = 1.0f;
     C.imgPlaneArea = C.opWidth * C.opHeight * sq(C.imgPlaneDistance / objPlaneDistance);
+    C.kind = kCameraPerspective;
+    C.phiAngle = C.thetaAngle = 0.0f;
+    if (cam->type == "equirectangular") {
+        // EquirectangularCamera::set clamps the angles (scene.cpp:1805-1822);
+        // the camera is a point (cameras.cu:226-255)
+        C.kind = kCameraEquirectangular;
+        C.lensRadius = 0.0f;
+        C.sensitivity = std::isfinite(sensitivity) ? std::max(0.0f, sensitivity) : 1.0f;
+        C.phiAngle = std::min(std::max(cam->getFloat("h angle", 2 * kPi), 0.01f), 2 * kPi);
+        C.thetaAngle = std::min(std::max(cam->getFloat("v angle", kPi), 0.01f), kPi);
+    }
 }
 
 void Context::ensurePathBuffers(uint32_t paths) {

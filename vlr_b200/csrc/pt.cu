@@ -73,15 +73,15 @@ __global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, 
         camFrame.y = cross(camFrame.z, camFrame.x);
         V3 lensPos = C.right * orgLocal.x + C.up * orgLocal.y + C.forward * orgLocal.z + C.position;
         float areaPDF = C.lensRadius > 0.0f ? 1.0f / (kPi * C.lensRadius * C.lensRadius) : 1.0f;
-        // PerspectiveCameraIDF::sampleInternal (cameras.cu:142-155)
+        // the camera's IDF sample (cameras.cu:142-155 perspective, :272-288
+        // equirectangular); the density is per pixel
         float u0 = fx / fp.width, u1 = fy / fp.height;
-        V3 pFocus(C.opWidth * (0.5f - u0), C.opHeight * (0.5f - u1), C.objPlaneDistance);
-        V3 dirLocal = normalize(pFocus - V3(C.lensRadius * lx, C.lensRadius * ly, 0.0f));
-        float dirPDF = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
+        float dirPDF;
+        V3 dirLocal = cameraSampleDir(C, C.lensRadius * lx, C.lensRadius * ly, u0, u1, &dirPDF);
         dirPDF *= static_cast<float>(fp.width * fp.height);
         V3 rayDir = camFrame.fromLocal(dirLocal);
         S4 We0(C.sensitivity);
-        S4 alpha = (We0 * S4::one()) * (absDot(rayDir, gn) / (areaPDF * dirPDF * selectWLPDF));
+        S4 alpha = (We0 * S4::one()) * (lensCos(C, rayDir, gn) / (areaPDF * dirPDF * selectWLPDF));
         pb.rng[p] = rng.state;
         pb.lambda[p] = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
         pb.flags[p] = wls.selected;

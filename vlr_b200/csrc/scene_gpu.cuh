@@ -77,14 +77,71 @@ struct EmitGroup {
     Dist1D prims;             // area distribution over the group's triangles
 };
 
+enum : uint32_t { kCameraPerspective = 0, kCameraEquirectangular = 1 };
+
 struct Camera {
     V3 position;
     V3 right, up, forward;    // orientation matrix columns
     float sensitivity;
-    float lensRadius;
+    float lensRadius;         // 0 for the equirectangular camera (a point)
     float imgPlaneDistance, objPlaneDistance;
     float opWidth, opHeight, imgPlaneArea;
+    uint32_t kind;            // kCamera*
+    float phiAngle, thetaAngle;   // equirectangular: horizontal and vertical extent (radians)
 };
+
+// The camera's IDF sample for screen position (u0, u1) in [0, 1)^2 from the
+// lens point (xOnLens, yOnLens): the direction in the lens frame (z =
+// forward) and its density per solid angle over the whole image
+// (PerspectiveCameraIDF::sampleInternal, cameras.cu:144-157;
+// EquirectangularCameraIDF::sampleInternal, :272-288).
+VLRB_HD V3 cameraSampleDir(const Camera &C, float xOnLens, float yOnLens, float u0, float u1, float* dirPDF) {
+    if (C.kind == kCameraEquirectangular) {
+        const float phi = kPi + C.phiAngle * (u0 - 0.5f);
+        const float theta = 0.5f * kPi + C.thetaAngle * (u1 - 0.5f);
+        float sinPhi, cosPhi, sinTheta, cosTheta;
+        fsincos(phi, &sinPhi, &cosPhi);
+        fsincos(theta, &sinTheta, &cosTheta);
+        *dirPDF = 1.0f / (C.phiAngle * C.thetaAngle * sinTheta);
+        return V3(sinPhi * sinTheta, cosTheta, -cosPhi * sinTheta);
+    }
+    V3 pFocus(C.opWidth * (0.5f - u0), C.opHeight * (0.5f - u1), C.objPlaneDistance);
+    V3 dirLocal = normalize(pFocus - V3(xOnLens, yOnLens, 0.0f));
+    *dirPDF = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
+    return dirLocal;
+}
+
+// Inverse of cameraSampleDir: the screen position a lens-frame direction
+// projects to and its density, false off the frame (evaluatePDFInternal and
+// backProjectDirection, cameras.cu:175-211, :301-341).
+VLRB_HD bool cameraProject(const Camera &C, float xOnLens, float yOnLens, const V3 &dirLocal, float* u0, float* u1,
+                           float* pdf) {
+    if (C.kind == kCameraEquirectangular) {
+        const float theta = acosf(vclamp(dirLocal.y, -1.0f, 1.0f));
+        const float phi = fmodf(atan2f(dirLocal.x, -dirLocal.z) + 2 * kPi, 2 * kPi);
+        *u0 = (phi - kPi) / C.phiAngle + 0.5f;
+        *u1 = (theta - 0.5f * kPi) / C.thetaAngle + 0.5f;
+        if (*u0 < 0.0f || *u0 >= 1.0f || *u1 < 0.0f || *u1 >= 1.0f) return false;
+        const float sinTheta = sqrtf(1.0f - sq(dirLocal.y));
+        *pdf = 1.0f / (C.phiAngle * C.thetaAngle * sinTheta);
+        return true;
+    }
+    if (dirLocal.z <= 0.0f) return false;
+    V3 org(xOnLens, yOnLens, 0.0f);
+    float objZ = C.objPlaneDistance / dirLocal.z;
+    V3 pFocus = dirLocal * objZ + org;
+    *u0 = -pFocus.x / C.opWidth + 0.5f;
+    *u1 = -pFocus.y / C.opHeight + 0.5f;
+    if (*u0 < 0.0f || *u0 >= 1.0f || *u1 < 0.0f || *u1 >= 1.0f) return false;
+    *pdf = sq(C.imgPlaneDistance) / (cube(dirLocal.z) * C.imgPlaneArea);
+    return true;
+}
+
+// SurfacePoint::calcCosTerm at the lens (shared/kernel_common.h:202-204):
+// the equirectangular camera is a point (cosine 1).
+VLRB_HD float lensCos(const Camera &C, const V3 &dirWorld, const V3 &lensNormal) {
+    return C.kind == kCameraEquirectangular ? 1.0f : absDot(dirWorld, lensNormal);
+}
 
 struct SceneBounds {
     V3 lo, hi, center;

@@ -202,7 +202,24 @@ bool initShaderNode(ShaderNode* n, const std::string &type) {
 }
 
 bool initCamera(api::Camera* c, const std::string &type) {
-    if (lower(type) != "perspective") return false;
+    const std::string t = lower(type);
+    if (t == "equirectangular") {
+        // EquirectangularCamera parameters and defaults (scene.cpp:1680-1725)
+        c->type = t;
+        c->addParam("position", kImm, "Point3D");
+        c->addParam("orientation", kImm, "Quaternion");
+        c->addParam("sensitivity", kImm, "Float");
+        c->addParam("h angle", kImm, "Float");
+        c->addParam("v angle", kImm, "Float");
+        c->floats["position"] = { 0, 0, 0 };
+        c->floats["orientation"] = { 0, 0, 0, 1 };
+        c->floats["sensitivity"] = { 1.0f };
+        c->floats["h angle"] = { 2 * kPi };
+        c->floats["v angle"] = { kPi };
+        return true;
+    }
+    if (t != "perspective") return false;
+    c->type = t;
     c->addParam("position", kImm, "Point3D");
     c->addParam("orientation", kImm, "Quaternion");
     c->addParam("aspect", kImm, "Float");

@@ -152,10 +152,15 @@ def build(ctx, desc):
         scene.add_child(node)
         keep.append(node)
     c = desc["camera"]
-    cam = ctx.createCamera("Perspective")
+    if c.get("type", "Perspective") == "Equirectangular":
+        cam = ctx.createCamera("Equirectangular")
+        keys = ("sensitivity", "h angle", "v angle")
+    else:
+        cam = ctx.createCamera("Perspective")
+        keys = ("aspect", "sensitivity", "fovy", "lens radius", "op distance")
     cam.set_point("position", c["position"])
     cam.set_quaternion("orientation", c["orientation"])
-    for k in ("aspect", "sensitivity", "fovy", "lens radius", "op distance"):
+    for k in keys:
         cam.set(k, c[k])
     return scene, cam, keep
 
