@@ -392,6 +392,34 @@ def test_equirectangular_camera_renderers_agree(angles):
     assert np.all(z < 6), z.max()
 
 
+def test_shrunk_preview_fills_the_top_left_region():
+    """vlrContextRender's shrinkCoeff (context.cpp:1414): a first frame with
+    shrinkCoeff 2 renders the image at half size into the film's top-left
+    quarter and keeps that size for the following frames; the rest of the
+    film stays empty.  A film pixel holds its own pixel's integral, so the
+    half-size image carries the same total as the full-size one."""
+    from vlr_b200 import vlr as VV, scenes
+    W = H = 64
+    desc = scenes.cornell_box_desc(W, H)
+    totals = []
+    for shrink in (1, 2):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = scenes.build(ctx, desc)
+        ctx.setScene(scene)
+        ctx.setOptions(max_path_length=8)
+        for f in range(256):
+            n = ctx.render(cam, f == 0, shrink=shrink)
+        assert n == 256
+        y = _y_of(ctx.read_film())
+        if shrink == 2:
+            assert np.all(y[H // 2:, :] == 0) and np.all(y[:, W // 2:] == 0)
+            assert (y[:H // 2, :W // 2] > 0).mean() > 0.5     # the box fills most of the view
+        totals.append(y.sum())
+        ctx.close()
+    assert abs(totals[1] / totals[0] - 1) < 0.03, totals
+
+
 def _trace(v, rays, rounds, any_hit):
     L = V.lib()
     L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

@@ -45,7 +45,8 @@ struct BptArgs {
     float wlPdf;
     uint32_t numLightPaths;
     uint32_t numPaths;
-    uint32_t width, height;
+    uint32_t width, height;   // the image being rendered
+    uint32_t stride;          // film row length in pixels
     uint32_t maxPathLength;
     uint32_t bounce;
     struct LtConnection* conn;   // light tracing: lens connections of the current stage
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
                     S4 c = mis * unweighted;
                     uint32_t ipx = static_cast<uint32_t>(u0 * a.width), ipy = static_cast<uint32_t>(u1 * a.height);
                     if (c.allFinite() && c.hasNonZero() && ipx < a.width && ipy < a.height)
-                        emitConnection(a, 0, sOrg, conDir, tmax, c, kSplatBit | (ipy * a.width + ipx));
+                        emitConnection(a, 0, sOrg, conDir, tmax, c, kSplatBit | (ipy * a.stride + ipx));
                 }
             }
         }
@@ -772,7 +773,8 @@ __global__ void __launch_bounds__(256) eyeFilmKernel(BptArgs a) {
         S4 c = toS4(a.pb.contrib[p]);
         if (!c.allFinite()) continue;
         const uint32_t pixel = p % (a.width * a.height);
-        filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, c);
+        const uint32_t fi = (pixel / a.width) * a.stride + pixel % a.width;
+        filmAdd(a.film.strata + static_cast<size_t>(fi) * kNumStrata, lam, c);
     }
 }
 
@@ -793,8 +795,8 @@ struct LtConnection {
 // frame; else the ray, the pixel, the vertex-side direction in its shading
 // frame and G / lensPDF with G = cos(vertex, geometric) cos(lens) / d^2.
 __device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, float lensAreaPDF, const SurfPt &sp,
-                                               uint32_t W, uint32_t H, V3* dir, V3* org, float* tmax,
-                                               uint32_t* pixel, V3* dirAtVertex, float* scalar) {
+                                               uint32_t W, uint32_t H, uint32_t stride, V3* dir, V3* org,
+                                               float* tmax, uint32_t* pixel, V3* dirAtVertex, float* scalar) {
     SurfPt spE;
     spE.position = L.position;
     spE.gn = L.frame.z;
@@ -807,7 +809,7 @@ __device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, f
     if (!idfProject(C, L, dLens, &u0, &u1, &pdf)) return false;
     const uint32_t ipx = static_cast<uint32_t>(u0 * W), ipy = static_cast<uint32_t>(u1 * H);
     if (ipx >= W || ipy >= H) return false;
-    *pixel = ipy * W + ipx;
+    *pixel = ipy * stride + ipx;
     *dirAtVertex = sp.frame.toLocal(-*dir);
     *scalar = absDot(*dir, sp.gn) * lensCos(C, *dir, L.frame.z) / dist2 / lensAreaPDF;
     return true;
@@ -868,7 +870,8 @@ __global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
             V3 dir, org, dv;
             float tmax, scalar;
             uint32_t pixel;
-            if (lensConnection(C, L, lensPDF, ls.sp, a.width, a.height, &dir, &org, &tmax, &pixel, &dv, &scalar)) {
+            if (lensConnection(C, L, lensPDF, ls.sp, a.width, a.height, a.stride, &dir, &org, &tmax, &pixel, &dv,
+                               &scalar)) {
                 const S4 Le1(dv.z > 0.0f ? 1.0f / kPi : 0.0f);      // DiffuseEDF / EnvironmentEDF evaluate
                 const S4 c = alpha * S4(C.sensitivity) * Le1 * scalar;
                 if (c.allFinite() && c.hasNonZero()) emitLensConnection(a, 0, org, dir, tmax, pixel, c, wls);
@@ -957,7 +960,8 @@ __global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
             V3 dir, org, dv;
             float tmax, scalar;
             uint32_t pixel;
-            if (lensConnection(C, L, lensPDF, sp, a.width, a.height, &dir, &org, &tmax, &pixel, &dv, &scalar)) {
+            if (lensConnection(C, L, lensPDF, sp, a.width, a.height, a.stride, &dir, &org, &tmax, &pixel, &dv,
+                               &scalar)) {
                 const S4 fs = bsdfEval(bsdf, q, gnLocal, dv, nullptr);
                 const S4 c = alpha * S4(C.sensitivity) * fs * scalar;
                 if (c.allFinite() && c.hasNonZero())
@@ -998,7 +1002,7 @@ __global__ void __launch_bounds__(256) ltSplatKernel(BptArgs a, uint32_t stage) 
         const Hit h = traceBvh<true>(a.S.bvh, V3(k.org.x, k.org.y, k.org.z), V3(k.dir.x, k.dir.y, k.dir.z), k.org.w);
         if (h.prim != 0xFFFFFFFFu) continue;
         const uint32_t pixel = __float_as_uint(k.dir.w);
-        if (pixel >= a.width * a.height) continue;
+        if (pixel >= a.stride * a.height) continue;
         const float lam[4] = { k.lambda.x, k.lambda.y, k.lambda.z, k.lambda.w };
         filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, toS4(k.contrib));
     }
@@ -1072,6 +1076,7 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
     a.numLightPaths = numLightPaths;
     a.width = fp.width;
     a.height = fp.height;
+    a.stride = fp.stride;
     a.maxPathLength = fp.maxPathLength;
     // light subpaths
     ck(cudaMemsetAsync(bb.counters, 0, 8, stream), "cache counters");
@@ -1156,6 +1161,7 @@ void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* 
     a.numPaths = numLightPaths;
     a.width = fp.width;
     a.height = fp.height;
+    a.stride = fp.stride;
     a.maxPathLength = fp.maxPathLength;
     a.conn = static_cast<LtConnection*>(connections);
     ck(cudaMemsetAsync(lightPaths.counters, 0, size_t(kMaxBounces + 1) * kCountersPerBounce * 4, stream), "counters");

@@ -657,15 +657,20 @@ void Context::trainGuide(cudaStream_t stream) {
 }
 
 void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
-                     uint32_t samples, uint32_t* numAccumFramesOut) {
+                     uint32_t samples, uint32_t* numAccumFramesOut, uint32_t shrink) {
     if (width == 0 || height == 0) throw std::runtime_error("no output buffer bound");
     if (builtGeneration != generation) buildScene(stream);
+    if (firstFrame || imgW == 0 || imgW > width || imgH > height) {
+        const uint32_t s = std::max<uint32_t>(shrink, 1u);
+        imgW = std::max<uint32_t>(width / s, 1u);
+        imgH = std::max<uint32_t>(height / s, 1u);
+    }
     if (firstFrame) {
         setupCamera(cam);
         numAccumFrames = 0;
         filmClear(filmDesc(), stream);
     }
-    const uint32_t pixels = width * height;
+    const uint32_t pixels = imgW * imgH;
     if (numAccumFrames + samples > limitFrames)
         samples = limitFrames > numAccumFrames ? limitFrames - numAccumFrames : 0;
     Film fl = filmDesc();
@@ -676,8 +681,9 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
         while (done < samples) {
             uint32_t k = std::min(perLaunch, samples - done);
             FrameParams fp{};
-            fp.width = width;
-            fp.height = height;
+            fp.width = imgW;
+            fp.height = imgH;
+            fp.stride = width;
             fp.sppPerLaunch = k;
             fp.numPaths = pixels * k;
             fp.maxPathLength = options.maxPathLength;

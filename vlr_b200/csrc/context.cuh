@@ -84,8 +84,11 @@ public:
     void bindOutput(uint32_t w, uint32_t h);
     void setScene(Scene* s) { scene = s; markDirty(); }
     void markDirty() { ++generation; }
+    // shrink: on a first frame, render the image at 1/shrink of the output
+    // size into the film's top-left region until the next first frame
+    // (vlrContextRender's shrinkCoeff, context.cpp:1414)
     void render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
-                uint32_t samples, uint32_t* numAccumFrames);
+                uint32_t samples, uint32_t* numAccumFrames, uint32_t shrink = 1);
     // Times short renders over a grid of (paths in flight, blocks per SM),
     // keeps the fastest in `options`, and returns every trial.  Leaves the
     // film holding the last trial (the next firstFrame render clears it).
@@ -107,6 +110,7 @@ public:
     bool logging;
     int device = 0, numSMs = 148;
     uint32_t width = 0, height = 0;
+    uint32_t imgW = 0, imgH = 0;    // the image being rendered (width, height unless shrunk)
     Scene* scene = nullptr;
     VLRRenderer renderer = VLRRenderer_PathTracing;
     RenderOptions options;

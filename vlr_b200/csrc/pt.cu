@@ -583,7 +583,8 @@ __global__ void __launch_bounds__(256) filmKernel(PathBuffers pb, Film film, Fra
         float4 l = pb.lambda[p];
         float lam[4] = { l.x, l.y, l.z, l.w };
         const uint32_t pixel = pixelOfPath(p, fp.width, fp.height);
-        double* dst = film.strata + static_cast<size_t>(pixel) * kNumStrata;
+        const uint32_t fi = (pixel / fp.width) * fp.stride + pixel % fp.width;
+        double* dst = film.strata + static_cast<size_t>(fi) * kNumStrata;
         for (int i = 0; i < 4; ++i) {
             uint32_t bin = vmin<uint32_t>(static_cast<uint32_t>((lam[i] - kWavelengthLow) /
                                           (kWavelengthHigh - kWavelengthLow) * kNumStrata), kNumStrata - 1);

@@ -45,7 +45,8 @@ struct PathBuffers {
 };
 
 struct FrameParams {
-    uint32_t width, height;
+    uint32_t width, height;   // the image being rendered (the film's top-left region when shrunk)
+    uint32_t stride;          // film row length in pixels
     uint32_t sppPerLaunch;    // paths per pixel in this launch
     uint32_t numPaths;        // width * height * sppPerLaunch
     uint32_t maxPathLength;   // hits after which a path stops scattering

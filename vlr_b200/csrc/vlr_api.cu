@@ -401,10 +401,11 @@ VLRResult vlrContextRender(VLRContext context, CUstream stream, VLRCameraConst c
     VLRResult e2 = VLRResult_NoError;
     const api::Camera* cam = checked<const api::Camera>(camera, &e2, kindCamera);
     if (!cam || !numAccumFrames) return VLRResult_InvalidArgument;
-    (void)denoise;
-    if (shrinkCoeff > 1) return VLRResult_InvalidArgument;
+    (void)denoise;   // the OptiX denoiser is not part of this library
+    if (shrinkCoeff == 0) return VLRResult_InvalidArgument;
     API_TRY
-    c->render(reinterpret_cast<cudaStream_t>(stream), cam, firstFrame, limitNumAccumFrames, 1, numAccumFrames);
+    c->render(reinterpret_cast<cudaStream_t>(stream), cam, firstFrame, limitNumAccumFrames, 1, numAccumFrames,
+              shrinkCoeff);
     return VLRResult_NoError;
     API_CATCH("vlrContextRender")
 }

@@ -387,10 +387,11 @@ class Context:
         check(_api().vlrbContextGetGuidingStats(self.h, ctypes.byref(st)), "getGuidingStats")
         return {k: getattr(st, k) for k, _ in VLRBGuidingStats._fields_}
 
-    def render(self, camera, first_frame, limit=1 << 30, stream=0):
-        """One sample per pixel, exactly like vlrContextRender."""
+    def render(self, camera, first_frame, limit=1 << 30, stream=0, shrink=1):
+        """One sample per pixel, exactly like vlrContextRender (shrink: the
+        shrinkCoeff preview, fixed at a first frame)."""
         n = ctypes.c_uint32()
-        check(_api().vlrContextRender(self.h, c_void_p(stream), camera.h, False, 1, first_frame, limit,
+        check(_api().vlrContextRender(self.h, c_void_p(stream), camera.h, False, shrink, first_frame, limit,
                                       ctypes.byref(n)), "vlrContextRender")
         return n.value
 
