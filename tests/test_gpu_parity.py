@@ -420,6 +420,105 @@ def test_shrunk_preview_fills_the_top_left_region():
     assert abs(totals[1] / totals[0] - 1) < 0.03, totals
 
 
+def _point_lit_box(ctx, W, H, emitter):
+    """The diffuse Cornell box lit only by a PointSurfaceNode with one point
+    at (0, 2.4, 0) ("point") or by the ceiling quad with a directional
+    emitter facing down ("directional")."""
+    from vlr_b200 import vlr as VV, scenes
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    if emitter == "directional":
+        desc["materials"]["light"] = ("DirectionalEmitter", {"emittance": ("Rec709(D65)", 5.0, 5.0, 5.0)})
+    else:
+        desc["materials"]["light"] = ("Matte", {"albedo": ("Rec709(D65)", 0.8, 0.8, 0.8)})
+    scene, cam, keep = scenes.build(ctx, desc)
+    if emitter == "point":
+        mat = ctx.createSurfaceMaterial("PointEmitter")
+        mat.set("intensity", VV.Spectrum("Rec709(D65)", 4.0, 4.0, 4.0))
+        pts = ctx.createPointSurfaceNode("bulb")
+        pts.set_vertices(np.array([[0.0, 2.4, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0]], np.float32))
+        pts.add_material_group([0], mat)
+        scene.add_child(pts)
+        keep += [mat, pts]
+    return scene, cam, keep
+
+
+def test_point_light_path_tracing_and_light_tracing_agree():
+    """A point emitter (PointSurfaceNode + PointEmitter, point.cu:40-80 and
+    materials.cu:2166-2250): path tracing reaches it only by next-event
+    estimation (a delta position), the light tracer starts its subpaths there
+    with uniform-sphere emission; the two images must agree (whole image
+    within 2%, lit 8x8 blocks within 6 combined standard errors).  LVC-BPT
+    reports that it does not render point emitters."""
+    from vlr_b200 import vlr as VV
+    W = H = 64
+    images = []
+    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = _point_lit_box(ctx, W, H, "point")
+        ctx.setScene(scene)
+        ctx.setRenderer(renderer)
+        ctx.setOptions(max_path_length=6)
+        ctx.render_samples(cam, True, 1024)
+        y = _y_of(ctx.read_film())
+        assert np.isfinite(y).all() and y.sum() > 0
+        images.append(y)
+        ctx.close()
+    c, g = images
+    # The light tracer also draws the point itself (its first lens
+    # connection): the camera at (0, 1.5, 6) with a 40-degree field of view
+    # sees (0, 2.4, 0) at column 32, row 64 (0.5 - tan(atan(0.9 / 6)) /
+    # (2 tan 20 deg)) = 18.8.  Path tracing never reaches a point; compare
+    # everything else.
+    row = int(64 * (0.5 - (0.9 / 6.0) / (2 * np.tan(np.radians(20.0)))))
+    assert g[row - 1:row + 2, 30:34].max() == g.max()
+    mask = np.ones_like(g, bool)
+    mask[row - 2:row + 3, 29:35] = False
+    g, c = g * mask, c * mask
+    assert abs(g.sum() / c.sum() - 1) < 0.02, g.sum() / c.sum()
+    gb = g.reshape(8, 8, 8, 8).sum(axis=(1, 3))
+    cb = c.reshape(8, 8, 8, 8).sum(axis=(1, 3))
+    sg = g.reshape(8, 8, 8, 8).std(axis=(1, 3)) * 8
+    sc = c.reshape(8, 8, 8, 8).std(axis=(1, 3)) * 8
+    lit = cb > 1e-3 * cb.max()
+    z = np.abs(gb - cb)[lit] / np.sqrt(sg[lit] ** 2 + sc[lit] ** 2 + (1e-3 * cb[lit]) ** 2)
+    assert np.all(z < 6), z.max()
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = _point_lit_box(ctx, W, H, "point")
+    ctx.setScene(scene)
+    ctx.setRenderer(VV.RENDERER_BPT)
+    with pytest.raises(VV.VLRError):
+        ctx.render_samples(cam, True, 1)
+    ctx.close()
+
+
+def test_directional_emitter_is_seen_by_light_subpaths_only():
+    """A directional emitter (materials.cu:2097-2160) emits along a delta
+    direction and evaluates to zero elsewhere: path tracing, which can only
+    hit emitters or sample their surfaces, gets no light from it, while the
+    light tracer's subpaths leave it along the normal and light the room."""
+    from vlr_b200 import vlr as VV
+    W = H = 32
+    sums = []
+    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = _point_lit_box(ctx, W, H, "directional")
+        ctx.setScene(scene)
+        ctx.setRenderer(renderer)
+        ctx.setOptions(max_path_length=6)
+        ctx.render_samples(cam, True, 64)
+        y = _y_of(ctx.read_film())
+        assert np.isfinite(y).all()
+        sums.append(y.sum())
+        ctx.close()
+    assert sums[0] == 0.0
+    assert sums[1] > 0.0
+
+
 def _trace(v, rays, rounds, any_hit):
     L = V.lib()
     L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

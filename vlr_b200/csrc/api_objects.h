@@ -115,6 +115,7 @@ struct TriangleMeshNode : Node {
 
 struct PointNode : Node {
     std::vector<VLRVertex> vertices;
+    std::vector<MaterialGroup> groups;   // indices are point (vertex) indices
     PointNode() : Node(Kind::PointSurfaceNode) {}
 };
 

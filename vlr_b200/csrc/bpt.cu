@@ -230,6 +230,7 @@ __global__ void __launch_bounds__(256) lightStartKernel(BptArgs a) {
             ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
             ls.material = S.envMaterial;
             ls.delta = false;
+            ls.isPoint = false;
             Le0 = kPi * envRadiance(S, uu, vv, a.wls) * S.mats[S.envMaterial].emitScale;
         }
         else {
@@ -795,8 +796,9 @@ struct LtConnection {
 // frame; else the ray, the pixel, the vertex-side direction in its shading
 // frame and G / lensPDF with G = cos(vertex, geometric) cos(lens) / d^2.
 __device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, float lensAreaPDF, const SurfPt &sp,
-                                               uint32_t W, uint32_t H, uint32_t stride, V3* dir, V3* org,
-                                               float* tmax, uint32_t* pixel, V3* dirAtVertex, float* scalar) {
+                                               bool vertexIsPoint, uint32_t W, uint32_t H, uint32_t stride, V3* dir,
+                                               V3* org, float* tmax, uint32_t* pixel, V3* dirAtVertex,
+                                               float* scalar) {
     SurfPt spE;
     spE.position = L.position;
     spE.gn = L.frame.z;
@@ -811,7 +813,7 @@ __device__ __forceinline__ bool lensConnection(const Camera &C, const Lens &L, f
     if (ipx >= W || ipy >= H) return false;
     *pixel = ipy * stride + ipx;
     *dirAtVertex = sp.frame.toLocal(-*dir);
-    *scalar = absDot(*dir, sp.gn) * lensCos(C, *dir, L.frame.z) / dist2 / lensAreaPDF;
+    *scalar = (vertexIsPoint ? 1.0f : absDot(*dir, sp.gn)) * lensCos(C, *dir, L.frame.z) / dist2 / lensAreaPDF;
     return true;
 }
 
@@ -855,6 +857,7 @@ __global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
             ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
             ls.material = S.envMaterial;
             ls.delta = false;
+            ls.isPoint = false;
             Le0 = kPi * envRadiance(S, uu, vv, wls) * S.mats[S.envMaterial].emitScale;
         }
         else {
@@ -862,6 +865,7 @@ __global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
             sampleTriangleGroup(S, grp, uPrim, ue0, ue1, &ls);
             Le0 = emittance(S.meng, S.mats[ls.material], wls);
         }
+        const uint32_t emitter = S.mats[ls.material].emitter;
         S4 alpha = Le0 / (a.numLightPaths * lightProb * ls.areaPDF * selectWLPDF);
         // explicit lens sampling from the light point (light_tracing.cu:70-106)
         {
@@ -870,23 +874,35 @@ __global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
             V3 dir, org, dv;
             float tmax, scalar;
             uint32_t pixel;
-            if (lensConnection(C, L, lensPDF, ls.sp, a.width, a.height, a.stride, &dir, &org, &tmax, &pixel, &dv,
-                               &scalar)) {
-                const S4 Le1(dv.z > 0.0f ? 1.0f / kPi : 0.0f);      // DiffuseEDF / EnvironmentEDF evaluate
+            if (lensConnection(C, L, lensPDF, ls.sp, ls.isPoint, a.width, a.height, a.stride, &dir, &org, &tmax,
+                               &pixel, &dv, &scalar)) {
+                const S4 Le1(edfEval(emitter, dv));
                 const S4 c = alpha * S4(C.sensitivity) * Le1 * scalar;
                 if (c.allFinite() && c.hasNonZero()) emitLensConnection(a, 0, org, dir, tmax, pixel, c, wls);
             }
         }
-        // emission direction (as the LVC light subpaths)
+        // emission direction: the EDF's sample (materials.cu:2057-2066 diffuse,
+        // :2110-2125 directional, :2190-2196 point, :2844-2857 environment)
         float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
         (void)uc;
         V3 dirLocal;
         float dirPDF;
+        float feValue = 1.0f / kPi;
         if (env) {
             float dx, dy;
             concentricDisk(ud0, ud1, &dx, &dy);
             dirLocal = V3(S.bounds.worldRadius * dx, S.bounds.worldRadius * dy, 1.0f);
             dirPDF = 1.0f / S.bounds.worldDiscArea;
+        }
+        else if (emitter == kEmitPoint) {
+            dirLocal = uniformSphere(ud0, ud1);
+            dirPDF = 1.0f / (4 * kPi);
+            feValue = 1.0f / (4 * kPi);
+        }
+        else if (emitter == kEmitDirectional) {
+            dirLocal = V3(0.0f, 0.0f, 1.0f);
+            dirPDF = 1.0f;
+            feValue = 1.0f;
         }
         else {
             dirLocal = cosineHemisphere(ud0, ud1);
@@ -900,7 +916,7 @@ __global__ void __launch_bounds__(256) ltStartKernel(BptArgs a) {
             dirLocal.y = 0;
         }
         const V3 rayDir = ls.sp.frame.fromLocal(dirLocal);
-        alpha *= S4(1.0f / kPi) * (absDot(rayDir, ls.sp.gn) / dirPDF);
+        alpha *= S4(feValue) * ((ls.isPoint ? 1.0f : absDot(rayDir, ls.sp.gn)) / dirPDF);
         a.pb.rng[p] = rng.state;
         a.pb.alpha[p] = toF4(alpha);
         a.pb.lambda[p] = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
@@ -960,8 +976,8 @@ __global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
             V3 dir, org, dv;
             float tmax, scalar;
             uint32_t pixel;
-            if (lensConnection(C, L, lensPDF, sp, a.width, a.height, a.stride, &dir, &org, &tmax, &pixel, &dv,
-                               &scalar)) {
+            if (lensConnection(C, L, lensPDF, sp, false, a.width, a.height, a.stride, &dir, &org, &tmax, &pixel,
+                               &dv, &scalar)) {
                 const S4 fs = bsdfEval(bsdf, q, gnLocal, dv, nullptr);
                 const S4 c = alpha * S4(C.sensitivity) * fs * scalar;
                 if (c.allFinite() && c.hasNonZero())
@@ -1063,6 +1079,9 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
         throw std::runtime_error("maxPathLength out of range");
     if (scene.lightInsts.n == 0)
         throw std::runtime_error("LVC-BPT needs at least one light");
+    if (scene.hasDeltaEmitters)
+        throw std::runtime_error("LVC-BPT here does not render point or directional emitters "
+                                 "(path tracing and light tracing do)");
     StageTimer dummy;
     StageTimer &T = timer ? *timer : dummy;
     const int grid = numSMs * static_cast<int>(fp.blocksPerSM ? fp.blocksPerSM : 8);

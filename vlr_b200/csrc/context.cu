@@ -251,6 +251,16 @@ MatDesc describeMaterial(const SurfaceMaterial* m) {
         d.emit = upsampleImm(spec("emittance"), SpType::LightSource);
         d.emitScale = m->getFloat("scale", 1.0f);
     }
+    else if (t == "pointemitter") {
+        d.emitter = kEmitPoint;
+        d.emit = upsampleImm(spec("intensity"), SpType::LightSource);
+        d.emitScale = m->getFloat("scale", 1.0f);
+    }
+    else if (t == "directionalemitter") {
+        d.emitter = kEmitDirectional;
+        d.emit = upsampleImm(spec("emittance"), SpType::LightSource);
+        d.emitScale = m->getFloat("scale", 1.0f);
+    }
     else if (t == "environmentemitter") {
         d.emitter = 2;
         d.emit = upsampleImm(spec("emittance"), SpType::LightSource);
@@ -271,6 +281,8 @@ struct FlatScene {
     std::vector<uint32_t> geomInstMaterial;
     std::vector<std::vector<uint32_t>> geomInstTris;
     std::vector<std::vector<float>> geomInstAreas;
+    std::vector<uint32_t> geomInstPoints;        // 1: the geometry instance is points (ids into pt*)
+    std::vector<float4> ptPos, ptNrm, ptTan;     // points of PointSurfaceNodes, world space
     uint32_t numInstances = 0;
     V3 lo{ FLT_MAX, FLT_MAX, FLT_MAX }, hi{ -FLT_MAX, -FLT_MAX, -FLT_MAX };
 };
@@ -306,6 +318,7 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
             f.geomInstMaterial.push_back(mi);
             f.geomInstTris.emplace_back();
             f.geomInstAreas.emplace_back();
+            f.geomInstPoints.push_back(0u);
             for (size_t k = 0; k + 2 < g.indices.size(); k += 3) {
                 uint32_t i0 = g.indices[k], i1 = g.indices[k + 1], i2 = g.indices[k + 2];
                 if (i0 >= mesh->vertices.size() || i1 >= mesh->vertices.size() || i2 >= mesh->vertices.size())
@@ -322,6 +335,38 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
                 V3 e2(vc.position.x - va.position.x, vc.position.y - va.position.y, vc.position.z - va.position.z);
                 f.geomInstTris.back().push_back(t);
                 f.geomInstAreas.back().push_back(0.5f * cross(e1, e2).length());
+            }
+        }
+        return;
+    }
+    if (n->kind == Kind::PointSurfaceNode) {
+        // points are light sources only: rays never hit them (point.cu:40-80
+        // samples them; a point of zero radius has no intersection)
+        const auto* pts = static_cast<const PointNode*>(n);
+        const uint32_t inst = f.numInstances++;
+        const uint32_t base = static_cast<uint32_t>(f.ptPos.size());
+        for (const VLRVertex &v : pts->vertices) {
+            V3 p = xfPoint(world, V3(v.position.x, v.position.y, v.position.z));
+            V3 nn = xfNormal(worldInv, V3(v.normal.x, v.normal.y, v.normal.z));
+            V3 tt = xfVector(world, V3(v.tc0Direction.x, v.tc0Direction.y, v.tc0Direction.z));
+            f.ptPos.push_back(make_float4(p.x, p.y, p.z, 0.0f));
+            f.ptNrm.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
+            f.ptTan.push_back(make_float4(tt.x, tt.y, tt.z, 0.0f));
+            f.lo = vmin3(f.lo, p);
+            f.hi = vmax3(f.hi, p);
+        }
+        for (const MaterialGroup &g : pts->groups) {
+            if (!g.material) continue;
+            const uint32_t mi = materialIndex(f, g.material);
+            f.geomInstInstance.push_back(inst);
+            f.geomInstMaterial.push_back(mi);
+            f.geomInstTris.emplace_back();
+            f.geomInstAreas.emplace_back();
+            f.geomInstPoints.push_back(1u);
+            for (uint32_t idx : g.indices) {
+                if (idx >= pts->vertices.size()) throw std::runtime_error("point index out of range");
+                f.geomInstTris.back().push_back(base + idx);
+                f.geomInstAreas.back().push_back(1.0f);   // uniform over the group's points (scene.cpp:380-393)
             }
         }
         return;
@@ -388,6 +433,9 @@ void Context::buildScene(cudaStream_t stream) {
             eg.firstTri = static_cast<uint32_t>(lightTris.size());
             eg.numTris = static_cast<uint32_t>(f.geomInstTris[g].size());
             eg.material = f.geomInstMaterial[g];
+            eg.points = f.geomInstPoints[g];
+            const uint32_t kind = f.mats[eg.material].emitter;
+            if (kind == kEmitPoint || kind == kEmitDirectional) sg.hasDeltaEmitters = 1u;
             lightTris.insert(lightTris.end(), f.geomInstTris[g].begin(), f.geomInstTris[g].end());
             groupDists.push_back(makeDist(f.geomInstAreas[g]));
             groups.push_back(eg);
@@ -432,6 +480,9 @@ void Context::buildScene(cudaStream_t stream) {
     geomInstGroup.push_back(0xFFFFFFFFu);
     sg.geomInstGroup = upload(geomInstGroup, stream);
     sg.lightTris = upload(lightTris, stream);
+    sg.ptPos = upload(f.ptPos, stream);
+    sg.ptNrm = upload(f.ptNrm, stream);
+    sg.ptTan = upload(f.ptTan, stream);
 
     // ---- geometry
     sg.numTris = numTris;

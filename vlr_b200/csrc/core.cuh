@@ -1217,6 +1217,27 @@ VLRB_HD float bsdfPDF(const Bsdf &B, const BsdfQuery &q, const V3 &d, float* rev
 // ---------------------------------------------------------------- EDFs
 // DiffuseEDF (materials.cu:2040-2093): Le = M / pi on the front hemisphere.
 VLRB_HD float diffuseEdfEval(const V3 &dirLocal) { return dirLocal.z > 0.0f ? 1.0f / kPi : 0.0f; }
+
+// uniformSampleSphere (random_distributions.h:141-145): theta = acos(1 - 2 u0),
+// phi = 2 pi u1, z up.
+VLRB_HD V3 uniformSphere(float u0, float u1) {
+    const float phi = 2 * kPi * u1, theta = acosf(1 - 2 * u0);
+    float sinPhi, cosPhi, sinTheta, cosTheta;
+    fsincos(phi, &sinPhi, &cosPhi);
+    fsincos(theta, &sinTheta, &cosTheta);
+    return V3(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+}
+
+// Emitter kinds (MatDesc::emitter) and their EDFs' directional factors
+// (materials.cu:2040-2250, 2830-2893): diffuse and environment 1/pi on the
+// front side, a point 1/(4 pi) everywhere, a directional emitter 0 (its
+// emission is a delta direction: only light subpaths carry it).
+enum : uint32_t { kEmitNone = 0, kEmitDiffuse = 1, kEmitEnvironment = 2, kEmitPoint = 3, kEmitDirectional = 4 };
+VLRB_HD float edfEval(uint32_t emitter, const V3 &dirLocal) {
+    if (emitter == kEmitPoint) return 1.0f / (4 * kPi);
+    if (emitter == kEmitDirectional) return 0.0f;
+    return diffuseEdfEval(dirLocal);
+}
 VLRB_HD float diffuseEdfPDF(const V3 &dirLocal) { return dirLocal.z <= 0.0f ? 0.0f : dirLocal.z / kPi; }
 
 } // namespace vlrb

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         // implicit light sampling
         S4 spEmittance = emittance(S.meng, mat, wls);
         if (spEmittance.hasNonZero()) {
-            S4 Le = spEmittance * diffuseEdfEval(dirOutLocal);
+            S4 Le = spEmittance * edfEval(mat.emitter, dirOutLocal);
             float MIS = 1.0f;
             if (!dir::isDelta(pb.prevType[p]) && pathLength > 1) {
                 float bsdfPDF = pb.prevDirPDF[p];
@@ -300,6 +300,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
                 ls.sp.atInfinity = true;
                 ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
                 ls.delta = false;
+                ls.isPoint = false;
                 ls.material = S.envMaterial;
                 M = kPi * envRadiance(S, uu, vv, wls) * S.mats[S.envMaterial].emitScale;
                 ok = uvPDF > 0.0f;
@@ -333,10 +334,10 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
                 float recSqDist = 1.0f / dist2;
                 V3 dirL = ls.sp.atInfinity ? V3(0.0f, 0.0f, 1.0f) : ls.sp.frame.toLocal(-shadowDir);
                 V3 dirSn = sp.frame.toLocal(shadowDir);
-                S4 Le = M * diffuseEdfEval(dirL);
+                S4 Le = M * edfEval(S.mats[ls.material].emitter, dirL);
                 float lightPDF = lightProb * ls.areaPDF;
                 S4 fs = bsdfEval(bsdf, q, gnLocal, dirSn, nullptr);
-                float cosLight = ls.sp.atInfinity ? absDot(-shadowDir, ls.sp.gn) : absDot(-shadowDir, ls.sp.gn);
+                float cosLight = ls.isPoint ? 1.0f : absDot(-shadowDir, ls.sp.gn);
                 float dirPdfV = bsdfPDF(bsdf, q, dirSn, nullptr);
                 if constexpr (kGuide) {
                     if (guided) dirPdfV = 0.5f * dirPdfV + 0.5f * guide::mixturePdf(mix, shadowDir);

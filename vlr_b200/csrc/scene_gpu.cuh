@@ -73,8 +73,8 @@ struct EmitGroup {
     uint32_t firstTri;        // offset into lightTris
     uint32_t numTris;
     uint32_t material;
-    uint32_t pad;
-    Dist1D prims;             // area distribution over the group's triangles
+    uint32_t points;          // 1: the group is points (lightTris holds point ids), 0: triangles
+    Dist1D prims;             // area distribution over the group's triangles (uniform over points)
 };
 
 enum : uint32_t { kCameraPerspective = 0, kCameraEquirectangular = 1 };
@@ -164,7 +164,11 @@ struct SceneGPU {
     const EmitGroup* groups;        // emitting material groups
     const float* geomLightPdfArea;  // per geomInst: instProb * groupProb / groupArea (0: not emitting)
     const uint32_t* geomInstGroup;  // per geomInst: emitting group index or ~0
-    const uint32_t* lightTris;      // triangle ids of all emitting groups
+    const uint32_t* lightTris;      // triangle ids of all emitting groups (point ids for point groups)
+    const float4* ptPos;            // emitting points (PointSurfaceNode), world space
+    const float4* ptNrm;
+    const float4* ptTan;
+    uint32_t hasDeltaEmitters;      // point or directional emitters present
     int32_t envInst;                // light-instance index of the environment, -1 if none
     uint32_t envMaterial;
     float envRotation;
@@ -232,7 +236,7 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
 }
 
 VLRB_HD S4 emittance(const MengTables &T, const MatDesc &m, const WLS &wls) {
-    if (m.emitter == 0) return S4::zero();
+    if (m.emitter == kEmitNone) return S4::zero();
     return matSpectrum(T, m, 3, wls) * m.emitScale;
 }
 
@@ -302,6 +306,7 @@ struct LightSample {
     float areaPDF;
     uint32_t material;
     bool delta;
+    bool isPoint;            // calcCosTerm is 1 at a point (kernel_common.h:202-204)
 };
 
 // Sample a point on an emitting triangle group (triangle.cu:113-177).
@@ -310,6 +315,26 @@ __device__ __forceinline__ void sampleTriangleGroup(const SceneGPU &S, uint32_t 
     const EmitGroup &G = S.groups[grp];
     float primProb;
     uint32_t local = G.prims.sample(uElem, &primProb, nullptr);
+    ls->isPoint = false;
+    if (G.points) {
+        // samplePoint (point.cu:40-80): a delta position with the
+        // hypothetical area of a unit sphere
+        const uint32_t pt = __ldg(S.lightTris + G.firstTri + local);
+        ls->areaPDF = primProb / (4 * kPi);
+        ls->material = G.material;
+        ls->delta = true;
+        ls->isPoint = true;
+        const V3 n = normalize(ld3(S.ptNrm, pt)), t = normalize(ld3(S.ptTan, pt));
+        ls->sp.position = ld3(S.ptPos, pt);
+        ls->sp.frame = Frame(t, n);
+        ls->sp.gn = n;
+        ls->sp.prim = pt;
+        ls->sp.geomInst = 0;
+        ls->sp.u = 0.0f;
+        ls->sp.v = 0.0f;
+        ls->sp.atInfinity = false;
+        return;
+    }
     uint32_t prim = __ldg(S.lightTris + G.firstTri + local);
     uint4 t = __ldg(S.tri + prim);
     V3 p0 = ld3(S.pos, t.x), p1 = ld3(S.pos, t.y), p2 = ld3(S.pos, t.z);

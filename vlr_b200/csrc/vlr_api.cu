@@ -172,8 +172,24 @@ bool initMaterial(SurfaceMaterial* m, const std::string &type) {
         setSpectrumDefault(m, "emittance", pi, pi, pi);
         m->floats["scale"] = { 1.0f };
     }
+    else if (t == "pointemitter") {
+        // PointEmitterSurfaceMaterial (materials.cpp:1900-1945)
+        m->addParam("intensity", kBoth, "Spectrum");
+        m->addParam("scale", kImm, "Float");
+        setSpectrumDefault(m, "intensity", pi, pi, pi);
+        m->floats["scale"] = { 1.0f };
+    }
+    else if (t == "directionalemitter") {
+        // DirectionalEmitterSurfaceMaterial (materials.cpp:1729-1763)
+        m->addParam("emittance", kBoth, "Spectrum");
+        m->addParam("scale", kImm, "Float");
+        m->addParam("direction", kBoth, "Vector3D");
+        setSpectrumDefault(m, "emittance", pi, pi, pi);
+        m->floats["scale"] = { 1.0f };
+        m->floats["direction"] = { 0.0f, 0.0f, 1.0f };
+    }
     else {
-        // OldStyle, Multi, DirectionalEmitter, PointEmitter: not rendered here.
+        // OldStyle, Multi: not rendered here.
         return false;
     }
     return true;
@@ -996,9 +1012,18 @@ VLRResult vlrPointSurfaceNodeSetVertices(VLRPointSurfaceNode surfaceNode, const 
 VLRResult vlrPointSurfaceNodeAddMaterialGroup(VLRPointSurfaceNode surfaceNode, const uint32_t* indices,
                                               uint32_t numIndices, VLRSurfaceMaterialConst material) {
     CHECK_HANDLE(n, PointNode, kindPoint, surfaceNode);
-    (void)n; (void)indices; (void)numIndices; (void)material;
-    // Point emitters are not rendered by this library.
-    return VLRResult_InvalidArgument;
+    if (!indices && numIndices > 0) return VLRResult_InvalidArgument;
+    VLRResult e2 = VLRResult_NoError;
+    const SurfaceMaterial* m = checked<const SurfaceMaterial>(material, &e2, kindMaterial);
+    if (!m) return e2;
+    API_TRY
+    MaterialGroup g;
+    g.indices.assign(indices, indices + numIndices);
+    g.material = m;
+    n->groups.push_back(std::move(g));
+    touch(n);
+    return VLRResult_NoError;
+    API_CATCH("vlrPointSurfaceNodeAddMaterialGroup")
 }
 
 VLRResult vlrParentNodeSetTransform(VLRParentNode node, VLRTransformConst localToWorld) {

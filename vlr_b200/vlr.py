@@ -104,6 +104,9 @@ def _api():
         "vlrTriangleMeshSurfaceNodeSetVertices": [v, v, ctypes.c_uint32],
         "vlrTriangleMeshSurfaceNodeAddMaterialGroup": [v, v, ctypes.c_uint32, v, VLRShaderNodePlug,
                                                        VLRShaderNodePlug, VLRShaderNodePlug],
+        "vlrPointSurfaceNodeCreate": [v, ctypes.c_char_p, ctypes.POINTER(v)],
+        "vlrPointSurfaceNodeSetVertices": [v, v, ctypes.c_uint32],
+        "vlrPointSurfaceNodeAddMaterialGroup": [v, v, ctypes.c_uint32, v],
         "vlrInternalNodeCreate": [v, ctypes.c_char_p, v, ctypes.POINTER(v)],
         "vlrParentNodeAddChild": [v, v],
         "vlrSceneCreate": [v, v, ctypes.POINTER(v)],
@@ -227,6 +230,25 @@ class TriangleMesh:
             "addMaterialGroup")
 
 
+class PointSet:
+    """A PointSurfaceNode: points that emit with a point-emitter material."""
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = handle
+
+    def set_vertices(self, verts):
+        """verts: float32 array (n, 11): position, normal, tc0Direction, texCoord."""
+        a = np.ascontiguousarray(verts, dtype=np.float32)
+        assert a.ndim == 2 and a.shape[1] == 11
+        self._verts = a
+        check(_api().vlrPointSurfaceNodeSetVertices(self.h, a.ctypes.data_as(c_void_p), a.shape[0]), "setVertices")
+
+    def add_material_group(self, indices, material):
+        idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        check(_api().vlrPointSurfaceNodeAddMaterialGroup(self.h, idx.ctypes.data_as(c_void_p), idx.size, material.h),
+              "addMaterialGroup")
+
+
 class ParentNode:
     def __init__(self, ctx, handle):
         self.ctx = ctx
@@ -295,6 +317,9 @@ class Context:
 
     def createTriangleMeshSurfaceNode(self, name):
         return TriangleMesh(self, self._new("vlrTriangleMeshSurfaceNodeCreate", name.encode()))
+
+    def createPointSurfaceNode(self, name):
+        return PointSet(self, self._new("vlrPointSurfaceNodeCreate", name.encode()))
 
     def createSurfaceMaterial(self, type_name):
         return Queryable(self, self._new("vlrSurfaceMaterialCreate", type_name.encode()))
