@@ -444,17 +444,19 @@ def _point_lit_box(ctx, W, H, emitter):
     return scene, cam, keep
 
 
-def test_point_light_path_tracing_and_light_tracing_agree():
+@pytest.mark.parametrize("other", ["light_tracing", "bpt"])
+def test_point_light_renderers_agree(other):
     """A point emitter (PointSurfaceNode + PointEmitter, point.cu:40-80 and
     materials.cu:2166-2250): path tracing reaches it only by next-event
-    estimation (a delta position), the light tracer starts its subpaths there
-    with uniform-sphere emission; the two images must agree (whole image
-    within 2%, lit 8x8 blocks within 6 combined standard errors).  LVC-BPT
-    reports that it does not render point emitters."""
+    estimation (a delta position); the light tracer and LVC-BPT start light
+    subpaths there with uniform-sphere emission and a delta origin in the MIS
+    recursion.  Each must agree with path tracing (whole image within 2%, lit
+    8x8 blocks within 6 combined standard errors)."""
     from vlr_b200 import vlr as VV
     W = H = 64
     images = []
-    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING):
+    second = VV.RENDERER_LIGHT_TRACING if other == "light_tracing" else VV.RENDERER_BPT
+    for renderer in (VV.RENDERER_PATH_TRACING, second):
         ctx = VV.Context()
         ctx.bindOutputBuffer(W, H)
         scene, cam, keep = _point_lit_box(ctx, W, H, "point")
@@ -467,8 +469,8 @@ def test_point_light_path_tracing_and_light_tracing_agree():
         images.append(y)
         ctx.close()
     c, g = images
-    # The light tracer also draws the point itself (its first lens
-    # connection): the camera at (0, 1.5, 6) with a 40-degree field of view
+    # The light tracer and LVC-BPT also draw the point itself (a lens
+    # connection of the light point): the camera at (0, 1.5, 6) with a 40-degree field of view
     # sees (0, 2.4, 0) at column 32, row 64 (0.5 - tan(atan(0.9 / 6)) /
     # (2 tan 20 deg)) = 18.8.  Path tracing never reaches a point; compare
     # everything else.
@@ -485,38 +487,32 @@ def test_point_light_path_tracing_and_light_tracing_agree():
     lit = cb > 1e-3 * cb.max()
     z = np.abs(gb - cb)[lit] / np.sqrt(sg[lit] ** 2 + sc[lit] ** 2 + (1e-3 * cb[lit]) ** 2)
     assert np.all(z < 6), z.max()
-    ctx = VV.Context()
-    ctx.bindOutputBuffer(W, H)
-    scene, cam, keep = _point_lit_box(ctx, W, H, "point")
-    ctx.setScene(scene)
-    ctx.setRenderer(VV.RENDERER_BPT)
-    with pytest.raises(VV.VLRError):
-        ctx.render_samples(cam, True, 1)
-    ctx.close()
 
 
 def test_directional_emitter_is_seen_by_light_subpaths_only():
     """A directional emitter (materials.cu:2097-2160) emits along a delta
     direction and evaluates to zero elsewhere: path tracing, which can only
     hit emitters or sample their surfaces, gets no light from it, while the
-    light tracer's subpaths leave it along the normal and light the room."""
+    light subpaths of the light tracer and LVC-BPT leave it along the normal
+    and light the room (the same total in both)."""
     from vlr_b200 import vlr as VV
     W = H = 32
     sums = []
-    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING):
+    for renderer in (VV.RENDERER_PATH_TRACING, VV.RENDERER_LIGHT_TRACING, VV.RENDERER_BPT):
         ctx = VV.Context()
         ctx.bindOutputBuffer(W, H)
         scene, cam, keep = _point_lit_box(ctx, W, H, "directional")
         ctx.setScene(scene)
         ctx.setRenderer(renderer)
         ctx.setOptions(max_path_length=6)
-        ctx.render_samples(cam, True, 64)
+        ctx.render_samples(cam, True, 512)
         y = _y_of(ctx.read_film())
         assert np.isfinite(y).all()
         sums.append(y.sum())
         ctx.close()
     assert sums[0] == 0.0
     assert sums[1] > 0.0
+    assert abs(sums[2] / sums[1] - 1) < 0.05, sums
 
 
 def _trace(v, rays, rounds, any_hit):

@@ -87,14 +87,14 @@ __device__ __forceinline__ void storeVertex(const BptArgs &a, const SurfPt &sp, 
                                             const V3 &dirInLocal, float backConv, float probDensity,
                                             float prevProbDensity, float secondPrevPartial, float secondPrevRatio,
                                             bool deltaSampled, bool prevDeltaSampled, bool wlSelected,
-                                            uint32_t pathLength) {
+                                            uint32_t pathLength, bool isPoint = false) {
     uint32_t slot = appendSlot(a.bb.counters, 0u);
     if (slot >= a.bb.capacity) {
         atomicAdd(a.bb.counters + 1, 1u);
         return;
     }
     uint32_t flags = (wlSelected ? 1u : 0u) | (deltaSampled ? 2u : 0u) | (prevDeltaSampled ? 4u : 0u) |
-                     (sp.atInfinity ? 8u : 0u) | (pathLength << 8);
+                     (sp.atInfinity ? 8u : 0u) | (isPoint ? 16u : 0u) | (pathLength << 8);
     LightVertex v;
     v.posMat = make_float4(sp.position.x, sp.position.y, sp.position.z, __uint_as_float(material));
     v.nrmFlags = make_float4(sp.frame.z.x, sp.frame.z.y, sp.frame.z.z, __uint_as_float(flags));
@@ -114,6 +114,7 @@ struct CachedVertex {
     S4 flux;
     V3 dirInLocal;
     float probDensity, prevProbDensity, secondPrevPartial, secondPrevRatio;
+    bool isPoint;      // a point light's position (calcCosTerm 1)
 };
 
 __device__ __forceinline__ void loadVertex(const BptArgs &a, uint32_t i, CachedVertex* c) {
@@ -135,6 +136,7 @@ __device__ __forceinline__ void loadVertex(const BptArgs &a, uint32_t i, CachedV
     c->secondPrevRatio = f6.z;
     c->sp.atInfinity = (c->flags & 8u) != 0;
     c->sp.prim = 0;
+    c->isPoint = (c->flags & 16u) != 0;
 }
 
 // The light vertex's scattering function: its BSDF in importance transport,
@@ -144,10 +146,13 @@ struct VertexBsdf {
     bool fromEdf;
     bool envEdf;
     float envDiscArea;
+    uint32_t emitter;   // fromEdf: the emitter kind (kEmit*)
 };
 
 __device__ __forceinline__ bool vbHasNonDelta(const VertexBsdf &v) {
-    if (v.fromEdf) return true;   // DiffuseEDF / EnvironmentEDF: Emission | LowFreq
+    // Diffuse, environment and point EDFs are Emission | LowFreq; a
+    // directional EDF is a delta direction (materials.cu:2097-2160)
+    if (v.fromEdf) return v.emitter != kEmitDirectional;
     return bsdfHasNonDelta(v.bsdf);
 }
 
@@ -158,11 +163,13 @@ __device__ __forceinline__ S4 vbEval(const VertexBsdf &v, const BsdfQuery &q, co
     float sn = fabsf(q.dirLocal.z / dot(q.dirLocal, ngLocal));
     if (!isfinite(sn)) { *rev = S4::zero(); return S4::zero(); }
     *rev = S4::zero();
-    return S4(d.z > 0.0f ? 1.0f / kPi : 0.0f) * sn;
+    return S4(edfEval(v.emitter, d)) * sn;
 }
 __device__ __forceinline__ float vbPdf(const VertexBsdf &v, const BsdfQuery &q, const V3 &d, float* rev) {
     if (!v.fromEdf) return bsdfPDF(v.bsdf, q, d, rev);
     *rev = 0.0f;
+    if (v.emitter == kEmitPoint) return 1.0f / (4 * kPi);
+    if (v.emitter == kEmitDirectional) return 0.0f;
     if (d.z <= 0.0f) return 0.0f;
     return v.envEdf ? 1.0f / v.envDiscArea : d.z / kPi;
 }
@@ -241,19 +248,34 @@ __global__ void __launch_bounds__(256) lightStartKernel(BptArgs a) {
         float probDensity0 = a.numLightPaths * lightProb * ls.areaPDF;
         S4 alpha = Le0 / probDensity0;
         storeVertex(a, ls.sp, ls.material, alpha, V3(0.0f, 0.0f, 1.0f), 0.0f, probDensity0, 1.0f, 0.0f, 1.0f,
-                    ls.delta, false, false, 0);
-        // EDF direction sample: cosine lobe (DiffuseEDF, materials.cu:2057-2066) or a
-        // point on the disc that covers the scene (EnvironmentEDF, :2844-2857).
+                    ls.delta, false, false, 0, ls.isPoint);
+        // EDF direction sample: cosine lobe (DiffuseEDF, materials.cu:2057-2066), a
+        // point on the disc that covers the scene (EnvironmentEDF, :2844-2857),
+        // the whole sphere (PointEDF, :2190-2196) or the normal (DirectionalEDF,
+        // :2110-2125, a delta direction)
+        const uint32_t emitter = env ? kEmitEnvironment : S.mats[ls.material].emitter;
         float uc = rng.uniform(), ud0 = rng.uniform(), ud1 = rng.uniform();
         (void)uc;
         V3 dirLocal;
         float dirPDF;
         S4 Le1(1.0f / kPi);
+        uint32_t emitType = dir::Emission | dir::LowFreq;
         if (env) {
             float dx, dy;
             concentricDisk(ud0, ud1, &dx, &dy);
             dirLocal = V3(S.bounds.worldRadius * dx, S.bounds.worldRadius * dy, 1.0f);
             dirPDF = 1.0f / envDisc;
+        }
+        else if (emitter == kEmitPoint) {
+            dirLocal = uniformSphere(ud0, ud1);
+            dirPDF = 1.0f / (4 * kPi);
+            Le1 = S4(1.0f / (4 * kPi));
+        }
+        else if (emitter == kEmitDirectional) {
+            dirLocal = V3(0.0f, 0.0f, 1.0f);
+            dirPDF = 1.0f;
+            Le1 = S4(1.0f);
+            emitType = dir::Emission | dir::Delta0D;
         }
         else {
             dirLocal = cosineHemisphere(ud0, ud1);
@@ -267,7 +289,7 @@ __global__ void __launch_bounds__(256) lightStartKernel(BptArgs a) {
             dirLocal.y = 0;
         }
         V3 rayDir = ls.sp.frame.fromLocal(dirLocal);
-        float cosTerm = absDot(rayDir, ls.sp.gn);
+        float cosTerm = ls.isPoint ? 1.0f : absDot(rayDir, ls.sp.gn);
         alpha *= Le1 * (cosTerm / dirPDF);
         a.pb.rng[p] = rng.state;
         a.pb.alpha[p] = toF4(alpha);
@@ -278,8 +300,9 @@ __global__ void __launch_bounds__(256) lightStartKernel(BptArgs a) {
         a.ex.prevProbDensity[p] = 1.0f;
         a.ex.secondPrevPartial[p] = 0.0f;
         a.ex.secondPrevRatio[p] = 1.0f;
-        a.pb.flags[p] = (ls.sp.atInfinity ? kFlagOriginInf : 0u) | (ls.delta ? kFlagPrevDelta : 0u);
-        a.pb.prevType[p] = dir::Emission | dir::LowFreq;
+        a.pb.flags[p] = (ls.sp.atInfinity ? kFlagOriginInf : 0u) | (ls.delta ? kFlagPrevDelta : 0u) |
+                        (ls.isPoint ? kFlagOriginPoint : 0u);
+        a.pb.prevType[p] = emitType;
         a.pb.rayOrg[p] = make_float4(rayOrg.x, rayOrg.y, rayOrg.z, FLT_MAX);
         a.pb.rayDir[p] = make_float4(rayDir.x, rayDir.y, rayDir.z, 0.0f);
         a.pb.active[0][p] = p;
@@ -452,6 +475,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
             vb.fromEdf = vPathLength == 0;
             vb.envEdf = v.sp.atInfinity;
             vb.envDiscArea = S.bounds.worldDiscArea;
+            vb.emitter = S.mats[v.material].emitter;
             if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls);
             V3 conDir, sOrg;
             float dist2, tmax;
@@ -466,7 +490,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
                 qL.importanceMode = 1;
                 V3 conLocalL = v.sp.frame.toLocal(-conDir);
                 V3 conLocalE = L.frame.toLocal(conDir);
-                float cosL = absDot(conDir, v.sp.gn);
+                float cosL = v.isPoint ? 1.0f : absDot(conDir, v.sp.gn);
                 float cosE = lensCos(C, conDir, gn);
                 float G = cosL * cosE * recSq;
                 float scalarConTerm = G / vertexProb;
@@ -482,6 +506,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
                 bool onScreen = idfProject(C, L, conLocalE, &u0, &u1, &fwdDirDensE);
                 if (onScreen) {
                     float fwdAreaDensE = fwdDirDensE * cosL * recSq;
+                    if (v.isPoint) fwdAreaDensE = 0;   // a delta position cannot be hit (lvc_bpt.cu:430-431)
                     bool lastValid = (!(v.flags & 2u) && !(v.flags & 4u)) && vPathLength > 1;
                     float lastToSecondLast = backAreaDensL / v.prevProbDensity;
                     float partialL = sq(lastToSecondLast) * (v.secondPrevPartial + (lastValid ? 1 : 0));
@@ -621,7 +646,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
         // s = 0: implicit light sampling (lvc_bpt.cu:611-670)
         S4 spEm = emittance(S.meng, mat, wls);
         if (spEm.hasNonZero()) {
-            S4 Le = spEm * diffuseEdfEval(dirOutLocal);
+            S4 Le = spEm * edfEval(mat.emitter, dirOutLocal);
             S4 unweighted = alpha * Le;
             if (flags & kFlagSingle) unweighted *= static_cast<float>(kNumLambdas);
             float fwdAreaDensL = a.numLightPaths * __ldg(S.geomLightPdfArea + sp.geomInst) * hypAreaPDF;
@@ -644,6 +669,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
             vb.fromEdf = vPathLength == 0;
             vb.envEdf = v.sp.atInfinity;
             vb.envDiscArea = S.bounds.worldDiscArea;
+            vb.emitter = S.mats[v.material].emitter;
             if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls);
             V3 conDir, sOrg;
             float dist2, tmax;
@@ -658,7 +684,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
                 qL.importanceMode = 1;
                 V3 conLocalL = v.sp.frame.toLocal(-conDir);
                 V3 conLocalE = sp.frame.toLocal(conDir);
-                float cosL = absDot(conDir, v.sp.gn);
+                float cosL = v.isPoint ? 1.0f : absDot(conDir, v.sp.gn);
                 float cosE = absDot(conDir, sp.gn);
                 float G = cosL * cosE * recSq;
                 float scalarConTerm = G / vertexProb;
@@ -679,6 +705,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
                 fwdDirDensE *= rrProb(fwdFsE, conLocalE, fwdDirDensE, gnLocal, wls.selected);
                 backDirDensE *= rrProb(backFsE, qE.dirLocal, backDirDensE, gnLocal, wls.selected);
                 float fwdAreaDensE = fwdDirDensE * cosL * recSq;
+                if (v.isPoint) fwdAreaDensE = 0;       // a delta position cannot be hit (lvc_bpt.cu:738-739)
                 float backAreaDensE = backDirDensE * cosTermIn / lastDist2;
                 float partialL;
                 {
@@ -1079,9 +1106,7 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
         throw std::runtime_error("maxPathLength out of range");
     if (scene.lightInsts.n == 0)
         throw std::runtime_error("LVC-BPT needs at least one light");
-    if (scene.hasDeltaEmitters)
-        throw std::runtime_error("LVC-BPT here does not render point or directional emitters "
-                                 "(path tracing and light tracing do)");
+
     StageTimer dummy;
     StageTimer &T = timer ? *timer : dummy;
     const int grid = numSMs * static_cast<int>(fp.blocksPerSM ? fp.blocksPerSM : 8);
