@@ -1187,7 +1187,7 @@ void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const P
 size_t ltConnectionBytes(uint32_t numPaths) { return a256(size_t(numPaths) * sizeof(LtConnection)); }
 
 void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* connections, const Film &film,
-                    const FrameParams &fp, uint32_t numLightPaths, int numSMs, cudaStream_t stream,
+                    const FrameParams &fp, uint32_t numLightPaths, uint32_t frames, int numSMs, cudaStream_t stream,
                     StageTimer* timer) {
     if (fp.maxPathLength == 0 || fp.maxPathLength >= kMaxBounces)
         throw std::runtime_error("maxPathLength out of range");
@@ -1201,8 +1201,8 @@ void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* 
     a.S = scene;
     a.pb = lightPaths;
     a.film = film;
-    a.numLightPaths = numLightPaths;
-    a.numPaths = numLightPaths;
+    a.numLightPaths = numLightPaths;            // per frame: the alpha normalisation
+    a.numPaths = numLightPaths * frames;        // slots: `frames` frames in one launch
     a.width = fp.width;
     a.height = fp.height;
     a.stride = fp.stride;
@@ -1216,7 +1216,7 @@ void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* 
     ltSplatKernel<<<grid, 256, 0, stream>>>(a, 0u);
     T.end(stream);
     FrameParams lf = fp;
-    lf.numPaths = numLightPaths;
+    lf.numPaths = a.numPaths;
     // at most maxPathLength - 1 traced segments before the lens connection
     // (the loop of light_tracing.cu:145-171 with MaxPathLength)
     for (uint32_t b = 0; b + 1 < fp.maxPathLength; ++b) {

@@ -44,12 +44,13 @@ void carveBptBuffers(void* base, uint32_t numLightPaths, uint32_t numEyePaths, u
 
 // One LVC-BPT frame: light subpaths fill the cache, then one eye subpath per
 // pixel connects to it.  All paths share the frame's wavelength samples.
-// Light tracing (light_tracing.cu:49-263): numLightPaths light subpaths with
-// wavelength samples of their own, each vertex connected to a lens sample and
-// splatted to the film.  `connections` holds ltConnectionBytes(numLightPaths).
+// Light tracing (light_tracing.cu:49-263): `frames` frames of numLightPaths
+// light subpaths each, in one launch, with wavelength samples of their own;
+// each vertex connects to a lens sample and splats to the film.  The path
+// buffers and `connections` (ltConnectionBytes) hold numLightPaths x frames.
 size_t ltConnectionBytes(uint32_t numPaths);
 void ltRenderLaunch(const SceneGPU &scene, const PathBuffers &lightPaths, void* connections, const Film &film,
-                    const FrameParams &fp, uint32_t numLightPaths, int numSMs, cudaStream_t stream,
+                    const FrameParams &fp, uint32_t numLightPaths, uint32_t frames, int numSMs, cudaStream_t stream,
                     StageTimer* timer);
 
 void bptRenderLaunch(const SceneGPU &scene, const PathBuffers &eyePaths, const PathBuffers &lightPaths,

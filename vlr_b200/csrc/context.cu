@@ -775,23 +775,27 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 // One frame per launch: light subpaths per frame default to
                 // the pixel count (the reference launches a fixed 500,000,
                 // context.h:303); each carries its own wavelength samples.
+                // As many frames per launch as the path budget holds.
                 const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame : pixels;
-                if (ltCapacity < lightPaths) {
-                    ltCapacity = lightPaths;
-                    const size_t pathBytes = pathBufferBytes(lightPaths);
-                    ltMem.resize(pathBytes + ltConnectionBytes(lightPaths));
-                    carvePathBuffers(ltMem.ptr, lightPaths, &ltPb);
+                const uint32_t frames = std::max<uint32_t>(
+                    1u, std::min<uint32_t>(samples - done, options.maxPathsInFlight / lightPaths));
+                const uint32_t slots = lightPaths * frames;
+                if (ltCapacity < slots) {
+                    ltCapacity = slots;
+                    const size_t pathBytes = pathBufferBytes(slots);
+                    ltMem.resize(pathBytes + ltConnectionBytes(slots));
+                    carvePathBuffers(ltMem.ptr, slots, &ltPb);
                     ltConn = ltMem.as<char>() + pathBytes;
-                    std::vector<uint64_t> seeds(lightPaths);
-                    seedPathRngs(seeds.data(), lightPaths, 459182033132123413ull);
+                    std::vector<uint64_t> seeds(slots);
+                    seedPathRngs(seeds.data(), slots, 459182033132123413ull);
                     ck(cudaMemcpy(ltPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
                     ck(cudaMemset(ltPb.totals, 0, 16), "totals");
                 }
                 FrameParams lf = fp;
-                lf.sppPerLaunch = 1;
-                lf.numPaths = lightPaths;
-                ltRenderLaunch(sg, ltPb, ltConn, fl, lf, lightPaths, numSMs, stream, &timer);
-                k = 1;
+                lf.sppPerLaunch = frames;
+                lf.numPaths = slots;
+                ltRenderLaunch(sg, ltPb, ltConn, fl, lf, lightPaths, frames, numSMs, stream, &timer);
+                k = frames;
             }
             else if (guiding.enabled || guiding.train) {
                 ensureGuiding(pathCapacity);
