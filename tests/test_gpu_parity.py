@@ -515,6 +515,89 @@ def test_directional_emitter_is_seen_by_light_subpaths_only():
     assert abs(sums[2] / sums[1] - 1) < 0.05, sums
 
 
+def _poster_box(ctx, W, H, texels, nearest):
+    """The diffuse Cornell box with its back wall split off as a "poster"
+    whose albedo is an Image2DTexture of `texels` (an h x w x 3 linear-RGB
+    array; None: the immediate white of the other walls), u running left to
+    right and v bottom to top across the wall."""
+    from vlr_b200 import vlr as VV, scenes
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    desc["materials"]["poster"] = ("Matte", {"albedo": ("Rec709(D65) sRGB Gamma", 0.75, 0.75, 0.75)})
+    mesh = desc["meshes"][0]
+    verts = mesh["verts"].copy()
+    verts[4:8, 9:11] = [[0, 0], [1, 0], [1, 1], [0, 1]]
+    mesh["verts"] = verts
+    groups = [(np.array([0, 1, 2, 0, 2, 3, 8, 9, 10, 8, 10, 11], np.uint32), "white"),
+              (np.array([4, 5, 6, 4, 6, 7], np.uint32), "poster")]
+    mesh["groups"] = groups + mesh["groups"][1:]
+    scene, cam, keep = scenes.build(ctx, desc)
+    if texels is not None:
+        poster = keep[list(desc["materials"]).index("poster")]
+        rgba = np.concatenate([texels, np.ones(texels.shape[:2] + (1,))], axis=2).astype(np.float32)
+        img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
+        tex = ctx.createShaderNode("Image2DTexture")
+        tex.set("image", img)
+        if nearest:
+            tex.set_enum("mag filter", "Nearest")
+            tex.set_enum("min filter", "Nearest")
+        poster.set("albedo", tex.plug())
+        keep += [img, tex]
+    return scene, cam, keep
+
+
+def _srgb_degamma(v):
+    return v / 12.92 if v <= 0.04045 else ((v + 0.055) / 1.055) ** 2.4
+
+
+def test_constant_texture_renders_like_the_immediate_colour():
+    """An Image2DTexture (shader_nodes.cu:410-445: filtered RGB, upsampled at
+    the hit) holding the immediate colour's linear value everywhere renders
+    the image of the immediate colour: same seeds, so all but a few pixels
+    agree to float round-off and the totals within 0.1%."""
+    from vlr_b200 import vlr as VV
+    W = H = 64
+    lin = _srgb_degamma(0.75)
+    films = []
+    for texels in (None, np.full((4, 4, 3), lin)):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = _poster_box(ctx, W, H, texels, False)
+        ctx.setScene(scene)
+        ctx.setOptions(max_path_length=6)
+        ctx.render_samples(cam, True, 64)
+        films.append(_y_of(ctx.read_film()))
+        ctx.close()
+    a, b = films
+    assert abs(b.sum() / a.sum() - 1) < 1e-3, b.sum() / a.sum()
+    differ = np.abs(a - b) > 1e-4 * np.maximum(np.abs(a), 1e-30)
+    assert differ.mean() < 0.05, differ.mean()
+
+
+def test_texture_pattern_lands_on_the_surface():
+    """A 2 x 1 texture, black then white, on the back wall with nearest
+    filtering: the wall's left half (u < 0.5) reflects nothing and its right
+    half reflects light, so the pixels that see the wall left of centre stay
+    black while those right of centre do not."""
+    from vlr_b200 import vlr as VV
+    W = H = 64
+    texels = np.array([[[0.0, 0.0, 0.0], [0.9, 0.9, 0.9]]])
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = _poster_box(ctx, W, H, texels, True)
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=6)
+    ctx.render_samples(cam, True, 64)
+    y = _y_of(ctx.read_film())
+    ctx.close()
+    # the wall at y = 2.0, x = -/+0.75 projects to row 0.41 H, columns 0.36 W / 0.64 W
+    left = y[24:28, 20:25]
+    right = y[24:28, 39:44]
+    assert np.all(left == 0.0), left.max()
+    assert np.all(right > 0.0)
+
+
 def _trace(v, rays, rounds, any_hit):
     L = V.lib()
     L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

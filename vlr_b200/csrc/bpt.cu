@@ -103,6 +103,7 @@ __device__ __forceinline__ void storeVertex(const BptArgs &a, const SurfPt &sp, 
     v.flux = toF4(flux);
     v.dirInPdf = make_float4(dirInLocal.x, dirInLocal.y, dirInLocal.z, probDensity);
     v.misPdfs = make_float4(prevProbDensity, secondPrevPartial, secondPrevRatio, 0.0f);
+    v.texCoord = make_float4(sp.tu, sp.tv, 0.0f, 0.0f);
     a.bb.cache[slot] = v;
 }
 
@@ -119,7 +120,7 @@ struct CachedVertex {
 
 __device__ __forceinline__ void loadVertex(const BptArgs &a, uint32_t i, CachedVertex* c) {
     const float4* p = reinterpret_cast<const float4*>(a.bb.cache + i);
-    float4 f0 = p[0], f1 = p[1], f2 = p[2], f3 = p[3], f4 = p[4], f5 = p[5], f6 = p[6];
+    float4 f0 = p[0], f1 = p[1], f2 = p[2], f3 = p[3], f4 = p[4], f5 = p[5], f6 = p[6], f7 = p[7];
     c->sp.position = V3(f0.x, f0.y, f0.z);
     c->material = __float_as_uint(f0.w);
     V3 n(f1.x, f1.y, f1.z), t(f2.x, f2.y, f2.z);
@@ -136,6 +137,8 @@ __device__ __forceinline__ void loadVertex(const BptArgs &a, uint32_t i, CachedV
     c->secondPrevRatio = f6.z;
     c->sp.atInfinity = (c->flags & 8u) != 0;
     c->sp.prim = 0;
+    c->sp.tu = f7.x;
+    c->sp.tv = f7.y;
     c->isPoint = (c->flags & 16u) != 0;
 }
 
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(256) lightShadeKernel(BptArgs a) {
         SurfPt sp;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, nullptr);
         const uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
-        Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls);
+        Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls, sp.tu, sp.tv);
         float4 o4 = a.pb.rayOrg[p], d4 = a.pb.rayDir[p];
         V3 dirInLocal = sp.frame.toLocal(-V3(d4.x, d4.y, d4.z));
         V3 gnLocal = sp.frame.toLocal(sp.gn);
@@ -476,7 +479,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
             vb.envEdf = v.sp.atInfinity;
             vb.envDiscArea = S.bounds.worldDiscArea;
             vb.emitter = S.mats[v.material].emitter;
-            if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls);
+            if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls, v.sp.tu, v.sp.tv);
             V3 conDir, sOrg;
             float dist2, tmax;
             visibilityRay(spE, v.sp, &conDir, &dist2, &sOrg, &tmax);
@@ -633,7 +636,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
         float hypAreaPDF;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, &hypAreaPDF);
         const MatDesc &mat = S.mats[__ldg(S.triMaterial + __float_as_uint(h.w))];
-        Bsdf bsdfE = buildBsdf(S.meng, mat, wls);
+        Bsdf bsdfE = buildBsdf(S.meng, mat, wls, sp.tu, sp.tv);
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);
         V3 gnLocal = sp.frame.toLocal(sp.gn);
         BsdfQuery qE;
@@ -670,7 +673,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
             vb.envEdf = v.sp.atInfinity;
             vb.envDiscArea = S.bounds.worldDiscArea;
             vb.emitter = S.mats[v.material].emitter;
-            if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls);
+            if (!vb.fromEdf) vb.bsdf = buildBsdf(S.meng, S.mats[v.material], wls, v.sp.tu, v.sp.tv);
             V3 conDir, sOrg;
             float dist2, tmax;
             visibilityRay(sp, v.sp, &conDir, &dist2, &sOrg, &tmax);
@@ -987,7 +990,7 @@ __global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
         SurfPt sp;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, nullptr);
         const uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
-        const Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls);
+        const Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls, sp.tu, sp.tv);
         const float4 d4 = a.pb.rayDir[p];
         BsdfQuery q;
         q.dirLocal = sp.frame.toLocal(-V3(d4.x, d4.y, d4.z));

@@ -18,6 +18,7 @@ struct LightVertex {
     float4 flux;          // light-subpath throughput, 4 wavelengths
     float4 dirInPdf;      // incoming direction in the shading frame, probDensity
     float4 misPdfs;       // prevProbDensity, secondPrevPartialDenomMisWeight, secondPrevProbRatioToFirst, -
+    float4 texCoord;      // texture coordinates (u, v), -, -
 };
 
 // Per-path bidirectional MIS bookkeeping (the light and eye path payloads of

@@ -194,6 +194,8 @@ namespace {
 MatDesc describeMaterial(const SurfaceMaterial* m) {
     MatDesc d{};
     std::memset(&d, 0, sizeof(d));
+    for (int32_t &k : d.table) k = -1;
+    for (int32_t &k : d.tex) k = -1;
     d.bsdfKind = kNullBSDF;
     d.emitScale = 1.0f;
     const std::string t = lower(m->typeName);
@@ -271,6 +273,7 @@ MatDesc describeMaterial(const SurfaceMaterial* m) {
 
 struct FlatScene {
     std::vector<float4> pos, nrm, tan;
+    std::vector<float2> uv;
     std::vector<uint4> tri;
     std::vector<uint32_t> triMaterial;
     std::vector<float> triVerts;                 // 9 floats per triangle for the BVH build
@@ -307,6 +310,7 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
             f.pos.push_back(make_float4(p.x, p.y, p.z, 0.0f));
             f.nrm.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
             f.tan.push_back(make_float4(tt.x, tt.y, tt.z, 0.0f));
+            f.uv.push_back(make_float2(v.texCoord.u, v.texCoord.v));
             f.lo = vmin3(f.lo, p);
             f.hi = vmax3(f.hi, p);
         }
@@ -388,7 +392,51 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
 
 } // namespace
 
+Context::SceneTexture::~SceneTexture() {
+    if (tex) cudaDestroyTextureObject(tex);
+    if (array) cudaFreeArray(array);
+}
+
+namespace {
+
+// Material parameters whose Spectrum plug may be an Image2DTexture, with the
+// MatDesc spectrum slot each drives (the slots describeMaterial fills).
+const std::map<std::string, std::vector<std::pair<std::string, int>>> &textureSlots() {
+    static const std::map<std::string, std::vector<std::pair<std::string, int>>> m = {
+        { "matte", { { "albedo", 0 } } },
+        { "specularreflection", { { "coeff", 0 }, { "eta", 1 }, { "k", 2 } } },
+        { "specularscattering", { { "coeff", 0 }, { "eta ext", 1 }, { "eta int", 2 } } },
+        { "microfacetreflection", { { "eta", 1 }, { "k", 2 } } },
+        { "microfacetscattering", { { "coeff", 0 }, { "eta ext", 1 }, { "eta int", 2 } } },
+        { "lambertianscattering", { { "coeff", 0 } } },
+        { "ue4", { { "base color", 0 } } },
+    };
+    return m;
+}
+
+SpType parseSpectrumType(const std::string &s) {
+    const std::string l = lower(s);
+    if (l.find("light") != std::string::npos) return SpType::LightSource;
+    if (l.find("ior") != std::string::npos || l.find("refraction") != std::string::npos) return SpType::IOR;
+    return SpType::Reflectance;
+}
+
+cudaTextureAddressMode parseWrap(const std::string &s) {
+    const std::string l = lower(s);
+    if (l == "clamp to edge") return cudaAddressModeClamp;
+    if (l == "mirror") return cudaAddressModeMirror;
+    if (l == "clamp to border") return cudaAddressModeBorder;
+    return cudaAddressModeWrap;
+}
+
+} // namespace
+
 void Context::buildScene(cudaStream_t stream) {
+    if (!sceneTextures.empty()) {
+        // kernels of earlier frames may still read the textures
+        ck(cudaDeviceSynchronize(), "texture release");
+        sceneTextures.clear();
+    }
     sceneBufs.clear();
     std::memset(&sg, 0, sizeof(sg));
     sg.meng = deviceMengTables();
@@ -492,6 +540,68 @@ void Context::buildScene(cudaStream_t stream) {
     sg.tri = upload(f.tri, stream);
     sg.triMaterial = upload(f.triMaterial, stream);
     for (MatDesc &md : f.mats) md.bsdfFlags = options.consistentDielectricPdf ? kBsdfConsistentPdf : 0u;
+    // Image2DTexture plugs on material spectra
+    {
+        std::map<const Object*, int32_t> texIndex;
+        std::vector<unsigned long long> texObjs;
+        std::vector<uint32_t> texTypes;
+        for (size_t i = 0; i < f.matObjs.size() && i < f.mats.size(); ++i) {
+            const SurfaceMaterial* m = f.matObjs[i];
+            auto slots = textureSlots().find(lower(m->typeName));
+            if (slots == textureSlots().end()) continue;
+            for (const auto &ps : slots->second) {
+                auto pl = m->plugs.find(ps.first);
+                if (pl == m->plugs.end() || !pl->second.nodeRef) continue;
+                const auto* node = reinterpret_cast<const ShaderNode*>(pl->second.nodeRef);
+                if (lower(node->typeName) != "image2dtexture") continue;
+                auto it = texIndex.find(node);
+                if (it == texIndex.end()) {
+                    auto io = node->objects.find("image");
+                    const auto* img = io != node->objects.end() ? static_cast<const Image2D*>(io->second) : nullptr;
+                    if (!img || img->width == 0 || img->height == 0 ||
+                        img->rgba.size() < size_t(img->width) * img->height * 4)
+                        continue;
+                    auto st = std::make_unique<SceneTexture>();
+                    const cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+                    ck(cudaMallocArray(&st->array, &ch, img->width, img->height), "texture array");
+                    ck(cudaMemcpy2DToArray(st->array, 0, 0, img->rgba.data(), size_t(img->width) * 16,
+                                           size_t(img->width) * 16, img->height, cudaMemcpyHostToDevice),
+                       "texture upload");
+                    cudaResourceDesc rd{};
+                    rd.resType = cudaResourceTypeArray;
+                    rd.res.array.array = st->array;
+                    cudaTextureDesc td{};
+                    auto en = [&](const char* k, const char* d) {
+                        auto e = node->enums.find(k);
+                        return e != node->enums.end() ? e->second : std::string(d);
+                    };
+                    td.addressMode[0] = parseWrap(en("wrap u", "Repeat"));
+                    td.addressMode[1] = parseWrap(en("wrap v", "Repeat"));
+                    td.filterMode = lower(en("mag filter", "Linear")) == "nearest" ? cudaFilterModePoint
+                                                                                   : cudaFilterModeLinear;
+                    td.readMode = cudaReadModeElementType;
+                    td.normalizedCoords = 1;
+                    ck(cudaCreateTextureObject(&st->tex, &rd, &td, nullptr), "texture object");
+                    it = texIndex.emplace(node, static_cast<int32_t>(texObjs.size())).first;
+                    texObjs.push_back(static_cast<unsigned long long>(st->tex));
+                    // 8-bit sRGB images are linearised when created (vlrLinearImage2DCreate)
+                    const bool eightBit = img->format != "RGBA32Fx4" && img->format != "Gray32F";
+                    const ColorSp cs = eightBit && parseColorSpace(img->colorSpace) == ColorSp::sRGB
+                                           ? ColorSp::Rec709 : parseColorSpace(img->colorSpace);
+                    texTypes.push_back(static_cast<uint32_t>(parseSpectrumType(img->spectrumType)) |
+                                       (static_cast<uint32_t>(cs) << 8));
+                    sceneTextures.push_back(std::move(st));
+                }
+                f.mats[i].tex[ps.second] = it->second;
+            }
+        }
+        if (!texObjs.empty()) {
+            sg.meng.textures = upload(texObjs, stream);
+            sg.meng.texSpType = upload(texTypes, stream);
+            sg.meng.colorMats = deviceColorMatrices();
+            sg.uv = upload(f.uv, stream);
+        }
+    }
     // Material spectra are immediate colours: each is tabulated once here on
     // the 95-sample grid, so a hit interpolates one table per spectrum.
     {

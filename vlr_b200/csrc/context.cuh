@@ -137,6 +137,17 @@ private:
 
     SceneGPU sg{};
     std::vector<std::unique_ptr<DeviceBuffer>> sceneBufs;
+    // Image2DTexture nodes of the bound scene: each image in a CUDA array
+    // read through a texture object with the node's filter and wrap modes
+    struct SceneTexture {
+        cudaArray_t array = nullptr;
+        cudaTextureObject_t tex = 0;
+        SceneTexture() = default;
+        SceneTexture(const SceneTexture &) = delete;
+        SceneTexture &operator=(const SceneTexture &) = delete;
+        ~SceneTexture();
+    };
+    std::vector<std::unique_ptr<SceneTexture>> sceneTextures;
     DeviceBuffer film, output, pathMem, lbvhScratch, bptMem;
     PathBuffers pb{};
     PathBuffers lightPb{};

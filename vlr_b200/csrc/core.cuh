@@ -261,10 +261,15 @@ VLRB_HD bool isDispersive(uint32_t t) { return (t & Dispersive) != 0; }
 // ---------------------------------------------------------------- Meng-Simon upsampling
 // Tables: 12x14 grid cells of 8 bytes {inside, numPoints, idx[6]} and 186 data
 // points of 99 floats {xystar[2], uv[2], spectrum[95]}.
+struct ColorMatrices;
 struct MengTables {
     const uint8_t* grid;
     const float* points;
     const float* blended;   // optional: per-material spectra on the 95-sample grid (mengBlend)
+    // optional: Image2DTexture textures of material spectra (device only)
+    const unsigned long long* textures;   // cudaTextureObject_t per texture
+    const uint32_t* texSpType;            // per texture: SpType | ColorSp << 8 of its image
+    const ColorMatrices* colorMats;
 };
 constexpr uint32_t kMengGridW = 12, kMengGridH = 14, kMengSamples = 95, kMengPointStride = 99;
 constexpr uint32_t kMengNumPoints = 186;

@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         float hypAreaPDF;
         decodeHit(S, prim, h.y, h.z, &sp, &hypAreaPDF);
         const MatDesc &mat = S.mats[__ldg(S.triMaterial + prim)];
-        Bsdf bsdf = buildBsdf(S.meng, mat, wls);
+        Bsdf bsdf = buildBsdf(S.meng, mat, wls, sp.tu, sp.tv);
         float4 o4 = pb.rayOrg[p], d4 = pb.rayDir[p];
         V3 rayOrg(o4.x, o4.y, o4.z), rayDir(d4.x, d4.y, d4.z);
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);

@@ -26,11 +26,26 @@ struct MatDesc {
     uint32_t bsdfFlags;     // Bsdf::flags bits chosen at scene build (kBsdfConsistentPdf)
     int32_t table[4] = { -1, -1, -1, -1 };   // sp[0..2], emit: index of the blended spectrum
                                              // in MengTables::blended (-1: evaluate the UpSpec)
+    int32_t tex[3] = { -1, -1, -1 };         // sp[0..2]: Image2DTexture index (-1: none)
 };
 
-// Spectrum slot 0-2 (sp) or 3 (emit) of material m at the path's wavelengths:
-// the scene's blended table when it has one, else the UpSpec.
-VLRB_HD S4 matSpectrum(const MengTables &T, const MatDesc &m, int slot, const WLS &wls) {
+// Spectrum slot 0-2 (sp) or 3 (emit) of material m at the path's wavelengths
+// and texture coordinates (tu, tv): a texture's filtered RGB upsampled at the
+// hit (Image2DTextureShaderNode_Spectrum, shader_nodes.cu:410-445), else the
+// scene's blended table, else the UpSpec.
+VLRB_HD S4 matSpectrum(const MengTables &T, const MatDesc &m, int slot, const WLS &wls, float tu = 0.0f,
+                       float tv = 0.0f) {
+#if defined(__CUDA_ARCH__)
+    if (slot < 3 && m.tex[slot] >= 0 && T.textures) {
+        const float4 c = tex2DLod<float4>(T.textures[m.tex[slot]], tu, tv, 0.0f);
+        const uint32_t info = T.texSpType[m.tex[slot]];
+        const UpSpec up = mengUpsample(T, *T.colorMats, static_cast<SpType>(info & 0xFFu),
+                                       static_cast<ColorSp>(info >> 8), c.x, c.y, c.z);
+        return mengEvaluate(T, up, wls);
+    }
+#else
+    (void)tu; (void)tv;
+#endif
     if (T.blended && m.table[slot] >= 0) return blendedEvaluate(T.blended + m.table[slot] * kMengSamples, wls);
     return mengEvaluate(T, slot < 3 ? m.sp[slot] : m.emit, wls);
 }
@@ -154,6 +169,7 @@ struct SceneGPU {
     const float4* pos;        // [numVerts] world position
     const float4* nrm;        // [numVerts] world shading normal
     const float4* tan;        // [numVerts] world tc0Direction
+    const float2* uv;         // [numVerts] texture coordinates (null when no material is textured)
     const uint4* tri;         // [numTris] i0, i1, i2, geomInst
     const uint32_t* triMaterial;
     const MatDesc* mats;
@@ -188,6 +204,7 @@ struct SurfPt {
     uint32_t geomInst;
     float u, v;
     bool atInfinity;
+    float tu = 0.0f, tv = 0.0f;   // texture coordinates (scenes with textures)
 };
 
 // Instantiate the BSDF of material m at the given wavelengths (the setupBSDF
@@ -195,7 +212,7 @@ struct SurfPt {
 // K >= 0: the material is known to be of that kind (the shade kernels
 // specialised per material queue), which lets every BSDF dispatch fold.
 template <int K = -1>
-VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
+VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls, float tu = 0.0f, float tv = 0.0f) {
     Bsdf B;
     const uint32_t kind = K >= 0 ? static_cast<uint32_t>(K) : m.bsdfKind;
     B.kind = kind;
@@ -204,24 +221,24 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls) {
     switch (kind) {
     case kMatte:
     case kLambertianBSDF:
-        B.a = matSpectrum(T, m, 0, wls);
+        B.a = matSpectrum(T, m, 0, wls, tu, tv);
         break;
     case kSpecularBRDF:
     case kSpecularBSDF:
     case kMicrofacetBSDF:
-        B.a = matSpectrum(T, m, 0, wls);
-        B.b = matSpectrum(T, m, 1, wls);
-        B.c = matSpectrum(T, m, 2, wls);
+        B.a = matSpectrum(T, m, 0, wls, tu, tv);
+        B.b = matSpectrum(T, m, 1, wls, tu, tv);
+        B.c = matSpectrum(T, m, 2, wls, tu, tv);
         if (kind == kSpecularBSDF) B.flags = wls.single ? 0u : 1u;
         if (kind == kMicrofacetBSDF) B.flags = m.bsdfFlags & kBsdfConsistentPdf;
         break;
     case kMicrofacetBRDF:
-        B.b = matSpectrum(T, m, 1, wls);
-        B.c = matSpectrum(T, m, 2, wls);
+        B.b = matSpectrum(T, m, 1, wls, tu, tv);
+        B.c = matSpectrum(T, m, 2, wls, tu, tv);
         break;
     case kUE4: {
         // UE4SurfaceMaterial_setupBSDF (materials.cu:1959-1978); f[1] = metallic.
-        S4 base = matSpectrum(T, m, 0, wls);
+        S4 base = matSpectrum(T, m, 0, wls, tu, tv);
         const float metallic = m.f[1];
         const float specular = 0.5f;
         B.a = base * (1 - metallic);
@@ -282,6 +299,16 @@ __device__ __forceinline__ void decodeHit(const SceneGPU &S, uint32_t prim, floa
     sp->frame = Frame(normalize(tc0), normalize(sn));
     sp->gn = normalize(gn);
     sp->prim = prim;
+    if (S.uv) {
+        // texCoord = b0 t0 + b1 t1 + b2 t2 (triangle.cu:35)
+        const float2 a = __ldg(S.uv + t.x), b = __ldg(S.uv + t.y), c = __ldg(S.uv + t.z);
+        sp->tu = b0 * a.x + b1 * b.x + b2 * c.x;
+        sp->tv = b0 * a.y + b1 * b.y + b2 * c.y;
+    }
+    else {
+        sp->tu = 0.0f;
+        sp->tv = 0.0f;
+    }
     sp->u = b0;
     sp->v = b1;
     sp->atInfinity = false;

@@ -205,6 +205,25 @@ bool initShaderNode(ShaderNode* n, const std::string &type) {
         n->enums["mag filter"] = "Linear";
         return true;
     }
+    if (t == "image2dtexture") {
+        // Image2DTextureShaderNode parameters and defaults (shader_nodes.cpp:1593-1647);
+        // its Spectrum plug drives a material's colour parameters
+        n->addParam("image", kNode, "Image");
+        n->addParam("bump type", kImm, "BumpType");
+        n->addParam("bump coeff", kImm, "Float");
+        n->addParam("min filter", kImm, "TextureFilter");
+        n->addParam("mag filter", kImm, "TextureFilter");
+        n->addParam("wrap u", kImm, "TextureWrapMode");
+        n->addParam("wrap v", kImm, "TextureWrapMode");
+        n->addParam("texcoord", kNode, "TextureCoordinates");
+        n->enums["bump type"] = "Normal Map (DirectX)";
+        n->floats["bump coeff"] = { 1.0f };
+        n->enums["min filter"] = "Linear";
+        n->enums["mag filter"] = "Linear";
+        n->enums["wrap u"] = "Repeat";
+        n->enums["wrap v"] = "Repeat";
+        return true;
+    }
     if (t == "tripletspectrum") {
         n->addParam("spectrum type", kImm, "SpectrumType");
         n->addParam("color space", kImm, "ColorSpace");

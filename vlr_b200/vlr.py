@@ -90,6 +90,7 @@ def _api():
         "vlrShaderNodeGetPlug": [v, ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(VLRShaderNodePlug)],
         "vlrQueryableSetImmediateSpectrum": [v, ctypes.c_char_p, ctypes.POINTER(VLRImmediateSpectrum)],
         "vlrQueryableSetFloat": [v, ctypes.c_char_p, ctypes.c_float],
+        "vlrQueryableSetEnumValue": [v, ctypes.c_char_p, ctypes.c_char_p],
         "vlrQueryableSetFloatTuple": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float), ctypes.c_uint32],
         "vlrQueryableSetPoint3D": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 3)],
         "vlrQueryableSetQuaternion": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 4)],
@@ -172,6 +173,9 @@ class Queryable:
 
     def set_quaternion(self, name, q):
         check(_api().vlrQueryableSetQuaternion(self.h, name.encode(), ctypes.byref((ctypes.c_float * 4)(*q))), name)
+
+    def set_enum(self, name, value):
+        check(_api().vlrQueryableSetEnumValue(self.h, name.encode(), value.encode()), name)
 
     def get_float(self, name):
         v = ctypes.c_float()
