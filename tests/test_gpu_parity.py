@@ -598,6 +598,196 @@ def test_texture_pattern_lands_on_the_surface():
     assert np.all(right > 0.0)
 
 
+_LOOK_DOWN = (np.sqrt(0.5), 0.0, 0.0, np.sqrt(0.5))   # forward (0, -1, 0)
+
+
+def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=None, blocker_alpha=None):
+    """A 4 x 4 white floor at y = 0 (u along +x, v along +z; tangent +x) lit
+    by a 1 x 1 downward-facing light at height 2 centred over `light_at`
+    (x, z), seen by a camera at height 0.9 looking straight down.
+    floor_normal: the floor's vertex normal; normal_plug: the floor group's
+    nodeNormal.  blocker_alpha: a black 6 x 6 sheet at height 1, between
+    the floor and the light and above the camera, with a constant alpha map
+    of this value (None: no sheet)."""
+    from vlr_b200 import vlr as VV
+    lin = "Rec709(D65)"
+    keep = []
+
+    def mat(typ, **params):
+        m = ctx.createSurfaceMaterial(typ)
+        for k, v in params.items():
+            m.set(k, VV.Spectrum(lin, *v))
+        keep.append(m)
+        return m
+
+    def quad(name, corners, n, t, uvs, material, **plugs):
+        verts = np.array([list(p) + list(n) + list(t) + list(uv) for p, uv in zip(corners, uvs)], np.float32)
+        node = ctx.createTriangleMeshSurfaceNode(name)
+        node.set_vertices(verts)
+        node.add_material_group(np.array([0, 1, 2, 0, 2, 3], np.uint32), material, **plugs)
+        keep.append(node)
+        return node
+
+    scene = ctx.createScene()
+    uvs = [(0, 0), (0, 1), (1, 1), (1, 0)]
+    fn = np.asarray(floor_normal, np.float64)
+    fn = tuple(fn / np.linalg.norm(fn))
+    scene.add_child(quad("floor", [(-2, 0, -2), (-2, 0, 2), (2, 0, 2), (2, 0, -2)], fn, (1, 0, 0), uvs,
+                         mat("Matte", albedo=(0.8, 0.8, 0.8)), normal=normal_plug))
+    lx, lz = light_at
+    scene.add_child(quad("light", [(lx - .5, 2, lz - .5), (lx + .5, 2, lz - .5), (lx + .5, 2, lz + .5),
+                                   (lx - .5, 2, lz + .5)], (0, -1, 0), (1, 0, 0), uvs,
+                         mat("DiffuseEmitter", emittance=(10.0, 10.0, 10.0))))
+    if blocker_alpha is not None:
+        rgba = np.zeros((2, 2, 4), np.float32)
+        rgba[..., 3] = blocker_alpha
+        img = ctx.createLinearImage2D(rgba, "Reflectance", lin)
+        tex = ctx.createShaderNode("Image2DTexture")
+        tex.set("image", img)
+        keep += [img, tex]
+        scene.add_child(quad("sheet", [(-3, 1, -3), (3, 1, -3), (3, 1, 3), (-3, 1, 3)], (0, -1, 0), (1, 0, 0), uvs,
+                             mat("Matte", albedo=(0.0, 0.0, 0.0)), alpha=tex.plug(VV.PLUG_ALPHA, 3)))
+    cam = ctx.createCamera("Perspective")
+    cam.set_point("position", (0.0, 0.9, 0.0))
+    cam.set_quaternion("orientation", _LOOK_DOWN)
+    for k, v in (("aspect", W / H), ("sensitivity", 1.0), ("fovy", 40 * np.pi / 180), ("lens radius", 0.0),
+                 ("op distance", 1.0)):
+        cam.set(k, v)
+    return scene, cam, keep
+
+
+def _floor_sum(renderer, spp, **kw):
+    from vlr_b200 import vlr as VV
+    W = H = 48
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = _floor_scene(ctx, W, H, **kw)
+    ctx.setScene(scene)
+    ctx.setRenderer(renderer)
+    ctx.setOptions(max_path_length=4)
+    ctx.render_samples(cam, True, spp)
+    y = _y_of(ctx.read_film())
+    ctx.close()
+    assert np.isfinite(y).all()
+    return y.sum()
+
+
+@pytest.mark.parametrize("renderer", ["path_tracing", "light_tracing", "bpt"])
+def test_alpha_map_scales_the_light_through_a_sheet(renderer):
+    """An alpha-mapped sheet between the floor and its light
+    (path_tracing.cu:15-25 stochastic alpha for scattered rays,
+    light_transport_common.h:206-219 fractional visibility for shadow and
+    connection rays): with alpha 0 the floor is lit exactly as without the
+    sheet, with alpha 1 not at all (up to rays lost through the sheet's
+    diagonal edge), and with alpha 1/2 by half (the sheet is black, so all
+    the floor's light crosses it once)."""
+    from vlr_b200 import vlr as VV
+    r = {"path_tracing": VV.RENDERER_PATH_TRACING, "light_tracing": VV.RENDERER_LIGHT_TRACING,
+         "bpt": VV.RENDERER_BPT}[renderer]
+    spp = 1024
+    bare = _floor_sum(r, spp, light_at=(0.0, 0.0))
+    clear = _floor_sum(r, spp, light_at=(0.0, 0.0), blocker_alpha=0.0)
+    opaque = _floor_sum(r, spp, light_at=(0.0, 0.0), blocker_alpha=1.0)
+    half = _floor_sum(r, spp, light_at=(0.0, 0.0), blocker_alpha=0.5)
+    assert bare > 0.0
+    assert abs(clear / bare - 1) < 1e-3, clear / bare
+    # rays that graze the sheet's shared diagonal can slip between its two
+    # triangles (the ray/triangle test is not watertight): about 1e-6 of the light
+    assert opaque / bare < 1e-4, opaque / bare
+    assert abs(half / bare - 0.5) < 0.02, half / bare
+
+
+def _normal_map_node(ctx, local_normal, bump_type, extra=()):
+    """A 2 x 2 constant Image2DTexture encoding a shading-frame normal as
+    RGB = (n + 1) / 2 (y stored flipped for DirectX maps)."""
+    n = np.asarray(local_normal, np.float64)
+    stored = n.copy()
+    if bump_type == "Normal Map (DirectX)":
+        stored[1] = -stored[1]
+    rgba = np.ones((2, 2, 4), np.float32)
+    rgba[..., :3] = (stored + 1) / 2
+    img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
+    tex = ctx.createShaderNode("Image2DTexture")
+    tex.set("image", img)
+    tex.set_enum("bump type", bump_type)
+    for k, v in extra:
+        tex.set_enum(k, v)
+    return img, tex
+
+
+def _bumped_world_normal(local_normal, coeff):
+    """World normal of the floor's bumped frame (tangent +x, bitangent
+    cross(n, t) = -z, normal +y) for a map normal whose tangential part the
+    node scales by the decoded coefficient."""
+    n = np.array([local_normal[0] * coeff, local_normal[1] * coeff, local_normal[2]], np.float64)
+    n /= np.linalg.norm(n)
+    return (n[0], n[2], -n[1])
+
+
+@pytest.mark.parametrize("bump_type", ["Normal Map (OpenGL)", "Normal Map (DirectX)"])
+def test_normal_map_tilts_the_shading_frame_like_vertex_normals(bump_type):
+    """A constant normal map (shader_nodes.cu:349-391, applyBumpMapping in
+    renderer_common.h:554-576) shades a flat floor as vertex normals tilted
+    to the same world normal do; the default bump coefficient 1 reaches the
+    kernel as 17/16 (5-bit storage, shader_nodes.cpp:1684-1686).  The light
+    sits off to +x, -z, so the tilt (in both tangent directions) changes the
+    floor's brightness well beyond the tolerance."""
+    from vlr_b200 import vlr as VV
+    local = (0.3, 0.4, np.sqrt(0.75))
+    world = _bumped_world_normal(local, 17 / 16)
+    spp = 256
+    flat = _floor_sum(VV.RENDERER_PATH_TRACING, spp, light_at=(1.2, -1.2))
+    tilted = _floor_sum(VV.RENDERER_PATH_TRACING, spp, light_at=(1.2, -1.2), floor_normal=world)
+    W = H = 48
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    img, tex = _normal_map_node(ctx, local, bump_type)
+    scene, cam, keep = _floor_scene(ctx, W, H, light_at=(1.2, -1.2), normal_plug=tex.plug(VV.PLUG_NORMAL3D, 0))
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=4)
+    ctx.render_samples(cam, True, spp)
+    mapped = _y_of(ctx.read_film()).sum()
+    ctx.close()
+    assert abs(tilted / flat - 1) > 0.1, tilted / flat
+    assert abs(mapped / tilted - 1) < 0.01, (mapped / tilted, tilted / flat)
+
+
+def test_height_map_slope_tilts_the_shading_frame():
+    """A height map (shader_nodes.cu:380-387) rising linearly in -u by
+    `step` per texel gives the normal (-dh/du, 0, 1) with dh/du = 5/1024 x
+    width x the difference of neighbouring texels, read from the bilinear
+    footprint; clamped at the edges, which the camera does not see."""
+    from vlr_b200 import vlr as VV
+    Wt = 64
+    step = -1.5
+    coeff = 17 / 16
+    h = (100.0 + step * np.arange(Wt))[None, :].repeat(8, axis=0)
+    rgba = np.ones((8, Wt, 4), np.float32)
+    rgba[..., 0] = h
+    dhdu = (5.0 / 1024) * Wt * step
+    world = _bumped_world_normal((-dhdu, 0.0, 1.0), coeff)
+    spp = 256
+    tilted = _floor_sum(VV.RENDERER_PATH_TRACING, spp, light_at=(1.2, 0.0), floor_normal=world)
+    flat = _floor_sum(VV.RENDERER_PATH_TRACING, spp, light_at=(1.2, 0.0))
+    W = H = 48
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
+    tex = ctx.createShaderNode("Image2DTexture")
+    tex.set("image", img)
+    tex.set_enum("bump type", "Height Map")
+    tex.set_enum("wrap u", "Clamp to Edge")
+    tex.set_enum("wrap v", "Clamp to Edge")
+    scene, cam, keep = _floor_scene(ctx, W, H, light_at=(1.2, 0.0), normal_plug=tex.plug(VV.PLUG_NORMAL3D, 0))
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=4)
+    ctx.render_samples(cam, True, spp)
+    mapped = _y_of(ctx.read_film()).sum()
+    ctx.close()
+    assert abs(tilted / flat - 1) > 0.1, tilted / flat
+    assert abs(mapped / tilted - 1) < 0.01, (mapped / tilted, tilted / flat)
+
+
 def _trace(v, rays, rounds, any_hit):
     L = V.lib()
     L.vlrbTraceRaysHost.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

@@ -783,16 +783,17 @@ __global__ void __launch_bounds__(256) connectKernel(BptArgs a) {
     const float lam[4] = { a.wls.lambda[0], a.wls.lambda[1], a.wls.lambda[2], a.wls.lambda[3] };
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         ShadowRay sr = a.pb.shadow[i];
-        Hit h = traceBvh<true>(a.S.bvh, V3(sr.org.x, sr.org.y, sr.org.z), V3(sr.dir.x, sr.dir.y, sr.dir.z), sr.org.w);
-        if (h.prim != 0xFFFFFFFFu) continue;
+        const float vis = shadowVisibility(a.S, V3(sr.org.x, sr.org.y, sr.org.z), V3(sr.dir.x, sr.dir.y, sr.dir.z),
+                                           sr.org.w);
+        if (vis == 0.0f) continue;
         uint32_t target = __float_as_uint(sr.dir.w);
         if (target & kSplatBit) {
             uint32_t pixel = target & ~kSplatBit;
-            filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, toS4(sr.contrib));
+            filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, vis * toS4(sr.contrib));
         }
         else {
             float4 c = a.pb.contrib[target];
-            c.x += sr.contrib.x; c.y += sr.contrib.y; c.z += sr.contrib.z; c.w += sr.contrib.w;
+            c.x += vis * sr.contrib.x; c.y += vis * sr.contrib.y; c.z += vis * sr.contrib.z; c.w += vis * sr.contrib.w;
             a.pb.contrib[target] = c;
         }
     }
@@ -1045,12 +1046,12 @@ __global__ void __launch_bounds__(256) ltSplatKernel(BptArgs a, uint32_t stage) 
     const uint32_t n = min(bounceCounters(a.pb, stage)[kCntShadow], a.numPaths);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const LtConnection k = a.conn[i];
-        const Hit h = traceBvh<true>(a.S.bvh, V3(k.org.x, k.org.y, k.org.z), V3(k.dir.x, k.dir.y, k.dir.z), k.org.w);
-        if (h.prim != 0xFFFFFFFFu) continue;
+        const float vis = shadowVisibility(a.S, V3(k.org.x, k.org.y, k.org.z), V3(k.dir.x, k.dir.y, k.dir.z), k.org.w);
+        if (vis == 0.0f) continue;
         const uint32_t pixel = __float_as_uint(k.dir.w);
         if (pixel >= a.stride * a.height) continue;
         const float lam[4] = { k.lambda.x, k.lambda.y, k.lambda.z, k.lambda.w };
-        filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, toS4(k.contrib));
+        filmAdd(a.film.strata + static_cast<size_t>(pixel) * kNumStrata, lam, vis * toS4(k.contrib));
     }
 }
 

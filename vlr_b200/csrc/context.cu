@@ -285,6 +285,7 @@ struct FlatScene {
     std::vector<std::vector<uint32_t>> geomInstTris;
     std::vector<std::vector<float>> geomInstAreas;
     std::vector<uint32_t> geomInstPoints;        // 1: the geometry instance is points (ids into pt*)
+    std::vector<VLRShaderNodePlug> geomInstNormal, geomInstAlpha;   // the group's nodeNormal / nodeAlpha
     std::vector<float4> ptPos, ptNrm, ptTan;     // points of PointSurfaceNodes, world space
     uint32_t numInstances = 0;
     V3 lo{ FLT_MAX, FLT_MAX, FLT_MAX }, hi{ -FLT_MAX, -FLT_MAX, -FLT_MAX };
@@ -323,6 +324,8 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
             f.geomInstTris.emplace_back();
             f.geomInstAreas.emplace_back();
             f.geomInstPoints.push_back(0u);
+            f.geomInstNormal.push_back(g.nodeNormal);
+            f.geomInstAlpha.push_back(g.nodeAlpha);
             for (size_t k = 0; k + 2 < g.indices.size(); k += 3) {
                 uint32_t i0 = g.indices[k], i1 = g.indices[k + 1], i2 = g.indices[k + 2];
                 if (i0 >= mesh->vertices.size() || i1 >= mesh->vertices.size() || i2 >= mesh->vertices.size())
@@ -367,6 +370,8 @@ void flattenNode(FlatScene &f, const Node* n, const float world[16], const float
             f.geomInstTris.emplace_back();
             f.geomInstAreas.emplace_back();
             f.geomInstPoints.push_back(1u);
+            f.geomInstNormal.push_back(VLRShaderNodePlug{});
+            f.geomInstAlpha.push_back(VLRShaderNodePlug{});
             for (uint32_t idx : g.indices) {
                 if (idx >= pts->vertices.size()) throw std::runtime_error("point index out of range");
                 f.geomInstTris.back().push_back(base + idx);
@@ -419,6 +424,16 @@ SpType parseSpectrumType(const std::string &s) {
     if (l.find("light") != std::string::npos) return SpType::LightSource;
     if (l.find("ior") != std::string::npos || l.find("refraction") != std::string::npos) return SpType::IOR;
     return SpType::Reflectance;
+}
+
+// Image2DTexture's bump coefficient as kernels see it: stored in 5 bits as
+// min(round(31 * c / 2), 31) and read back as (stored + 1) / 16
+// (shader_nodes.cpp:1684-1686, shared/shared.h:743-746).
+float decodedBumpCoeff(float c) {
+    const uint32_t maxInt = 31;
+    const float r = std::round(maxInt * c * 0.5f);
+    const uint32_t stored = r <= 0.0f ? 0u : std::min<uint32_t>(static_cast<uint32_t>(r), maxInt);
+    return static_cast<float>(stored + 1) / 16.0f;
 }
 
 cudaTextureAddressMode parseWrap(const std::string &s) {
@@ -540,59 +555,100 @@ void Context::buildScene(cudaStream_t stream) {
     sg.tri = upload(f.tri, stream);
     sg.triMaterial = upload(f.triMaterial, stream);
     for (MatDesc &md : f.mats) md.bsdfFlags = options.consistentDielectricPdf ? kBsdfConsistentPdf : 0u;
-    // Image2DTexture plugs on material spectra
+    // Image2DTexture plugs: material spectra, then the groups' normal and alpha maps
     {
-        std::map<const Object*, int32_t> texIndex;
+        std::map<std::pair<const Object*, bool>, int32_t> texIndex;
         std::vector<unsigned long long> texObjs;
         std::vector<uint32_t> texTypes;
+        // Texture index of an Image2DTexture node (-1: not one, or no image);
+        // pointSampled: a nearest-filtered object of the same image (height maps).
+        auto textureOf = [&](const VLRShaderNodePlug &plug, bool pointSampled, const Image2D** imgOut) -> int32_t {
+            if (!plug.nodeRef) return -1;
+            const auto* node = reinterpret_cast<const ShaderNode*>(plug.nodeRef);
+            if (lower(node->typeName) != "image2dtexture") return -1;
+            auto io = node->objects.find("image");
+            const auto* img = io != node->objects.end() ? static_cast<const Image2D*>(io->second) : nullptr;
+            if (!img || img->width == 0 || img->height == 0 ||
+                img->rgba.size() < size_t(img->width) * img->height * 4)
+                return -1;
+            if (imgOut) *imgOut = img;
+            auto it = texIndex.find({ node, pointSampled });
+            if (it != texIndex.end()) return it->second;
+            auto st = std::make_unique<SceneTexture>();
+            const cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+            ck(cudaMallocArray(&st->array, &ch, img->width, img->height), "texture array");
+            ck(cudaMemcpy2DToArray(st->array, 0, 0, img->rgba.data(), size_t(img->width) * 16,
+                                   size_t(img->width) * 16, img->height, cudaMemcpyHostToDevice),
+               "texture upload");
+            cudaResourceDesc rd{};
+            rd.resType = cudaResourceTypeArray;
+            rd.res.array.array = st->array;
+            cudaTextureDesc td{};
+            auto en = [&](const char* k, const char* d) {
+                auto e = node->enums.find(k);
+                return e != node->enums.end() ? e->second : std::string(d);
+            };
+            td.addressMode[0] = parseWrap(en("wrap u", "Repeat"));
+            td.addressMode[1] = parseWrap(en("wrap v", "Repeat"));
+            td.filterMode = pointSampled || lower(en("mag filter", "Linear")) == "nearest" ? cudaFilterModePoint
+                                                                                          : cudaFilterModeLinear;
+            td.readMode = cudaReadModeElementType;
+            td.normalizedCoords = 1;
+            ck(cudaCreateTextureObject(&st->tex, &rd, &td, nullptr), "texture object");
+            const int32_t index = static_cast<int32_t>(texObjs.size());
+            texIndex.emplace(std::make_pair(static_cast<const Object*>(node), pointSampled), index);
+            texObjs.push_back(static_cast<unsigned long long>(st->tex));
+            // 8-bit sRGB images are linearised when created (vlrLinearImage2DCreate)
+            const bool eightBit = img->format != "RGBA32Fx4" && img->format != "Gray32F";
+            const ColorSp cs = eightBit && parseColorSpace(img->colorSpace) == ColorSp::sRGB
+                                   ? ColorSp::Rec709 : parseColorSpace(img->colorSpace);
+            texTypes.push_back(static_cast<uint32_t>(parseSpectrumType(img->spectrumType)) |
+                               (static_cast<uint32_t>(cs) << 8));
+            sceneTextures.push_back(std::move(st));
+            return index;
+        };
         for (size_t i = 0; i < f.matObjs.size() && i < f.mats.size(); ++i) {
             const SurfaceMaterial* m = f.matObjs[i];
             auto slots = textureSlots().find(lower(m->typeName));
             if (slots == textureSlots().end()) continue;
             for (const auto &ps : slots->second) {
                 auto pl = m->plugs.find(ps.first);
-                if (pl == m->plugs.end() || !pl->second.nodeRef) continue;
-                const auto* node = reinterpret_cast<const ShaderNode*>(pl->second.nodeRef);
-                if (lower(node->typeName) != "image2dtexture") continue;
-                auto it = texIndex.find(node);
-                if (it == texIndex.end()) {
-                    auto io = node->objects.find("image");
-                    const auto* img = io != node->objects.end() ? static_cast<const Image2D*>(io->second) : nullptr;
-                    if (!img || img->width == 0 || img->height == 0 ||
-                        img->rgba.size() < size_t(img->width) * img->height * 4)
-                        continue;
-                    auto st = std::make_unique<SceneTexture>();
-                    const cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
-                    ck(cudaMallocArray(&st->array, &ch, img->width, img->height), "texture array");
-                    ck(cudaMemcpy2DToArray(st->array, 0, 0, img->rgba.data(), size_t(img->width) * 16,
-                                           size_t(img->width) * 16, img->height, cudaMemcpyHostToDevice),
-                       "texture upload");
-                    cudaResourceDesc rd{};
-                    rd.resType = cudaResourceTypeArray;
-                    rd.res.array.array = st->array;
-                    cudaTextureDesc td{};
-                    auto en = [&](const char* k, const char* d) {
-                        auto e = node->enums.find(k);
-                        return e != node->enums.end() ? e->second : std::string(d);
-                    };
-                    td.addressMode[0] = parseWrap(en("wrap u", "Repeat"));
-                    td.addressMode[1] = parseWrap(en("wrap v", "Repeat"));
-                    td.filterMode = lower(en("mag filter", "Linear")) == "nearest" ? cudaFilterModePoint
-                                                                                   : cudaFilterModeLinear;
-                    td.readMode = cudaReadModeElementType;
-                    td.normalizedCoords = 1;
-                    ck(cudaCreateTextureObject(&st->tex, &rd, &td, nullptr), "texture object");
-                    it = texIndex.emplace(node, static_cast<int32_t>(texObjs.size())).first;
-                    texObjs.push_back(static_cast<unsigned long long>(st->tex));
-                    // 8-bit sRGB images are linearised when created (vlrLinearImage2DCreate)
-                    const bool eightBit = img->format != "RGBA32Fx4" && img->format != "Gray32F";
-                    const ColorSp cs = eightBit && parseColorSpace(img->colorSpace) == ColorSp::sRGB
-                                           ? ColorSp::Rec709 : parseColorSpace(img->colorSpace);
-                    texTypes.push_back(static_cast<uint32_t>(parseSpectrumType(img->spectrumType)) |
-                                       (static_cast<uint32_t>(cs) << 8));
-                    sceneTextures.push_back(std::move(st));
+                if (pl == m->plugs.end()) continue;
+                const int32_t t = textureOf(pl->second, false, nullptr);
+                if (t >= 0) f.mats[i].tex[ps.second] = t;
+            }
+        }
+        std::vector<GeomMaps> maps(f.geomInstMaterial.size() + 1);
+        bool anyMap = false;
+        for (size_t g = 0; g < f.geomInstMaterial.size(); ++g) {
+            if (f.geomInstPoints[g]) continue;
+            const VLRShaderNodePlug &np = f.geomInstNormal[g];
+            if (np.nodeRef && (np.info & 0xFFu) == VLRShaderNodePlugType_Normal3D) {
+                const auto* node = reinterpret_cast<const ShaderNode*>(np.nodeRef);
+                auto bt = node->enums.find("bump type");
+                const std::string b = lower(bt != node->enums.end() ? bt->second : std::string("Normal Map (DirectX)"));
+                const uint32_t bump = b == "height map" ? kBumpHeight
+                                      : b == "normal map (opengl)" ? kBumpNormalOpenGL : kBumpNormalDirectX;
+                const Image2D* img = nullptr;
+                const int32_t t = textureOf(np, bump == kBumpHeight, &img);
+                if (t >= 0) {
+                    maps[g].normalTex = t;
+                    maps[g].normalInfo = bump | (((np.info >> 8) & 0xFFu) << 8);
+                    maps[g].bumpCoeff = decodedBumpCoeff(node->getFloat("bump coeff", 1.0f));
+                    maps[g].texW = static_cast<float>(img->width);
+                    maps[g].texH = static_cast<float>(img->height);
+                    anyMap = true;
                 }
-                f.mats[i].tex[ps.second] = it->second;
+            }
+            const VLRShaderNodePlug &ap = f.geomInstAlpha[g];
+            if (ap.nodeRef && (ap.info & 0xFFu) == VLRShaderNodePlugType_Alpha) {
+                const int32_t t = textureOf(ap, false, nullptr);
+                if (t >= 0) {
+                    maps[g].alphaTex = t;
+                    maps[g].alphaOption = (ap.info >> 8) & 0xFFu;
+                    sg.hasAlphaMaps = 1;
+                    anyMap = true;
+                }
             }
         }
         if (!texObjs.empty()) {
@@ -601,6 +657,7 @@ void Context::buildScene(cudaStream_t stream) {
             sg.meng.colorMats = deviceColorMatrices();
             sg.uv = upload(f.uv, stream);
         }
+        if (anyMap) sg.geomMaps = upload(maps, stream);
     }
     // Material spectra are immediate colours: each is tabulated once here on
     // the 95-sample grid, so a hit interpolates one table per spectrum.

@@ -78,11 +78,19 @@ __device__ __forceinline__ bool triTest(const BvhTri &tr, const V3 &org, const V
 
 constexpr int kTraversalStack = 64;
 
+// Accepts every intersection (opaque geometry).
+struct AcceptAll {
+    __device__ __forceinline__ bool operator()(uint32_t, float, float) const { return true; }
+};
+
 // Closest hit (anyHit == false) or first hit (anyHit == true) along
-// org + t*dir, t in (0, tmax).  Ordered front-to-back descent with a short
+// org + t*dir, t in (0, tmax), among the intersections `accept(prim, b1, b2)`
+// keeps (the any-hit program's role: an ignored intersection neither ends
+// the ray nor shortens it).  Ordered front-to-back descent with a short
 // per-thread stack.
-template <bool anyHit>
-__device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 &dir, float tmax) {
+template <bool anyHit, class Accept>
+__device__ __forceinline__ Hit traceBvhWith(const Bvh &bvh, const V3 &org, const V3 &dir, float tmax,
+                                            Accept &accept) {
     Hit h;
     h.t = tmax;
     h.prim = 0xFFFFFFFFu;
@@ -123,7 +131,7 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
             BvhTri tr;
             tr.v0 = __ldg(tp + 0); tr.e1 = __ldg(tp + 1); tr.e2 = __ldg(tp + 2);
             float t, b1, b2;
-            if (triTest(tr, org, dir, h.t, &t, &b1, &b2)) {
+            if (triTest(tr, org, dir, h.t, &t, &b1, &b2) && accept(__float_as_uint(tr.v0.w), b1, b2)) {
                 h.t = t; h.b1 = b1; h.b2 = b2;
                 h.prim = __float_as_uint(tr.v0.w);
                 if (anyHit) return h;
@@ -134,6 +142,12 @@ __device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 
     }
     if (overflow && bvh.errorFlag) atomicOr(bvh.errorFlag, 2u);
     return h;
+}
+
+template <bool anyHit>
+__device__ __forceinline__ Hit traceBvh(const Bvh &bvh, const V3 &org, const V3 &dir, float tmax) {
+    AcceptAll all;
+    return traceBvhWith<anyHit>(bvh, org, dir, tmax, all);
 }
 
 #endif

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) traceKernel(SceneGPU S, PathBuffers pb, F
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = queue[i];
         float4 o = pb.rayOrg[p], d = pb.rayDir[p];
-        Hit h = traceBvh<false>(S.bvh, V3(o.x, o.y, o.z), V3(d.x, d.y, d.z), o.w);
+        Hit h = traceClosest(S, V3(o.x, o.y, o.z), V3(d.x, d.y, d.z), o.w, S.hasAlphaMaps ? pb.rng[p] : 0ull);
         pb.hit[p] = make_float4(h.t, h.b1, h.b2, __uint_as_float(h.prim));
         uint32_t key = kNumBsdfKinds;
         if (h.prim != 0xFFFFFFFFu)
@@ -192,7 +192,7 @@ __device__ __forceinline__ void loadMixture(const GuideFrame &gf, uint32_t P, ui
     m.scale[4] = s1.x; m.scale[5] = s1.y; m.scale[6] = s1.z; m.scale[7] = s1.w;
 }
 
-template <bool kGuide>
+template <bool kGuide, bool kMaps>
 __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb, FrameParams fp, GuideFrame gf) {
     uint32_t* ctr = bounceCounters(pb, fp.bounce);
     uint32_t* next = bounceCounters(pb, fp.bounce + 1);
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         const uint32_t prim = __float_as_uint(h.w);
         SurfPt sp;
         float hypAreaPDF;
-        decodeHit(S, prim, h.y, h.z, &sp, &hypAreaPDF);
+        decodeHit<kMaps>(S, prim, h.y, h.z, &sp, &hypAreaPDF);
         const MatDesc &mat = S.mats[__ldg(S.triMaterial + prim)];
         Bsdf bsdf = buildBsdf(S.meng, mat, wls, sp.tu, sp.tv);
         float4 o4 = pb.rayOrg[p], d4 = pb.rayDir[p];
@@ -422,11 +422,12 @@ __global__ void __launch_bounds__(256) shadowKernel(SceneGPU S, PathBuffers pb, 
     const uint32_t n = bounceCounters(pb, fp.bounce)[kCntShadow];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         ShadowRay sr = pb.shadow[i];
-        Hit h = traceBvh<true>(S.bvh, V3(sr.org.x, sr.org.y, sr.org.z), V3(sr.dir.x, sr.dir.y, sr.dir.z), sr.org.w);
-        if (h.prim == 0xFFFFFFFFu) {
+        const float vis = shadowVisibility(S, V3(sr.org.x, sr.org.y, sr.org.z), V3(sr.dir.x, sr.dir.y, sr.dir.z),
+                                           sr.org.w);
+        if (vis != 0.0f) {
             uint32_t p = __float_as_uint(sr.dir.w);
             float4 c = pb.contrib[p];
-            c.x += sr.contrib.x; c.y += sr.contrib.y; c.z += sr.contrib.z; c.w += sr.contrib.w;
+            c.x += vis * sr.contrib.x; c.y += vis * sr.contrib.y; c.z += vis * sr.contrib.z; c.w += vis * sr.contrib.w;
             pb.contrib[p] = c;
         }
     }
@@ -780,8 +781,11 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
             T.end(stream);
         }
         T.begin(kStageShade, stream, pMain + (guiding ? sizeof(GuideFrame) : 0));
-        if (guiding) shadeKernel<true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
-        else shadeKernel<false><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
+        const bool maps = scene.geomMaps != nullptr;
+        if (guiding && maps) shadeKernel<true, true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
+        else if (guiding) shadeKernel<true, false><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
+        else if (maps) shadeKernel<false, true><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
+        else shadeKernel<false, false><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
         T.end(stream);
         T.begin(kStageShadow, stream, pMain);
         shadowKernel<<<grid, 256, 0, stream>>>(scene, pb, fp);

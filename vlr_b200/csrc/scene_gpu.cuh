@@ -29,6 +29,23 @@ struct MatDesc {
     int32_t tex[3] = { -1, -1, -1 };         // sp[0..2]: Image2DTexture index (-1: none)
 };
 
+// Bump types of Image2DTexture (shared/shared.h:147-151).
+enum BumpKind : uint32_t { kBumpNormalDirectX = 0, kBumpNormalOpenGL = 1, kBumpHeight = 2 };
+
+// Normal and alpha maps of one geometry instance: the material group's
+// nodeNormal and nodeAlpha plugs when they are Image2DTexture nodes
+// (kernel_common.h:70-72).  Texture indices address MengTables::textures;
+// height maps read a point-sampled texture of their image.
+struct GeomMaps {
+    int32_t normalTex = -1;     // -1: no normal map
+    uint32_t normalInfo = 0;    // BumpKind | plug option << 8
+    float bumpCoeff = 1.0f;     // decoded 5-bit coefficient
+    float texW = 0.0f, texH = 0.0f;   // size of the normal map's image
+    int32_t alphaTex = -1;      // -1: opaque
+    uint32_t alphaOption = 0;   // channel read as alpha
+    uint32_t pad = 0;
+};
+
 // Spectrum slot 0-2 (sp) or 3 (emit) of material m at the path's wavelengths
 // and texture coordinates (tu, tv): a texture's filtered RGB upsampled at the
 // hit (Image2DTextureShaderNode_Spectrum, shader_nodes.cu:410-445), else the
@@ -36,7 +53,7 @@ struct MatDesc {
 VLRB_HD S4 matSpectrum(const MengTables &T, const MatDesc &m, int slot, const WLS &wls, float tu = 0.0f,
                        float tv = 0.0f) {
 #if defined(__CUDA_ARCH__)
-    if (slot < 3 && m.tex[slot] >= 0 && T.textures) {
+    if (T.textures && slot < 3 && m.tex[slot] >= 0) {
         const float4 c = tex2DLod<float4>(T.textures[m.tex[slot]], tu, tv, 0.0f);
         const uint32_t info = T.texSpType[m.tex[slot]];
         const UpSpec up = mengUpsample(T, *T.colorMats, static_cast<SpType>(info & 0xFFu),
@@ -173,6 +190,8 @@ struct SceneGPU {
     const uint4* tri;         // [numTris] i0, i1, i2, geomInst
     const uint32_t* triMaterial;
     const MatDesc* mats;
+    const GeomMaps* geomMaps;       // [numGeomInsts], null when no group has a normal or alpha map
+    uint32_t hasAlphaMaps;          // some group has an alpha map: traversal runs the alpha test
     // lights
     Dist1D lightInsts;              // over light instances (env first if present)
     const uint32_t* instFirstGroup; // per light instance
@@ -264,8 +283,144 @@ __device__ __forceinline__ V3 ld3(const float4* p, uint32_t i) {
     return V3(v.x, v.y, v.z);
 }
 
+// The four texels of the bilinear footprint at (tu, tv), one channel, in
+// texture-gather order (w z over x y: w the footprint's first row and
+// column); `tex` is point-sampled, so each fetch at a texel centre returns
+// that texel, wrapped by the texture's address mode.
+__device__ __forceinline__ float4 footprintTexels(cudaTextureObject_t tex, float tu, float tv, uint32_t channel,
+                                                  float w, float h) {
+    const float i0 = floorf(tu * w - 0.5f), j0 = floorf(tv * h - 0.5f);
+    auto at = [&](float i, float j) {
+        const float4 c = tex2DLod<float4>(tex, (i + 0.5f) / w, (j + 0.5f) / h, 0.0f);
+        return channel == 0 ? c.x : channel == 1 ? c.y : channel == 2 ? c.z : c.w;
+    };
+    return make_float4(at(i0, j0 + 1), at(i0 + 1, j0 + 1), at(i0 + 1, j0), at(i0, j0));
+}
+
+// Image2DTextureShaderNode_Normal3D (shader_nodes.cu:349-391): the normal in
+// the shading frame from a normal map (RGB or GBA by plug option, [0,1] ->
+// [-1,1], y flipped for DirectX maps) or from height-map differences
+// (5/1024 per texel), its tangential part scaled by the bump coefficient.
+__device__ __forceinline__ V3 mapNormal(const unsigned long long* textures, const GeomMaps &gm, float tu, float tv) {
+    const cudaTextureObject_t tex = textures[gm.normalTex];
+    const uint32_t bump = gm.normalInfo & 0xFFu, option = gm.normalInfo >> 8;
+    V3 n(0.0f, 0.0f, 1.0f);
+    if (bump != kBumpHeight) {
+        if (option < 2) {
+            const float4 c = tex2DLod<float4>(tex, tu, tv, 0.0f);
+            n = option == 0 ? V3(c.x, c.y, c.z) : V3(c.y, c.z, c.w);
+            n = V3(2 * n.x - 1.0f, 2 * n.y - 1.0f, 2 * n.z - 1.0f);
+            if (bump == kBumpNormalDirectX) n.y = -n.y;
+        }
+    }
+    else {
+        const float4 g = footprintTexels(tex, tu, tv, option, gm.texW, gm.texH);
+        const float coeff = 5.0f / 1024;
+        const float dhdu = (coeff * gm.texW) * (g.y - g.x);
+        const float dhdv = (coeff * gm.texH) * (g.x - g.w);
+        n = V3(-dhdu, dhdv, 1.0f);
+    }
+    n.x *= gm.bumpCoeff;
+    n.y *= gm.bumpCoeff;
+    return normalize(n);
+}
+
+// applyBumpMapping (renderer_common.h:554-576): rotate the shading frame by
+// the rotation that carries its normal (0, 0, 1) onto n, written as a unit
+// quaternion about the axis (-n.y, n.x, 0) by the tilt angle.
+__device__ __forceinline__ void bumpFrame(const V3 &n, Frame* frame) {
+    if (n.x == 0.0f && n.y == 0.0f) return;
+    const float projLength = sqrtf(n.x * n.x + n.y * n.y);
+    const float tilt = atanf(projLength / n.z);
+    float qSin, qCos;
+    sincosf(tilt / 2, &qSin, &qCos);
+    const float qX = (-n.y / projLength) * qSin, qY = (n.x / projLength) * qSin, qW = qCos;
+    const V3 t(1 - 2 * qY * qY, 2 * qX * qY, -2 * qY * qW);
+    const V3 b(2 * qX * qY, 1 - 2 * qX * qX, 2 * qX * qW);
+    *frame = Frame(frame->fromLocal(t), frame->fromLocal(b), frame->fromLocal(n));
+}
+
+// The shading frame after a group's normal map; kept out of line so that the
+// hit shaders of scenes without normal maps do not carry its registers.
+static __device__ __noinline__ Frame normalMappedFrame(const GeomMaps* gm, const unsigned long long* textures, float tu,
+                                                       float tv, Frame frame) {
+    bumpFrame(mapNormal(textures, *gm, tu, tv), &frame);
+    return frame;
+}
+
+// Alpha of triangle `prim` at barycentrics (b1, b2): its group's alpha map
+// channel (Image2DTextureShaderNode_Alpha, shader_nodes.cu:437-455), 1 for a
+// group without one (getAlpha, renderer_common.h:532-547).
+__device__ __forceinline__ float alphaAt(const SceneGPU &S, uint32_t prim, float b1, float b2) {
+    const uint4 t = __ldg(S.tri + prim);
+    const GeomMaps &gm = S.geomMaps[t.w];
+    if (gm.alphaTex < 0) return 1.0f;
+    const float b0 = 1 - b1 - b2;
+    const float2 a = __ldg(S.uv + t.x), b = __ldg(S.uv + t.y), c = __ldg(S.uv + t.z);
+    const float4 v = tex2DLod<float4>(S.meng.textures[gm.alphaTex], b0 * a.x + b1 * b.x + b2 * c.x,
+                                      b0 * a.y + b1 * b.y + b2 * c.y, 0.0f);
+    const uint32_t o = gm.alphaOption;
+    return o == 0 ? v.x : o == 1 ? v.y : o == 2 ? v.z : o == 3 ? v.w : 0.0f;
+}
+
+// Uniform [0, 1) number for the pair (seed, prim): the SplitMix64 finalizer
+// (Steele, Lea and Flood, "Fast splittable pseudorandom number generators",
+// OOPSLA 2014) of seed + prim times the golden-ratio increment.
+__device__ __forceinline__ float hashUniform(uint64_t seed, uint32_t prim) {
+    uint64_t z = seed + (static_cast<uint64_t>(prim) + 1) * 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return static_cast<float>(static_cast<uint32_t>(z >> 40)) * (1.0f / 16777216.0f);
+}
+
+// Stochastic alpha test of a closest-hit ray (pathTracingAnyHitWithAlpha,
+// path_tracing.cu:15-25): an intersection is kept when u < alpha.  u comes
+// from the path's RNG state mixed with the primitive, so it does not advance
+// the path's stream and a ray meets each triangle with one decision.
+struct StochasticAlpha {
+    const SceneGPU* S;
+    uint64_t seed;
+    __device__ __forceinline__ bool operator()(uint32_t prim, float b1, float b2) const {
+        const float a = alphaAt(*S, prim, b1, b2);
+        return a >= 1.0f || hashUniform(seed, prim) < a;
+    }
+};
+
+// Shadow rays (shadowAnyHitWithAlpha, light_transport_common.h:206-219): the
+// visibility is the product of (1 - alpha) over the surfaces the segment
+// crosses; an intersection ends the ray once that product reaches 0.
+struct AlphaVisibility {
+    const SceneGPU* S;
+    float visibility;
+    __device__ __forceinline__ bool operator()(uint32_t prim, float b1, float b2) {
+        visibility *= 1.0f - alphaAt(*S, prim, b1, b2);
+        return visibility == 0.0f;
+    }
+};
+
+// Fractional visibility of the segment org + t dir, t in (0, tmax).
+__device__ __forceinline__ float shadowVisibility(const SceneGPU &S, const V3 &org, const V3 &dir, float tmax) {
+    if (!S.hasAlphaMaps) return traceBvh<true>(S.bvh, org, dir, tmax).prim == 0xFFFFFFFFu ? 1.0f : 0.0f;
+    AlphaVisibility av{ &S, 1.0f };
+    const Hit h = traceBvhWith<true>(S.bvh, org, dir, tmax, av);
+    return h.prim == 0xFFFFFFFFu ? av.visibility : 0.0f;
+}
+
+// Closest hit of a path's ray, alpha-tested with the path's RNG state.
+__device__ __forceinline__ Hit traceClosest(const SceneGPU &S, const V3 &org, const V3 &dir, float tmax,
+                                            uint64_t rngState) {
+    if (!S.hasAlphaMaps) return traceBvh<false>(S.bvh, org, dir, tmax);
+    StochasticAlpha sa{ &S, rngState };
+    return traceBvhWith<false>(S.bvh, org, dir, tmax, sa);
+}
+
 // decodeLocalHitPointForTriangle + calcSurfacePoint (triangle.cu:6-53,
-// renderer_common.h:609-626) on world-space vertices.
+// renderer_common.h:609-626) on world-space vertices, the group's normal map
+// applied to the shading frame.
+// kNormalMaps false: the caller knows the scene has no normal maps (a
+// hit shader compiled without the normal-map call keeps its registers).
+template <bool kNormalMaps = true>
 __device__ __forceinline__ void decodeHit(const SceneGPU &S, uint32_t prim, float b1, float b2, SurfPt* sp,
                                           float* hypAreaPDF) {
     uint4 t = __ldg(S.tri + prim);
@@ -309,6 +464,8 @@ __device__ __forceinline__ void decodeHit(const SceneGPU &S, uint32_t prim, floa
         sp->tu = 0.0f;
         sp->tv = 0.0f;
     }
+    if (kNormalMaps && S.geomMaps && S.geomMaps[g].normalTex >= 0)
+        sp->frame = normalMappedFrame(S.geomMaps + g, S.meng.textures, sp->tu, sp->tv, sp->frame);
     sp->u = b0;
     sp->v = b1;
     sp->atInfinity = false;

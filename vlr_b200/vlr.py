@@ -67,7 +67,9 @@ class VLRBBatchItem(ctypes.Structure):
 RENDERER_PATH_TRACING = 0
 RENDERER_LIGHT_TRACING = 1
 RENDERER_BPT = 2
+PLUG_NORMAL3D = 6
 PLUG_SPECTRUM = 7
+PLUG_ALPHA = 8
 
 
 def _api():
@@ -227,10 +229,13 @@ class TriangleMesh:
         check(_api().vlrTriangleMeshSurfaceNodeSetVertices(self.h, a.ctypes.data_as(c_void_p), a.shape[0]),
               "setVertices")
 
-    def add_material_group(self, indices, material):
+    def add_material_group(self, indices, material, normal=None, tangent=None, alpha=None):
+        """normal / tangent / alpha: Plug objects (the group's nodeNormal,
+        nodeTangent and nodeAlpha), None for none."""
         idx = np.ascontiguousarray(indices, dtype=np.uint32)
+        P = lambda pl: pl.plug if pl is not None else NULL_PLUG
         check(_api().vlrTriangleMeshSurfaceNodeAddMaterialGroup(
-            self.h, idx.ctypes.data_as(c_void_p), idx.size, material.h, NULL_PLUG, NULL_PLUG, NULL_PLUG),
+            self.h, idx.ctypes.data_as(c_void_p), idx.size, material.h, P(normal), P(tangent), P(alpha)),
             "addMaterialGroup")
 
 
