@@ -85,6 +85,9 @@ typedef struct VLRBRenderOptions {
     uint32_t blocksPerSM;         /* grid of the wavefront kernels = SMs x this (0 = 8) */
     uint32_t bvhTreeletRounds;    /* treelet restructuring rounds after the LBVH build
                                      (vlrbBvhBuildOptimizedHost), 0..8; default 3 */
+    uint32_t auxBuffers;          /* 1: fill the denoiser's guide buffers (first-hit albedo and
+                                     normal) with every render, as vlrContextRender(denoise = true)
+                                     does for its own call; read with vlrbContextReadAuxBuffers */
 } VLRBRenderOptions;
 
 VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOptions* options);
@@ -160,6 +163,24 @@ VLRResult vlrbContextGetGuideNet(VLRContext context, VLRBGuideNet* net);
 /* Copies the FP64 spectral film (width * height * 16 doubles, strata of
  * 29.375 nm over 360-830 nm, sum over accumulated samples) to host memory. */
 VLRResult vlrbContextReadFilm(VLRContext context, double* strata);
+
+/* The denoiser's guide images of the current accumulation (the reference's
+ * linearAlbedoBuffer / linearNormalBuffer, post_process.cu:33-91): first-hit
+ * base colour in linear Rec.709 and the shading normal in the camera frame
+ * (x negated), width * height RGBA32F each; either pointer may be NULL.
+ * InvalidArgument until a render with VLRBRenderOptions::auxBuffers or
+ * denoise has filled them since the accumulation started. */
+VLRResult vlrbContextReadAuxBuffers(VLRContext context, float* albedo, float* normal);
+
+/* Writes <pathWithoutExtension>.png (8-bit RGBA: max(0), x brightnessCoeff,
+ * 1 - exp(-x), sRGB gamma, as HostProgram/main.cpp:120-168 tone-maps) and
+ * <pathWithoutExtension>.exr (linear, half-float A/B/G/R, no compression)
+ * from a width * height RGBA32F image in host memory.  Host-only. */
+VLRResult vlrbWriteOutputImages(const float* rgba, uint32_t width, uint32_t height,
+                                const char* pathWithoutExtension, float brightnessCoeff);
+
+/* vlrbWriteOutputImages of the context's output image. */
+VLRResult vlrbContextSaveOutputImages(VLRContext context, const char* pathWithoutExtension, float brightnessCoeff);
 
 /* Device address of the RGBA32F output image (width * height * 16 bytes). */
 VLRResult vlrbContextGetOutputDevicePointer(VLRContext context, void** devicePtr);

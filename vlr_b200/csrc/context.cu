@@ -182,6 +182,14 @@ void Context::readOutput(float* host) {
     ck(cudaMemcpy(host, output.ptr, size_t(width) * height * 16, cudaMemcpyDeviceToHost), "read output");
 }
 
+bool Context::readAux(float* albedo, float* normal) {
+    if (!auxCurrent || auxSamples == 0) return false;
+    const size_t bytes = size_t(width) * height * sizeof(float4);
+    if (albedo) ck(cudaMemcpy(albedo, aux.linAlbedo, bytes, cudaMemcpyDeviceToHost), "read aux");
+    if (normal) ck(cudaMemcpy(normal, aux.linNormal, bytes, cudaMemcpyDeviceToHost), "read aux");
+    return true;
+}
+
 void Context::readFilm(double* host) {
     ck(cudaMemcpy(host, film.ptr, size_t(width) * height * kNumStrata * 8, cudaMemcpyDeviceToHost), "read film");
 }
@@ -875,7 +883,7 @@ void Context::trainGuide(cudaStream_t stream) {
 }
 
 void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
-                     uint32_t samples, uint32_t* numAccumFramesOut, uint32_t shrink) {
+                     uint32_t samples, uint32_t* numAccumFramesOut, uint32_t shrink, bool denoise) {
     if (width == 0 || height == 0) throw std::runtime_error("no output buffer bound");
     if (builtGeneration != generation) buildScene(stream);
     if (firstFrame || imgW == 0 || imgW > width || imgH > height) {
@@ -989,6 +997,28 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
     }
     if (samples > 0) filmAddFrames(fl, samples, stream);
     filmToRGBA(fl, output.as<float4>(), stream);
+    // Guide buffers (auxBufferGenerator, run with every frame of every
+    // renderer in the reference, context.cpp:1440-1530): up to 4 first-hit
+    // samples per call; restarted with the accumulation.
+    const bool wantAux = denoise || options.auxBuffers;
+    if (wantAux) {
+        const size_t bytes = auxBufferBytes(width, height);
+        if (auxMem.bytes < bytes || aux.stride != width) {
+            auxMem.resize(bytes);
+            carveAuxBuffers(auxMem.ptr, width, height, &aux);
+            auxCurrent = false;
+        }
+        if (firstFrame || !auxCurrent) {
+            auxClear(aux, height, stream);
+            auxSamples = 0;
+        }
+        const uint32_t auxNow = std::min<uint32_t>(std::max<uint32_t>(samples, 1u), 4u);
+        auxLaunch(sg, aux, imgW, imgH, auxNow, 0x2545F4914F6CDD1DULL * ++auxSeed, stream);
+        auxSamples += auxNow;
+        auxToLinear(sg, aux, imgW, imgH, auxSamples, stream);
+        if (denoise) denoiseLaunch(aux, output.as<float4>(), imgW, imgH, stream);
+    }
+    auxCurrent = wantAux;
     ++timer.totalLaunches;
     timer.paramBytes += sizeof(Film) + 4 + 40 + sizeof(void*);
     if (numAccumFramesOut) *numAccumFramesOut = numAccumFrames;

@@ -5,6 +5,7 @@
 #include "api_objects.h"
 #include "pt.cuh"
 #include "bpt.cuh"
+#include "post.cuh"
 #include "guide_net.h"
 
 #include <memory>
@@ -36,6 +37,7 @@ struct RenderOptions {
     bool consistentDielectricPdf = false;   // see mfBsdfPDF; false = the reference's pdf
     uint32_t blocksPerSM = 8;         // wavefront kernel grid = SMs x blocksPerSM
     uint32_t bvhTreeletRounds = 3;    // treelet restructuring rounds after the LBVH build
+    bool auxBuffers = false;          // fill the denoiser's guide buffers on every render
 };
 
 struct AutotuneTrial {
@@ -87,14 +89,19 @@ public:
     // shrink: on a first frame, render the image at 1/shrink of the output
     // size into the film's top-left region until the next first frame
     // (vlrContextRender's shrinkCoeff, context.cpp:1414)
+    // denoise: fill the guide buffers (as options.auxBuffers does) and
+    // replace the output image by its denoised version.
     void render(cudaStream_t stream, const Camera* cam, bool firstFrame, uint32_t limitFrames,
-                uint32_t samples, uint32_t* numAccumFrames, uint32_t shrink = 1);
+                uint32_t samples, uint32_t* numAccumFrames, uint32_t shrink = 1, bool denoise = false);
     // Times short renders over a grid of (paths in flight, blocks per SM),
     // keeps the fastest in `options`, and returns every trial.  Leaves the
     // film holding the last trial (the next firstFrame render clears it).
     std::vector<AutotuneTrial> autotune(cudaStream_t stream, const Camera* cam, uint32_t samplesPerTrial);
     void readOutput(float* host);
     void readFilm(double* host);
+    // Linear guide images (Rec.709 albedo, camera-space normal), width x
+    // height float4 each; false when no render has filled them.
+    bool readAux(float* albedo, float* normal);
     void readStats(RenderStats* out);
     CUarray outputArray();
     void* outputDevicePtr() const { return output.ptr; }
@@ -148,7 +155,11 @@ private:
         ~SceneTexture();
     };
     std::vector<std::unique_ptr<SceneTexture>> sceneTextures;
-    DeviceBuffer film, output, pathMem, lbvhScratch, bptMem;
+    DeviceBuffer film, output, pathMem, lbvhScratch, bptMem, auxMem;
+    AuxBuffers aux{};
+    uint32_t auxSamples = 0;       // guide samples accumulated since the buffers were cleared
+    uint64_t auxSeed = 0;
+    bool auxCurrent = false;       // the guide buffers follow the current accumulation
     PathBuffers pb{};
     PathBuffers lightPb{};
     std::mt19937_64 bptRng{ 459182033132123413ull };

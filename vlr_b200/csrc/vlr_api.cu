@@ -436,11 +436,11 @@ VLRResult vlrContextRender(VLRContext context, CUstream stream, VLRCameraConst c
     VLRResult e2 = VLRResult_NoError;
     const api::Camera* cam = checked<const api::Camera>(camera, &e2, kindCamera);
     if (!cam || !numAccumFrames) return VLRResult_InvalidArgument;
-    (void)denoise;   // the OptiX denoiser is not part of this library
     if (shrinkCoeff == 0) return VLRResult_InvalidArgument;
     API_TRY
+    // denoise: the guided wavelet denoiser stands in for the OptiX one
     c->render(reinterpret_cast<cudaStream_t>(stream), cam, firstFrame, limitNumAccumFrames, 1, numAccumFrames,
-              shrinkCoeff);
+              shrinkCoeff, denoise);
     return VLRResult_NoError;
     API_CATCH("vlrContextRender")
 }
@@ -1223,6 +1223,7 @@ VLRResult vlrbContextSetRenderOptions(VLRContext context, const VLRBRenderOption
         options->maxPathsInFlight == 0 || options->blocksPerSM > 64 || options->bvhTreeletRounds > 8)
         return VLRResult_InvalidArgument;
     c->options.blocksPerSM = options->blocksPerSM ? options->blocksPerSM : 8;
+    c->options.auxBuffers = options->auxBuffers != 0;
     c->options.maxPathLength = options->maxPathLength;
     c->options.maxPathsInFlight = options->maxPathsInFlight;
     c->options.lightPathsPerFrame = options->lightPathsPerFrame;
@@ -1248,6 +1249,7 @@ VLRResult vlrbContextGetRenderOptions(VLRContext context, VLRBRenderOptions* opt
     options->consistentDielectricPdf = c->options.consistentDielectricPdf ? 1u : 0u;
     options->blocksPerSM = c->options.blocksPerSM;
     options->bvhTreeletRounds = c->options.bvhTreeletRounds;
+    options->auxBuffers = c->options.auxBuffers ? 1u : 0u;
     return VLRResult_NoError;
 }
 
@@ -1379,6 +1381,24 @@ VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats) {
     stats->numTriangles = c->numTriangles();
     return VLRResult_NoError;
     API_CATCH("vlrbContextGetStats")
+}
+
+VLRResult vlrbContextSaveOutputImages(VLRContext context, const char* pathWithoutExtension, float brightnessCoeff) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!pathWithoutExtension || c->width == 0 || c->height == 0) return VLRResult_InvalidArgument;
+    API_TRY
+    std::vector<float> rgba(size_t(c->width) * c->height * 4);
+    c->readOutput(rgba.data());
+    return vlrbWriteOutputImages(rgba.data(), c->width, c->height, pathWithoutExtension, brightnessCoeff);
+    API_CATCH("vlrbContextSaveOutputImages")
+}
+
+VLRResult vlrbContextReadAuxBuffers(VLRContext context, float* albedo, float* normal) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!albedo && !normal) return VLRResult_InvalidArgument;
+    API_TRY
+    return c->readAux(albedo, normal) ? VLRResult_NoError : VLRResult_InvalidArgument;
+    API_CATCH("vlrbContextReadAuxBuffers")
 }
 
 VLRResult vlrbContextReadFilm(VLRContext context, double* strata) {

@@ -33,7 +33,8 @@ class VLRBRenderOptions(ctypes.Structure):
     _fields_ = [("maxPathLength", ctypes.c_uint32), ("maxPathsInFlight", ctypes.c_uint32),
                 ("lightPathsPerFrame", ctypes.c_uint32), ("rngSeed", ctypes.c_uint64),
                 ("consistentDielectricPdf", ctypes.c_uint32), ("blocksPerSM", ctypes.c_uint32),
-                ("bvhTreeletRounds", ctypes.c_uint32)]
+                ("bvhTreeletRounds", ctypes.c_uint32),
+                ("auxBuffers", ctypes.c_uint32)]
 
 
 class VLRBAutotuneTrial(ctypes.Structure):
@@ -83,6 +84,9 @@ def _api():
         "vlrContextBindOutputBuffer": [v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
         "vlrContextGetOutputBufferSize": [v, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)],
         "vlrContextReadOutputBuffer": [v, v],
+        "vlrbContextReadAuxBuffers": [v, v, v],
+        "vlrbWriteOutputImages": [v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_float],
+        "vlrbContextSaveOutputImages": [v, ctypes.c_char_p, ctypes.c_float],
         "vlrContextSetScene": [v, v],
         "vlrContextSetRenderer": [v, ctypes.c_int],
         "vlrContextRender": [v, v, v, ctypes.c_bool, ctypes.c_uint32, ctypes.c_bool, ctypes.c_uint32,
@@ -358,7 +362,7 @@ class Context:
         check(_api().vlrContextSetRenderer(self.h, renderer), "setRenderer")
 
     def setOptions(self, max_path_length=None, max_paths_in_flight=None, light_paths_per_frame=None, rng_seed=None,
-                   consistent_dielectric_pdf=None, blocks_per_sm=None, bvh_treelet_rounds=None):
+                   consistent_dielectric_pdf=None, blocks_per_sm=None, bvh_treelet_rounds=None, aux_buffers=None):
         o = VLRBRenderOptions()
         check(_api().vlrbContextGetRenderOptions(self.h, ctypes.byref(o)), "getOptions")
         if max_path_length is not None:
@@ -375,6 +379,8 @@ class Context:
             o.blocksPerSM = blocks_per_sm
         if bvh_treelet_rounds is not None:
             o.bvhTreeletRounds = bvh_treelet_rounds
+        if aux_buffers is not None:
+            o.auxBuffers = int(bool(aux_buffers))
         check(_api().vlrbContextSetRenderOptions(self.h, ctypes.byref(o)), "setOptions")
 
     def autotune(self, camera, samples_per_trial=4, stream=0):
@@ -421,13 +427,27 @@ class Context:
         check(_api().vlrbContextGetGuidingStats(self.h, ctypes.byref(st)), "getGuidingStats")
         return {k: getattr(st, k) for k, _ in VLRBGuidingStats._fields_}
 
-    def render(self, camera, first_frame, limit=1 << 30, stream=0, shrink=1):
+    def render(self, camera, first_frame, limit=1 << 30, stream=0, shrink=1, denoise=False):
         """One sample per pixel, exactly like vlrContextRender (shrink: the
-        shrinkCoeff preview, fixed at a first frame)."""
+        shrinkCoeff preview, fixed at a first frame; denoise: the output is
+        the denoised image)."""
         n = ctypes.c_uint32()
-        check(_api().vlrContextRender(self.h, c_void_p(stream), camera.h, False, shrink, first_frame, limit,
+        check(_api().vlrContextRender(self.h, c_void_p(stream), camera.h, bool(denoise), shrink, first_frame, limit,
                                       ctypes.byref(n)), "vlrContextRender")
         return n.value
+
+    def read_aux(self):
+        """(albedo, normal): the denoiser's guide images, height x width x 4 each."""
+        a = np.empty((self.height, self.width, 4), np.float32)
+        nrm = np.empty((self.height, self.width, 4), np.float32)
+        check(_api().vlrbContextReadAuxBuffers(self.h, a.ctypes.data_as(c_void_p), nrm.ctypes.data_as(c_void_p)),
+              "readAuxBuffers")
+        return a, nrm
+
+    def save_images(self, path_without_extension, brightness=1.0):
+        """<path>.png (tone-mapped) and <path>.exr (linear half) of the output."""
+        check(_api().vlrbContextSaveOutputImages(self.h, str(path_without_extension).encode(),
+                                                 ctypes.c_float(brightness)), "saveOutputImages")
 
     def render_samples(self, camera, first_frame, samples, limit=1 << 30, stream=0):
         n = ctypes.c_uint32()
@@ -511,6 +531,14 @@ class RenderBatch:
             self.close()
         except Exception:
             pass
+
+
+def write_images(rgba, path_without_extension, brightness=1.0):
+    """vlrbWriteOutputImages: <path>.png and <path>.exr from an H x W x 4 float image."""
+    a = np.ascontiguousarray(rgba, np.float32)
+    h, w = a.shape[:2]
+    check(_api().vlrbWriteOutputImages(a.ctypes.data_as(c_void_p), w, h, str(path_without_extension).encode(),
+                                       ctypes.c_float(brightness)), "writeOutputImages")
 
 
 def quat_rotate_y(angle):
