@@ -601,14 +601,17 @@ def test_texture_pattern_lands_on_the_surface():
 _LOOK_DOWN = (np.sqrt(0.5), 0.0, 0.0, np.sqrt(0.5))   # forward (0, -1, 0)
 
 
-def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=None, blocker_alpha=None):
+def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=None, blocker_alpha=None,
+                 floor_mat=None, light_mat=None):
     """A 4 x 4 white floor at y = 0 (u along +x, v along +z; tangent +x) lit
     by a 1 x 1 downward-facing light at height 2 centred over `light_at`
     (x, z), seen by a camera at height 0.9 looking straight down.
     floor_normal: the floor's vertex normal; normal_plug: the floor group's
     nodeNormal.  blocker_alpha: a black 6 x 6 sheet at height 1, between
     the floor and the light and above the camera, with a constant alpha map
-    of this value (None: no sheet)."""
+    of this value (None: no sheet).  floor_mat / light_mat: functions
+    (ctx, make) -> material replacing the white Matte / the emitter, where
+    make(type, **spectra) creates a material with linear Rec.709 spectra."""
     from vlr_b200 import vlr as VV
     lin = "Rec709(D65)"
     keep = []
@@ -632,12 +635,13 @@ def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=
     uvs = [(0, 0), (0, 1), (1, 1), (1, 0)]
     fn = np.asarray(floor_normal, np.float64)
     fn = tuple(fn / np.linalg.norm(fn))
+    fm = floor_mat(ctx, mat) if floor_mat else mat("Matte", albedo=(0.8, 0.8, 0.8))
     scene.add_child(quad("floor", [(-2, 0, -2), (-2, 0, 2), (2, 0, 2), (2, 0, -2)], fn, (1, 0, 0), uvs,
-                         mat("Matte", albedo=(0.8, 0.8, 0.8)), normal=normal_plug))
+                         fm, normal=normal_plug))
     lx, lz = light_at
     scene.add_child(quad("light", [(lx - .5, 2, lz - .5), (lx + .5, 2, lz - .5), (lx + .5, 2, lz + .5),
                                    (lx - .5, 2, lz + .5)], (0, -1, 0), (1, 0, 0), uvs,
-                         mat("DiffuseEmitter", emittance=(10.0, 10.0, 10.0))))
+                         light_mat(ctx, mat) if light_mat else mat("DiffuseEmitter", emittance=(10.0, 10.0, 10.0))))
     if blocker_alpha is not None:
         rgba = np.zeros((2, 2, 4), np.float32)
         rgba[..., 3] = blocker_alpha
@@ -656,7 +660,7 @@ def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=
     return scene, cam, keep
 
 
-def _floor_sum(renderer, spp, **kw):
+def _floor_sum(renderer, spp, with_albedo=False, **kw):
     from vlr_b200 import vlr as VV
     W = H = 48
     ctx = VV.Context()
@@ -664,12 +668,13 @@ def _floor_sum(renderer, spp, **kw):
     scene, cam, keep = _floor_scene(ctx, W, H, **kw)
     ctx.setScene(scene)
     ctx.setRenderer(renderer)
-    ctx.setOptions(max_path_length=4)
+    ctx.setOptions(max_path_length=4, aux_buffers=with_albedo)
     ctx.render_samples(cam, True, spp)
     y = _y_of(ctx.read_film())
+    albedo = ctx.read_aux()[0] if with_albedo else None
     ctx.close()
     assert np.isfinite(y).all()
-    return y.sum()
+    return (y.sum(), albedo) if with_albedo else y.sum()
 
 
 @pytest.mark.parametrize("renderer", ["path_tracing", "light_tracing", "bpt"])
@@ -949,3 +954,51 @@ def test_context_saves_png_and_exr(tmp_path):
     assert png[:8] == b"\x89PNG\r\n\x1a\n"
     assert len(exr) > W * H * 8
     assert out[..., :3].max() > 0.0
+
+
+def _multi(*parts):
+    """A Multi material of the given (type, spectra) parts."""
+    def make_multi(ctx, make):
+        m = ctx.createSurfaceMaterial("Multi")
+        for k, (typ, spectra) in enumerate(parts):
+            m.set(str(k), make(typ, **spectra))
+        return m
+    return make_multi
+
+
+@pytest.mark.parametrize("renderer", ["path_tracing", "light_tracing", "bpt"])
+def test_multi_material_sums_its_bsdfs(renderer):
+    """MultiBSDF (materials.cu:2255-2594) is the sum of its BSDFs: a Multi of
+    grey Mattes 0.3 and 0.4 (Meng spectra of one chromaticity scale with
+    brightness, so their sum is the 0.7 spectrum) shades like Matte 0.7 in
+    every renderer (here by choosing one component per hit with weight n),
+    and its guide albedo is the sum of the components' (getBaseColor,
+    :2307-2319)."""
+    from vlr_b200 import vlr as VV
+    r = {"path_tracing": VV.RENDERER_PATH_TRACING, "light_tracing": VV.RENDERER_LIGHT_TRACING,
+         "bpt": VV.RENDERER_BPT}[renderer]
+    spp = 1024
+    single, a1 = _floor_sum(r, spp, with_albedo=True, light_at=(0.6, 0.0),
+                            floor_mat=lambda ctx, make: make("Matte", albedo=(0.7, 0.7, 0.7)))
+    multi, a2 = _floor_sum(r, spp, with_albedo=True, light_at=(0.6, 0.0),
+                           floor_mat=_multi(("Matte", {"albedo": (0.3, 0.3, 0.3)}),
+                                            ("Matte", {"albedo": (0.4, 0.4, 0.4)})))
+    assert single > 0.0
+    assert abs(multi / single - 1) < 0.02, multi / single
+    assert np.allclose(a2[..., :3].mean(axis=(0, 1)), a1[..., :3].mean(axis=(0, 1)), rtol=0.01)
+
+
+@pytest.mark.parametrize("renderer", ["path_tracing", "bpt"])
+def test_multi_material_emits_the_sum_of_its_emitters(renderer):
+    """MultiEDF (materials.cu:2600-2823): a Multi of two diffuse emitters
+    lights the floor like one emitter with the summed emittance."""
+    from vlr_b200 import vlr as VV
+    r = {"path_tracing": VV.RENDERER_PATH_TRACING, "bpt": VV.RENDERER_BPT}[renderer]
+    spp = 512
+    single = _floor_sum(r, spp, light_at=(0.6, 0.0),
+                        light_mat=lambda ctx, make: make("DiffuseEmitter", emittance=(10.0, 10.0, 10.0)))
+    multi = _floor_sum(r, spp, light_at=(0.6, 0.0),
+                       light_mat=_multi(("DiffuseEmitter", {"emittance": (4.0, 4.0, 4.0)}),
+                                        ("DiffuseEmitter", {"emittance": (6.0, 6.0, 6.0)})))
+    assert single > 0.0
+    assert abs(multi / single - 1) < 0.02, multi / single

@@ -337,7 +337,10 @@ __global__ void __launch_bounds__(256) lightShadeKernel(BptArgs a) {
         float4 h = a.pb.hit[p];
         SurfPt sp;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, nullptr);
-        const uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
+        float bsdfScale = 1.0f;
+        uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
+        if (S.mats[mat].bsdfKind == kMultiBSDF)
+            mat = bsdfMaterial(S, mat, a.pb.rng[p], __float_as_uint(h.w), &bsdfScale);
         Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls, sp.tu, sp.tv);
         float4 o4 = a.pb.rayOrg[p], d4 = a.pb.rayDir[p];
         V3 dirInLocal = sp.frame.toLocal(-V3(d4.x, d4.y, d4.z));
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(256) lightShadeKernel(BptArgs a) {
         float lastDist2 = (V3(o4.x, o4.y, o4.z) - sp.position).sqLength();
         if (flags & kFlagOriginInf) lastDist2 = 1;
         float probDensity = a.pb.prevDirPDF[p] * absDot(dirInLocal, gnLocal) / lastDist2;
-        S4 alpha = toS4(a.pb.alpha[p]);
+        S4 alpha = toS4(a.pb.alpha[p]) * bsdfScale;   // a Multi material's component choice
         const uint32_t sampledType = a.pb.prevType[p];
         const float cosTermIn = a.ex.cosTerm[p];
         storeVertex(a, sp, mat, alpha, dirInLocal, cosTermIn / lastDist2, probDensity, prevProbDensity,
@@ -635,8 +638,13 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
         SurfPt sp;
         float hypAreaPDF;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, &hypAreaPDF);
-        const MatDesc &mat = S.mats[__ldg(S.triMaterial + __float_as_uint(h.w))];
-        Bsdf bsdfE = buildBsdf(S.meng, mat, wls, sp.tu, sp.tv);
+        const uint32_t matIndex = __ldg(S.triMaterial + __float_as_uint(h.w));
+        const MatDesc &mat = S.mats[matIndex];
+        float bsdfScale = 1.0f;
+        const uint32_t bsdfIndex = mat.bsdfKind == kMultiBSDF
+                                       ? bsdfMaterial(S, matIndex, a.pb.rng[p], __float_as_uint(h.w), &bsdfScale)
+                                       : matIndex;
+        Bsdf bsdfE = buildBsdf(S.meng, S.mats[bsdfIndex], wls, sp.tu, sp.tv);
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);
         V3 gnLocal = sp.frame.toLocal(sp.gn);
         BsdfQuery qE;
@@ -661,6 +669,7 @@ __global__ void __launch_bounds__(256) eyeShadeKernel(BptArgs a) {
             if (c.allFinite()) contrib += c;
         }
         a.pb.contrib[p] = toF4(contrib);
+        alpha *= bsdfScale;   // a Multi material's component choice (after the emission)
         PCG32 rng{ a.pb.rng[p] };
         // connection to one random cached light vertex (lvc_bpt.cu:672-803)
         if (bsdfHasNonDelta(bsdfE) && nCached > 0) {
@@ -990,7 +999,10 @@ __global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
         const float4 h = a.pb.hit[p];
         SurfPt sp;
         decodeHit(S, __float_as_uint(h.w), h.y, h.z, &sp, nullptr);
-        const uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
+        float bsdfScale = 1.0f;
+        uint32_t mat = __ldg(S.triMaterial + __float_as_uint(h.w));
+        if (S.mats[mat].bsdfKind == kMultiBSDF)
+            mat = bsdfMaterial(S, mat, a.pb.rng[p], __float_as_uint(h.w), &bsdfScale);
         const Bsdf bsdf = buildBsdf(S.meng, S.mats[mat], wls, sp.tu, sp.tv);
         const float4 d4 = a.pb.rayDir[p];
         BsdfQuery q;
@@ -999,7 +1011,7 @@ __global__ void __launch_bounds__(256) ltShadeKernel(BptArgs a) {
         q.filter = dir::All;
         q.importanceMode = 1;
         const V3 gnLocal = sp.frame.toLocal(sp.gn);
-        S4 alpha = toS4(a.pb.alpha[p]);
+        S4 alpha = toS4(a.pb.alpha[p]) * bsdfScale;   // a Multi material's component choice
         PCG32 rng{ a.pb.rng[p] };
         if (bsdfHasNonDelta(bsdf)) {
             float lensPDF;

@@ -204,6 +204,7 @@ MatDesc describeMaterial(const SurfaceMaterial* m) {
     std::memset(&d, 0, sizeof(d));
     for (int32_t &k : d.table) k = -1;
     for (int32_t &k : d.tex) k = -1;
+    for (int32_t &k : d.sub) k = -1;
     d.bsdfKind = kNullBSDF;
     d.emitScale = 1.0f;
     const std::string t = lower(m->typeName);
@@ -304,7 +305,29 @@ uint32_t materialIndex(FlatScene &f, const SurfaceMaterial* m) {
         if (f.matObjs[i] == m) return static_cast<uint32_t>(i);
     f.matObjs.push_back(m);
     f.mats.push_back(describeMaterial(m));
-    return static_cast<uint32_t>(f.mats.size() - 1);
+    const uint32_t index = static_cast<uint32_t>(f.mats.size() - 1);
+    if (lower(m->typeName) == "multi") {
+        // MultiSurfaceMaterial::setupMaterialDescriptor (materials.cpp:2098-2113)
+        // keeps the set sub-materials in order.  Here the BSDF-bearing ones
+        // (not nested Multis) become sub[]; the diffuse emitters' emittance
+        // is summed into this material's emission when the tables are built.
+        uint32_t n = 0;
+        bool emits = false;
+        for (const char* k : { "0", "1", "2", "3" }) {
+            auto it = m->objects.find(k);
+            if (it == m->objects.end() || !it->second) continue;
+            const auto* sub = static_cast<const SurfaceMaterial*>(it->second);
+            if (sub == m || lower(sub->typeName) == "multi") continue;
+            const uint32_t si = materialIndex(f, sub);
+            if (f.mats[si].emitter == kEmitDiffuse) emits = true;
+            if (f.mats[si].bsdfKind != kNullBSDF) f.mats[index].sub[n++] = static_cast<int32_t>(si);
+        }
+        f.mats[index].numSub = n;
+        f.mats[index].bsdfKind = n > 0 ? kMultiBSDF : kNullBSDF;
+        f.mats[index].emitter = emits ? kEmitDiffuse : kEmitNone;
+        f.mats[index].emitScale = 1.0f;
+    }
+    return index;
 }
 
 void flattenNode(FlatScene &f, const Node* n, const float world[16], const float worldInv[16]) {
@@ -677,6 +700,22 @@ void Context::buildScene(cudaStream_t stream) {
                 mengBlend(hostT, k < 3 ? f.mats[i].sp[k] : f.mats[i].emit, blended.data() + (i * 4 + k) * kMengSamples);
                 f.mats[i].table[k] = static_cast<int32_t>(i * 4 + k);
             }
+        // A Multi material emits the sum of its diffuse emitters' scaled
+        // emittance (MultiEDF::evaluateEmittanceInternal, materials.cu:2700-2715).
+        for (size_t i = 0; i < f.mats.size(); ++i) {
+            if (lower(f.matObjs[i]->typeName) != "multi") continue;
+            float* dst = blended.data() + (i * 4 + 3) * kMengSamples;
+            std::fill(dst, dst + kMengSamples, 0.0f);
+            for (const char* k : { "0", "1", "2", "3" }) {
+                auto it = f.matObjs[i]->objects.find(k);
+                if (it == f.matObjs[i]->objects.end() || !it->second) continue;
+                for (size_t j = 0; j < f.matObjs.size(); ++j) {
+                    if (f.matObjs[j] != it->second || j == i || f.mats[j].emitter != kEmitDiffuse) continue;
+                    const float* src = blended.data() + (j * 4 + 3) * kMengSamples;
+                    for (uint32_t w = 0; w < kMengSamples; ++w) dst[w] += f.mats[j].emitScale * src[w];
+                }
+            }
+        }
         sg.meng.blended = upload(blended, stream);
     }
     sg.mats = upload(f.mats, stream);

@@ -88,14 +88,21 @@ __global__ void __launch_bounds__(256) auxKernel(AuxArgs a) {
             SurfPt sp;
             decodeHit(S, h.prim, h.b1, h.b2, &sp, nullptr);
             const MatDesc &m = S.mats[__ldg(S.triMaterial + h.prim)];
+            const uint32_t parts = m.bsdfKind == kMultiBSDF ? m.numSub : 1u;
             // four wavelength sets at offsets (j + wo) / 4: 16 stratified
             // wavelengths per sample, so the guide is nearly free of
             // spectral noise after a few samples
             for (int j = 0; j < 4; ++j) {
                 float selectWLPDF;
                 const WLS wls = WLS::equalOffsets((j + wo) * 0.25f, ws, &selectWLPDF);
-                const Bsdf B = buildBsdf(S.meng, m, wls, sp.tu, sp.tv);
-                const S4 v = baseColor(B) * mengEvaluate(S.meng, a.white, wls) / (4.0f * selectWLPDF);
+                // a Multi material's base colour is the sum of its components'
+                // (MultiBSDF::getBaseColor, materials.cu:2307-2319)
+                S4 base = S4::zero();
+                for (uint32_t c = 0; c < parts; ++c) {
+                    const MatDesc &mc = m.bsdfKind == kMultiBSDF ? S.mats[m.sub[c]] : m;
+                    base += baseColor(buildBsdf(S.meng, mc, wls, sp.tu, sp.tv));
+                }
+                const S4 v = base * mengEvaluate(S.meng, a.white, wls) / (4.0f * selectWLPDF);
                 const float lam[4] = { wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3] };
                 filmAdd(a.ab.albedo + fi * kNumStrata, lam, v);
             }

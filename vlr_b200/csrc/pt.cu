@@ -108,8 +108,14 @@ __global__ void __launch_bounds__(256) traceKernel(SceneGPU S, PathBuffers pb, F
         Hit h = traceClosest(S, V3(o.x, o.y, o.z), V3(d.x, d.y, d.z), o.w, S.hasAlphaMaps ? pb.rng[p] : 0ull);
         pb.hit[p] = make_float4(h.t, h.b1, h.b2, __uint_as_float(h.prim));
         uint32_t key = kNumBsdfKinds;
-        if (h.prim != 0xFFFFFFFFu)
-            key = S.mats[__ldg(S.triMaterial + h.prim)].bsdfKind;
+        if (h.prim != 0xFFFFFFFFu) {
+            const uint32_t mi = __ldg(S.triMaterial + h.prim);
+            key = S.mats[mi].bsdfKind;
+            if (key == kMultiBSDF) {
+                float scale;
+                key = S.mats[bsdfMaterial(S, mi, pb.rng[p], h.prim, &scale)].bsdfKind;
+            }
+        }
         uint32_t slot = appendSlot(ctr + kCntBucket0 + key, key);
         pb.buckets[key * P + slot] = p;
     }
@@ -229,8 +235,12 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         SurfPt sp;
         float hypAreaPDF;
         decodeHit<kMaps>(S, prim, h.y, h.z, &sp, &hypAreaPDF);
-        const MatDesc &mat = S.mats[__ldg(S.triMaterial + prim)];
-        Bsdf bsdf = buildBsdf(S.meng, mat, wls, sp.tu, sp.tv);
+        const uint32_t matIndex = __ldg(S.triMaterial + prim);
+        const MatDesc &mat = S.mats[matIndex];
+        float bsdfScale = 1.0f;
+        const uint32_t bsdfIndex =
+            mat.bsdfKind == kMultiBSDF ? bsdfMaterial(S, matIndex, pb.rng[p], prim, &bsdfScale) : matIndex;
+        Bsdf bsdf = buildBsdf(S.meng, S.mats[bsdfIndex], wls, sp.tu, sp.tv);
         float4 o4 = pb.rayOrg[p], d4 = pb.rayDir[p];
         V3 rayOrg(o4.x, o4.y, o4.z), rayDir(d4.x, d4.y, d4.z);
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);
@@ -249,6 +259,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
             }
             contrib += alpha * Le * MIS;
         }
+        alpha *= bsdfScale;   // a Multi material's component choice (after the emission)
         // The record of the previous vertex closes after this vertex's
         // emission: light reached directly from there is NEE's job, and the
         // network learns the indirect light NEE cannot sample.

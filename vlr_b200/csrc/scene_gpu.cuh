@@ -27,7 +27,13 @@ struct MatDesc {
     int32_t table[4] = { -1, -1, -1, -1 };   // sp[0..2], emit: index of the blended spectrum
                                              // in MengTables::blended (-1: evaluate the UpSpec)
     int32_t tex[3] = { -1, -1, -1 };         // sp[0..2]: Image2DTexture index (-1: none)
+    int32_t sub[4] = { -1, -1, -1, -1 };     // Multi: the non-emitting sub-materials' indices
+    uint32_t numSub = 0;
 };
+
+// MatDesc::bsdfKind of a Multi material: outside the BSDF kinds, so nothing
+// shades it directly; hits resolve it to one of its sub-materials first.
+constexpr uint32_t kMultiBSDF = 0x100u;
 
 // Bump types of Image2DTexture (shared/shared.h:147-151).
 enum BumpKind : uint32_t { kBumpNormalDirectX = 0, kBumpNormalOpenGL = 1, kBumpHeight = 2 };
@@ -405,6 +411,25 @@ __device__ __forceinline__ float shadowVisibility(const SceneGPU &S, const V3 &o
     AlphaVisibility av{ &S, 1.0f };
     const Hit h = traceBvhWith<true>(S.bvh, org, dir, tmax, av);
     return h.prim == 0xFFFFFFFFu ? av.visibility : 0.0f;
+}
+
+// The material whose BSDF shades a hit on triangle `prim` of material `mat`.
+// A Multi material (MultiBSDF, materials.cu:2255-2594, the sum of up to four
+// BSDFs) picks one of its n sub-BSDFs uniformly and reports scale n: the
+// path's throughput times n x f_i is an unbiased estimate of the sum, the
+// sub-BSDF's own pdfs serve its sampling and MIS, and a hit's emission (the
+// sum of the sub-emitters) is not scaled.  The choice is a function of the
+// path's RNG state (not yet advanced between trace and shade) and the
+// primitive, so the trace kernel's material sort and the shader agree.
+__device__ __forceinline__ uint32_t bsdfMaterial(const SceneGPU &S, uint32_t mat, uint64_t rngState, uint32_t prim,
+                                                 float* scale) {
+    *scale = 1.0f;
+    const MatDesc &m = S.mats[mat];
+    if (m.bsdfKind != kMultiBSDF) return mat;
+    const uint32_t n = m.numSub;
+    const uint32_t i = min(static_cast<uint32_t>(hashUniform(rngState + 0x632BE59BD9B4E019ULL, prim) * n), n - 1);
+    *scale = static_cast<float>(n);
+    return static_cast<uint32_t>(m.sub[i]);
 }
 
 // Closest hit of a path's ray, alpha-tested with the path's RNG state.

@@ -188,8 +188,12 @@ bool initMaterial(SurfaceMaterial* m, const std::string &type) {
         m->floats["scale"] = { 1.0f };
         m->floats["direction"] = { 0.0f, 0.0f, 1.0f };
     }
+    else if (t == "multi") {
+        // MultiSurfaceMaterial (materials.cpp:2055-2160): up to four sub-materials "0".."3"
+        for (const char* k : { "0", "1", "2", "3" }) m->addParam(k, kNode, "SurfaceMaterial");
+    }
     else {
-        // OldStyle, Multi: not rendered here.
+        // OldStyle: not rendered here.
         return false;
     }
     return true;
@@ -683,6 +687,10 @@ VLRResult vlrQueryableSetImmediateSpectrum(VLRQueryable queryable, const char* p
 VLRResult vlrQueryableSetSurfaceMaterial(VLRQueryable queryable, const char* paramName, VLRSurfaceMaterialConst value) {
     CHECK_HANDLE(q, Queryable, isQueryable, queryable);
     if (!paramName || !paramOf(q, paramName, "SurfaceMaterial")) return VLRResult_InvalidArgument;
+    if (value) {
+        VLRResult e2 = VLRResult_NoError;
+        if (!checked<const Object>(value, &e2, kindMaterial)) return e2;
+    }
     q->objects[lower(paramName)] = reinterpret_cast<const Object*>(value);
     touch(q);
     return VLRResult_NoError;

@@ -101,6 +101,7 @@ def _api():
         "vlrQueryableSetPoint3D": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 3)],
         "vlrQueryableSetQuaternion": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float * 4)],
         "vlrQueryableSetImage2D": [v, ctypes.c_char_p, v],
+        "vlrQueryableSetSurfaceMaterial": [v, ctypes.c_char_p, v],
         "vlrQueryableSetShaderNodePlug": [v, ctypes.c_char_p, VLRShaderNodePlug],
         "vlrQueryableGetFloat": [v, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)],
         "vlrQueryableGetNumParameters": [v, ctypes.POINTER(ctypes.c_uint32)],
@@ -169,6 +170,8 @@ class Queryable:
             check(L.vlrQueryableSetShaderNodePlug(self.h, n, value.plug), f"set {name}")
         elif isinstance(value, Image):
             check(L.vlrQueryableSetImage2D(self.h, n, value.h), f"set {name}")
+        elif isinstance(value, SurfaceMaterial):
+            check(L.vlrQueryableSetSurfaceMaterial(self.h, n, value.h), f"set {name}")
         elif isinstance(value, (int, float)):
             check(L.vlrQueryableSetFloat(self.h, n, float(value)), f"set {name}")
         else:
@@ -211,6 +214,10 @@ class Image:
     def __init__(self, handle, keep):
         self.h = handle
         self._keep = keep
+
+
+class SurfaceMaterial(Queryable):
+    """A surface material; also the value of a Multi material's "0".."3"."""
 
 
 class ShaderNode(Queryable):
@@ -335,7 +342,7 @@ class Context:
         return PointSet(self, self._new("vlrPointSurfaceNodeCreate", name.encode()))
 
     def createSurfaceMaterial(self, type_name):
-        return Queryable(self, self._new("vlrSurfaceMaterialCreate", type_name.encode()))
+        return SurfaceMaterial(self, self._new("vlrSurfaceMaterialCreate", type_name.encode()))
 
     def createShaderNode(self, type_name):
         return ShaderNode(self, self._new("vlrShaderNodeCreate", type_name.encode()))
