@@ -1002,3 +1002,48 @@ def test_multi_material_emits_the_sum_of_its_emitters(renderer):
                                         ("DiffuseEmitter", {"emittance": (6.0, 6.0, 6.0)})))
     assert single > 0.0
     assert abs(multi / single - 1) < 0.02, multi / single
+
+
+def _scalar_material(typ, spectra, floats, plug_param=None, texel=None):
+    """floor_mat for _floor_scene: `typ` with linear spectra and float
+    immediates, or (texel given) its float3 plug `plug_param` fed by a
+    constant 2 x 2 Image2DTexture holding texel in RGB."""
+    from vlr_b200 import vlr as VV
+
+    def make_mat(ctx, make):
+        m = make(typ, **spectra)
+        for k, v in floats.items():
+            m.set(k, v)
+        if texel is not None:
+            rgba = np.ones((2, 2, 4), np.float32)
+            rgba[..., :3] = texel
+            img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
+            tex = ctx.createShaderNode("Image2DTexture")
+            tex.set("image", img)
+            m.set(plug_param, tex.plug(VV.PLUG_FLOAT3, 0))
+        return m
+    return make_mat
+
+
+@pytest.mark.parametrize("case", ["ue4", "microfacet"])
+def test_float3_texture_drives_the_scalar_parameters(case):
+    """A constant texture on UE4's occlusion/roughness/metallic or a
+    microfacet material's roughness/anisotropy/rotation (float3 plugs,
+    materials.cu:1521-1533, 1964-1969) shades like the same immediates; the
+    immediates themselves differ visibly from the material's defaults."""
+    from vlr_b200 import vlr as VV
+    if case == "ue4":
+        typ, spectra = "UE4", {"base color": (0.6, 0.5, 0.4)}
+        vals, plug, texel = {"roughness": 0.2, "metallic": 0.7}, "occlusion/roughness/metallic", (1.0, 0.2, 0.7)
+    else:
+        typ, spectra = "MicrofacetReflection", {"eta": (0.2, 0.4, 1.4), "k": (3.9, 2.4, 1.8)}
+        vals, plug, texel = {"roughness": 0.25, "anisotropy": 0.6, "rotation": 0.1}, "roughness/anisotropy/rotation", \
+            (0.25, 0.6, 0.1)
+    spp = 512
+    kw = dict(light_at=(0.6, 0.0))
+    imm = _floor_sum(VV.RENDERER_PATH_TRACING, spp, floor_mat=_scalar_material(typ, spectra, vals), **kw)
+    tex = _floor_sum(VV.RENDERER_PATH_TRACING, spp, floor_mat=_scalar_material(typ, spectra, {}, plug, texel), **kw)
+    dflt = _floor_sum(VV.RENDERER_PATH_TRACING, spp, floor_mat=_scalar_material(typ, spectra, {}), **kw)
+    assert imm > 0.0
+    assert abs(tex / imm - 1) < 1e-3, tex / imm
+    assert abs(dflt / imm - 1) > 0.02, dflt / imm

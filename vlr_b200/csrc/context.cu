@@ -205,6 +205,7 @@ MatDesc describeMaterial(const SurfaceMaterial* m) {
     for (int32_t &k : d.table) k = -1;
     for (int32_t &k : d.tex) k = -1;
     for (int32_t &k : d.sub) k = -1;
+    d.texF = -1;
     d.bsdfKind = kNullBSDF;
     d.emitScale = 1.0f;
     const std::string t = lower(m->typeName);
@@ -648,6 +649,21 @@ void Context::buildScene(cudaStream_t stream) {
                 const int32_t t = textureOf(pl->second, false, nullptr);
                 if (t >= 0) f.mats[i].tex[ps.second] = t;
             }
+        }
+        // float3 plugs of the scalar parameters
+        for (size_t i = 0; i < f.matObjs.size() && i < f.mats.size(); ++i) {
+            const std::string t = lower(f.matObjs[i]->typeName);
+            const char* param = t == "ue4" ? "occlusion/roughness/metallic"
+                                : (t == "microfacetreflection" || t == "microfacetscattering")
+                                    ? "roughness/anisotropy/rotation" : nullptr;
+            if (!param) continue;
+            auto pl = f.matObjs[i]->plugs.find(param);
+            if (pl == f.matObjs[i]->plugs.end() || (pl->second.info & 0xFFu) != VLRShaderNodePlugType_float3) continue;
+            const int32_t tx = textureOf(pl->second, false, nullptr);
+            if (tx < 0) continue;
+            f.mats[i].texF = tx;
+            sg.hasScalarTextures = 1;
+            f.mats[i].texFOpt = ((pl->second.info >> 8) & 0xFFu) == 1 ? 1u : 0u;
         }
         std::vector<GeomMaps> maps(f.geomInstMaterial.size() + 1);
         bool anyMap = false;

@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         float bsdfScale = 1.0f;
         const uint32_t bsdfIndex =
             mat.bsdfKind == kMultiBSDF ? bsdfMaterial(S, matIndex, pb.rng[p], prim, &bsdfScale) : matIndex;
-        Bsdf bsdf = buildBsdf(S.meng, S.mats[bsdfIndex], wls, sp.tu, sp.tv);
+        Bsdf bsdf = buildBsdf<-1, kMaps>(S.meng, S.mats[bsdfIndex], wls, sp.tu, sp.tv);
         float4 o4 = pb.rayOrg[p], d4 = pb.rayDir[p];
         V3 rayOrg(o4.x, o4.y, o4.z), rayDir(d4.x, d4.y, d4.z);
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);
@@ -792,7 +792,8 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
             T.end(stream);
         }
         T.begin(kStageShade, stream, pMain + (guiding ? sizeof(GuideFrame) : 0));
-        const bool maps = scene.geomMaps != nullptr;
+        // the kMaps variants: normal maps, and float3 textures on scalar parameters
+        const bool maps = scene.geomMaps != nullptr || scene.hasScalarTextures != 0;
         if (guiding && maps) shadeKernel<true, true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
         else if (guiding) shadeKernel<true, false><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
         else if (maps) shadeKernel<false, true><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});

@@ -29,6 +29,9 @@ struct MatDesc {
     int32_t tex[3] = { -1, -1, -1 };         // sp[0..2]: Image2DTexture index (-1: none)
     int32_t sub[4] = { -1, -1, -1, -1 };     // Multi: the non-emitting sub-materials' indices
     uint32_t numSub = 0;
+    int32_t texF = -1;      // float3 plug texture: roughness/anisotropy/rotation (microfacet) or
+                            // occlusion/roughness/metallic (UE4); -1: the immediate f[]
+    uint32_t texFOpt = 0;   // plug option: 0 the texel's xyz, 1 its yzw
 };
 
 // MatDesc::bsdfKind of a Multi material: outside the BSDF kinds, so nothing
@@ -198,6 +201,7 @@ struct SceneGPU {
     const MatDesc* mats;
     const GeomMaps* geomMaps;       // [numGeomInsts], null when no group has a normal or alpha map
     uint32_t hasAlphaMaps;          // some group has an alpha map: traversal runs the alpha test
+    uint32_t hasScalarTextures;     // some material has a float3 texture plug (MatDesc::texF)
     // lights
     Dist1D lightInsts;              // over light instances (env first if present)
     const uint32_t* instFirstGroup; // per light instance
@@ -236,13 +240,35 @@ struct SurfPt {
 // callables of materials.cu with immediate values).
 // K >= 0: the material is known to be of that kind (the shade kernels
 // specialised per material queue), which lets every BSDF dispatch fold.
-template <int K = -1>
+// kScalarTextures false: the caller knows no material has a float3 texture
+// plug (a hit shader compiled without that read keeps its registers).
+template <int K = -1, bool kScalarTextures = true>
 VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls, float tu = 0.0f, float tv = 0.0f) {
     Bsdf B;
     const uint32_t kind = K >= 0 ? static_cast<uint32_t>(K) : m.bsdfKind;
     B.kind = kind;
     B.flags = 0;
     B.f0 = m.f[0]; B.f1 = m.f[1]; B.f2 = m.f[2];
+    float metallic = m.f[1];
+#if defined(__CUDA_ARCH__)
+    if (kScalarTextures && T.textures && m.texF >= 0) {
+        // the float3 plug's texel (Image2DTextureShaderNode_float3,
+        // shader_nodes.cu:320-334), turned into the BSDF's scalars as the
+        // setupBSDF programs do (materials.cu:1521-1533, 1964-1969)
+        const float4 c = tex2DLod<float4>(T.textures[m.texF], tu, tv, 0.0f);
+        const float x = m.texFOpt == 0 ? c.x : c.y, y = m.texFOpt == 0 ? c.y : c.z, z = m.texFOpt == 0 ? c.z : c.w;
+        if (kind == kUE4) {
+            B.f0 = fmaxf(0.01f, y);
+            metallic = z;
+        }
+        else {
+            const float alpha = x * x, aspect = sqrtf(1 - 0.9f * y);
+            B.f0 = fmaxf(0.001f, alpha / aspect);
+            B.f1 = fmaxf(0.001f, alpha * aspect);
+            B.f2 = 2 * kPi * z;
+        }
+    }
+#endif
     switch (kind) {
     case kMatte:
     case kLambertianBSDF:
@@ -264,11 +290,9 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls, fl
     case kUE4: {
         // UE4SurfaceMaterial_setupBSDF (materials.cu:1959-1978); f[1] = metallic.
         S4 base = matSpectrum(T, m, 0, wls, tu, tv);
-        const float metallic = m.f[1];
         const float specular = 0.5f;
         B.a = base * (1 - metallic);
         B.b = lerpS(0.08f * specular * S4::one(), base, metallic);
-        B.f0 = m.f[0];
         break;
     }
     default:
