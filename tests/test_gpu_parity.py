@@ -1016,16 +1016,16 @@ def _scalar_material(typ, spectra, floats, plug_param=None, texel=None):
             m.set(k, v)
         if texel is not None:
             rgba = np.ones((2, 2, 4), np.float32)
-            rgba[..., :3] = texel
+            rgba[..., :len(texel)] = texel
             img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
             tex = ctx.createShaderNode("Image2DTexture")
             tex.set("image", img)
-            m.set(plug_param, tex.plug(VV.PLUG_FLOAT3, 0))
+            m.set(plug_param, tex.plug(VV.PLUG_FLOAT1 if len(texel) == 1 else VV.PLUG_FLOAT3, 0))
         return m
     return make_mat
 
 
-@pytest.mark.parametrize("case", ["ue4", "microfacet"])
+@pytest.mark.parametrize("case", ["ue4", "microfacet", "lambertian_f0"])
 def test_float3_texture_drives_the_scalar_parameters(case):
     """A constant texture on UE4's occlusion/roughness/metallic or a
     microfacet material's roughness/anisotropy/rotation (float3 plugs,
@@ -1035,6 +1035,9 @@ def test_float3_texture_drives_the_scalar_parameters(case):
     if case == "ue4":
         typ, spectra = "UE4", {"base color": (0.6, 0.5, 0.4)}
         vals, plug, texel = {"roughness": 0.2, "metallic": 0.7}, "occlusion/roughness/metallic", (1.0, 0.2, 0.7)
+    elif case == "lambertian_f0":
+        typ, spectra = "LambertianScattering", {"coeff": (0.7, 0.7, 0.7)}
+        vals, plug, texel = {"f0": 0.5}, "f0", (0.5,)
     else:
         typ, spectra = "MicrofacetReflection", {"eta": (0.2, 0.4, 1.4), "k": (3.9, 2.4, 1.8)}
         vals, plug, texel = {"roughness": 0.25, "anisotropy": 0.6, "rotation": 0.1}, "roughness/anisotropy/rotation", \

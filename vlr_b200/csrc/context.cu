@@ -653,17 +653,21 @@ void Context::buildScene(cudaStream_t stream) {
         // float3 plugs of the scalar parameters
         for (size_t i = 0; i < f.matObjs.size() && i < f.mats.size(); ++i) {
             const std::string t = lower(f.matObjs[i]->typeName);
+            const bool lambert = t == "lambertianscattering";
             const char* param = t == "ue4" ? "occlusion/roughness/metallic"
                                 : (t == "microfacetreflection" || t == "microfacetscattering")
-                                    ? "roughness/anisotropy/rotation" : nullptr;
+                                    ? "roughness/anisotropy/rotation"
+                                : lambert ? "f0" : nullptr;
             if (!param) continue;
             auto pl = f.matObjs[i]->plugs.find(param);
-            if (pl == f.matObjs[i]->plugs.end() || (pl->second.info & 0xFFu) != VLRShaderNodePlugType_float3) continue;
+            const uint32_t want = lambert ? VLRShaderNodePlugType_float1 : VLRShaderNodePlugType_float3;
+            if (pl == f.matObjs[i]->plugs.end() || (pl->second.info & 0xFFu) != want) continue;
             const int32_t tx = textureOf(pl->second, false, nullptr);
             if (tx < 0) continue;
+            const uint32_t option = (pl->second.info >> 8) & 0xFFu;
             f.mats[i].texF = tx;
+            f.mats[i].texFOpt = lambert ? std::min<uint32_t>(option, 3u) << 8 : (option == 1 ? 1u : 0u);
             sg.hasScalarTextures = 1;
-            f.mats[i].texFOpt = ((pl->second.info >> 8) & 0xFFu) == 1 ? 1u : 0u;
         }
         std::vector<GeomMaps> maps(f.geomInstMaterial.size() + 1);
         bool anyMap = false;

@@ -31,7 +31,8 @@ struct MatDesc {
     uint32_t numSub = 0;
     int32_t texF = -1;      // float3 plug texture: roughness/anisotropy/rotation (microfacet) or
                             // occlusion/roughness/metallic (UE4); -1: the immediate f[]
-    uint32_t texFOpt = 0;   // plug option: 0 the texel's xyz, 1 its yzw
+    uint32_t texFOpt = 0;   // plug option: 0 the texel's xyz, 1 its yzw; LambertianScattering's
+                            // "f0" (a float1 plug): the channel << 8
 };
 
 // MatDesc::bsdfKind of a Multi material: outside the BSDF kinds, so nothing
@@ -257,7 +258,12 @@ VLRB_HD Bsdf buildBsdf(const MengTables &T, const MatDesc &m, const WLS &wls, fl
         // setupBSDF programs do (materials.cu:1521-1533, 1964-1969)
         const float4 c = tex2DLod<float4>(T.textures[m.texF], tu, tv, 0.0f);
         const float x = m.texFOpt == 0 ? c.x : c.y, y = m.texFOpt == 0 ? c.y : c.z, z = m.texFOpt == 0 ? c.z : c.w;
-        if (kind == kUE4) {
+        if (kind == kLambertianBSDF) {
+            // "f0", a float1 plug: the option's channel (shader_nodes.cu:284-301)
+            const uint32_t o = m.texFOpt >> 8;
+            B.f0 = o == 0 ? c.x : o == 1 ? c.y : o == 2 ? c.z : c.w;
+        }
+        else if (kind == kUE4) {
             B.f0 = fmaxf(0.01f, y);
             metallic = z;
         }

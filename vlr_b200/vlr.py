@@ -68,6 +68,7 @@ class VLRBBatchItem(ctypes.Structure):
 RENDERER_PATH_TRACING = 0
 RENDERER_LIGHT_TRACING = 1
 RENDERER_BPT = 2
+PLUG_FLOAT1 = 0
 PLUG_FLOAT3 = 2
 PLUG_NORMAL3D = 6
 PLUG_SPECTRUM = 7
