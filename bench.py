@@ -448,6 +448,40 @@ def light_tracing_workload():
     return out
 
 
+def denoise_workload():
+    """vlrContextRender at 1920x1080 on the Cornell box, one sample per call,
+    without and with denoise: the difference per call is the post-processing
+    (guide sample: a camera ray, hit decode and base colour per pixel; guide
+    conversion; demodulation, five a-trous passes, remodulation).
+    Device-timed with CUDA events over 16 calls each."""
+    import torch
+    from vlr_b200 import vlr as V, scenes
+    w, h, calls = 1920, 1080, 16
+    ctx = V.Context()
+    ctx.bindOutputBuffer(w, h)
+    scene, cam, keep = scenes.build(ctx, scenes.cornell_box_desc(w, h))
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=MAX_PATH_LENGTH)
+    stream = torch.cuda.current_stream()
+    times = {}
+    for denoise in (False, True, False, True):      # the first pair warms up
+        ctx.render(cam, True, stream=stream.cuda_stream, denoise=denoise)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(calls):
+            ctx.render(cam, False, stream=stream.cuda_stream, denoise=denoise)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times[denoise] = e0.elapsed_time(e1) / calls
+    ctx.close()
+    post = times[True] - times[False]
+    return {"workload": f"denoise: Cornell box {w}x{h}, vlrContextRender 1 spp per call, max path length "
+                        f"{MAX_PATH_LENGTH}, with and without denoise = true",
+            "render_ms_per_call": times[False], "render_and_denoise_ms_per_call": times[True],
+            "post_ms_per_call": post, "post_mpixels_per_s": w * h / (post * 1e-3) / 1e6 if post > 0 else None}
+
+
 WORKLOADS = {
     "bsdf_batch": lambda: {"bsdf_batch": bsdf_batch_workload(measured_peaks()[0])},
     "terrain_pt": lambda: terrain_workloads(("terrain_pt",)),
@@ -455,6 +489,7 @@ WORKLOADS = {
     "multi_scene_batch": lambda: {"multi_scene_batch": batch_workload()},
     "glossy_guided": lambda: {"glossy_guided": glossy_guided_workload()},
     "light_tracing": lambda: {"light_tracing": light_tracing_workload()},
+    "denoise": lambda: {"denoise": denoise_workload()},
 }
 
 
@@ -695,7 +730,8 @@ def main():
         workloads = {}
         for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads,
                    lambda: {"multi_scene_batch": batch_workload()},
-                   lambda: {"light_tracing": light_tracing_workload()}):
+                   lambda: {"light_tracing": light_tracing_workload()},
+                   lambda: {"denoise": denoise_workload()}):
             try:
                 workloads.update(fn())
             except Exception as ex:  # reported, never fatal for the GPU line
