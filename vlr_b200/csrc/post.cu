@@ -3,6 +3,8 @@
 #include "tables.cuh"
 #include "wavefront.cuh"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <stdexcept>
 
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(256) auxLinearKernel(LinearArgs a) {
 // ---------------------------------------------------------------- denoiser
 constexpr float kAlbedoEps = 1e-3f;
 constexpr float kSigmaLuminance = 4.0f;
-constexpr float kSigmaNormal = 128.0f;     // exponent of the normal term
+// exponent of the normal term: 128 = 2^7 (computed by squaring)
 constexpr float kSigmaAlbedo2 = 0.02f;     // 2 x (0.1)^2
 constexpr int kWaveletPasses = 5;
 
@@ -160,8 +162,21 @@ struct DenoiseArgs {
     const float4* color;
     const float4* albedo;
     const float4* normal;
+    uint4* guide;
     uint32_t width, height, stride;
 };
+
+__device__ __forceinline__ uint32_t packHalf2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    uint32_t u;
+    memcpy(&u, &h, 4);
+    return u;
+}
+__device__ __forceinline__ float2 unpackHalf2(uint32_t u) {
+    __half2 h;
+    memcpy(&h, &u, 4);
+    return __half22float2(h);
+}
 
 __device__ __forceinline__ bool isGuided(const float4 &a) {
     return a.x + a.y + a.z > kAlbedoEps;
@@ -178,6 +193,11 @@ __global__ void demodulateKernel(DenoiseArgs a, float4* illum) {
     if (x >= static_cast<int>(a.width) || y >= static_cast<int>(a.height)) return;
     const size_t p = static_cast<size_t>(y) * a.stride + x;
     const float4 ap = a.albedo[p];
+    // the taps' guide record: albedo rgb, normal xyz as halves; albedo r
+    // negative marks a pixel that is not filtered
+    const float4 np = a.normal[p];
+    a.guide[p] = make_uint4(packHalf2(isGuided(ap) ? ap.x : -1.0f, ap.y), packHalf2(ap.z, np.x),
+                            packHalf2(np.y, np.z), 0u);
     if (!isGuided(ap)) { illum[p] = make_float4(0.f, 0.f, 0.f, 0.f); return; }
     float sum = 0.0f, sum2 = 0.0f, cnt = 0.0f;
     float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -210,12 +230,14 @@ __global__ void __launch_bounds__(256) waveletKernel(DenoiseArgs a, const float4
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= static_cast<int>(a.width) || y >= static_cast<int>(a.height)) return;
     const size_t p = static_cast<size_t>(y) * a.stride + x;
-    const float4 ap = a.albedo[p];
+    const uint4 gp = a.guide[p];
     const float4 ip = in[p];
-    if (!isGuided(ap)) { out[p] = ip; return; }
-    const float4 np = a.normal[p];
+    const float2 g0 = unpackHalf2(gp.x), g1 = unpackHalf2(gp.y), g2 = unpackHalf2(gp.z);
+    if (g0.x < 0.0f) { out[p] = ip; return; }
+    const float4 ap = make_float4(g0.x, g0.y, g1.x, 0.0f);
+    const float4 np = make_float4(g1.y, g2.x, g2.y, 0.0f);
     const float lp = luminance(ip);
-    const float sigmaL = kSigmaLuminance * sqrtf(ip.w) + 1e-6f;
+    const float recSigmaL = 1.0f / (kSigmaLuminance * sqrtf(ip.w) + 1e-6f);
     const float kernel[3] = { 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f };
     float sr = 0.f, sg = 0.f, sb = 0.f, wsum = 0.f, vsum = 0.f;
     for (int dy = -2; dy <= 2; ++dy)
@@ -223,16 +245,20 @@ __global__ void __launch_bounds__(256) waveletKernel(DenoiseArgs a, const float4
             const int qx = x + dx * step, qy = y + dy * step;
             if (qx < 0 || qy < 0 || qx >= static_cast<int>(a.width) || qy >= static_cast<int>(a.height)) continue;
             const size_t q = static_cast<size_t>(qy) * a.stride + qx;
-            const float4 aq = a.albedo[q];
-            if (!isGuided(aq)) continue;
+            const uint4 gq = a.guide[q];
+            const float2 h0 = unpackHalf2(gq.x), h1 = unpackHalf2(gq.y), h2 = unpackHalf2(gq.z);
+            if (h0.x < 0.0f) continue;
+            const float4 aq = make_float4(h0.x, h0.y, h1.x, 0.0f);
+            const float4 nq = make_float4(h1.y, h2.x, h2.y, 0.0f);
             const float4 iq = in[q];
-            const float4 nq = a.normal[q];
             const float h = kernel[dx < 0 ? -dx : dx] * kernel[dy < 0 ? -dy : dy];
-            const float wn = __powf(fmaxf(0.0f, np.x * nq.x + np.y * nq.y + np.z * nq.z), kSigmaNormal);
+            // normal term max(0, n.n')^128 by seven squarings; the albedo and
+            // luminance terms in one exponential (one special-function op a tap)
+            float wn = fmaxf(0.0f, np.x * nq.x + np.y * nq.y + np.z * nq.z);
+            for (int k = 0; k < 7; ++k) wn *= wn;
             const float da = sq(ap.x - aq.x) + sq(ap.y - aq.y) + sq(ap.z - aq.z);
-            const float wa = __expf(-da / kSigmaAlbedo2);
-            const float wl = __expf(-fabsf(lp - luminance(iq)) / sigmaL);
-            const float w = (dx == 0 && dy == 0) ? h : h * wn * wa * wl;
+            const float wal = __expf(-da * (1.0f / kSigmaAlbedo2) - fabsf(lp - luminance(iq)) * recSigmaL);
+            const float w = (dx == 0 && dy == 0) ? h : h * wn * wal;
             sr += w * iq.x; sg += w * iq.y; sb += w * iq.z;
             wsum += w;
             vsum += w * w * iq.w;
@@ -264,7 +290,7 @@ int numSMsOf() {
 
 size_t auxBufferBytes(uint32_t stride, uint32_t height) {
     const size_t px = static_cast<size_t>(stride) * height;
-    return align256(px * kNumStrata * sizeof(double)) + 6 * align256(px * sizeof(float4));
+    return align256(px * kNumStrata * sizeof(double)) + 7 * align256(px * sizeof(float4));
 }
 
 void carveAuxBuffers(void* base, uint32_t stride, uint32_t height, AuxBuffers* out) {
@@ -277,6 +303,7 @@ void carveAuxBuffers(void* base, uint32_t stride, uint32_t height, AuxBuffers* o
         *f = reinterpret_cast<float4*>(c);
         c += align256(px * sizeof(float4));
     }
+    out->guide = reinterpret_cast<uint4*>(c);
     out->stride = stride;
 }
 
@@ -329,7 +356,7 @@ void auxToLinear(const SceneGPU &scene, const AuxBuffers &ab, uint32_t width, ui
 
 void denoiseLaunch(const AuxBuffers &ab, float4* color, uint32_t width, uint32_t height, cudaStream_t stream) {
     if (width == 0 || height == 0) return;
-    DenoiseArgs a{ color, ab.linAlbedo, ab.linNormal, width, height, ab.stride };
+    DenoiseArgs a{ color, ab.linAlbedo, ab.linNormal, ab.guide, width, height, ab.stride };
     const dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
     demodulateKernel<<<grid, block, 0, stream>>>(a, ab.work[0]);
     const float4* in = ab.work[0];

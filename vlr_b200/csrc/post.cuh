@@ -25,6 +25,7 @@ struct AuxBuffers {
     float4* linAlbedo;    // [stride * height] Rec.709 albedo
     float4* linNormal;    // [stride * height] camera-space normal (x flipped, as the reference)
     float4* work[3];      // [stride * height] denoiser ping-pong buffers + variance
+    uint4* guide;         // [stride * height] albedo rgb + normal xyz as halves (the a-trous taps)
     uint32_t stride;      // pixels per row (the output buffer's width)
 };
 
