@@ -559,8 +559,10 @@ void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, c
     uint32_t* arrivals = reinterpret_cast<uint32_t*>(take(size_t(n) * 4));
     float* nodeBox = reinterpret_cast<float*>(take(size_t(n) * 24));
 
-    const uint32_t init[6] = { 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u };
-    ck(cudaMemcpyAsync(ordBox, init, sizeof(init), cudaMemcpyHostToDevice, stream), "init box");
+    // Ordered-int centroid box: min = 0xFFFFFFFF x3, max = 0 x3.  Set by
+    // memsets on the stream (no host source buffer involved).
+    ck(cudaMemsetAsync(ordBox, 0xFF, 3 * sizeof(uint32_t), stream), "init box min");
+    ck(cudaMemsetAsync(ordBox + 3, 0, 3 * sizeof(uint32_t), stream), "init box max");
     const uint32_t tb = 256;
     const uint32_t blocks = (n + tb - 1) / tb;
     const uint32_t redBlocks = blocks < 1184 ? blocks : 1184;

@@ -4,10 +4,10 @@
 //
 // Who needs it: a caller that must not allocate while it runs, such as a
 // renderer rebuilding a small dynamic mesh's BVH every frame from inside a
-// fixed per-frame memory budget, an embedding application whose device memory
-// is owned by its own pool, or code that is about to issue work it will later
-// replay and therefore must not create allocations in between.  The regular
-// entry (vlrbBvhBuildHost) allocates its scratch and outputs per call.
+// fixed per-frame memory budget, or an embedding application whose device
+// memory is owned by its own pool (a cudaMalloc there would bypass the pool's
+// accounting, and may stall every stream of the device while it runs).  The
+// regular entry (vlrbBvhBuildHost) allocates its scratch and outputs per call.
 //
 // Limits and rules:
 //   * at most kNoAllocMaxTriangles triangles per call (the static scratch is
@@ -20,7 +20,10 @@
 //     parent links, arrival counters) before using it;
 //   * the first call on a device performs a one-time set-up for that device
 //     (the symbol lookup below, which makes the runtime load this file's
-//     device code): make that first call before any stream capture begins.
+//     device code): make that first call before any stream capture begins;
+//   * the looked-up address is kept for the life of the process, so a
+//     device reset (cudaDeviceReset) between calls is not supported: the
+//     reset unloads the module and the kept address no longer points at it.
 #include "vlrb_internal.h"
 #include "lbvh_build.h"
 

@@ -195,8 +195,12 @@ __global__ void demodulateKernel(DenoiseArgs a, float4* illum) {
     const float4 ap = a.albedo[p];
     // the taps' guide record: albedo rgb, normal xyz as halves; albedo r
     // negative marks a pixel that is not filtered
+    // (albedo clamped to the largest finite half: an unclamped texture or
+    // plug value above it would pack to inf and turn tap weights into NaN)
     const float4 np = a.normal[p];
-    a.guide[p] = make_uint4(packHalf2(isGuided(ap) ? ap.x : -1.0f, ap.y), packHalf2(ap.z, np.x),
+    constexpr float kHalfMax = 65504.0f;
+    a.guide[p] = make_uint4(packHalf2(isGuided(ap) ? fminf(ap.x, kHalfMax) : -1.0f, fminf(ap.y, kHalfMax)),
+                            packHalf2(fminf(ap.z, kHalfMax), np.x),
                             packHalf2(np.y, np.z), 0u);
     if (!isGuided(ap)) { illum[p] = make_float4(0.f, 0.f, 0.f, 0.f); return; }
     float sum = 0.0f, sum2 = 0.0f, cnt = 0.0f;
