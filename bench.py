@@ -112,12 +112,15 @@ def cpu_baseline(seconds_target=12.0):
     flat = scenes.flatten_desc(desc)
     threads = os.cpu_count() or 1
     spp = 1
+    states = ref.seed_states(W * H)
     t0 = time.time()
-    _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, threads=threads)
+    _, states, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, rng_states=states,
+                                   threads=threads)
     dt = time.time() - t0
     spp = max(1, min(64, int(seconds_target / max(dt, 1e-3))))
     t0 = time.time()
-    _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, threads=threads)
+    _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp, MAX_PATH_LENGTH, rng_states=states,
+                              threads=threads)
     dt = time.time() - t0
     return {"value": seg / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{W}x{H} Cornell box, {spp} spp, max path length {MAX_PATH_LENGTH} "
@@ -125,7 +128,16 @@ def cpu_baseline(seconds_target=12.0):
                       f"own BSDF/spectral code, brute-force intersection"}
 
 
+REFERENCE_ARM_BUDGET_S = 240.0
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the path (the CPU restatement of
+    path_tracing.cu over the reference's own BSDF/spectral classes built for
+    the host) on all host cores, on this workload: one step = the full
+    512x512 frame of 256 spp when warm-up + timed steps fit in about four
+    minutes on this host, else as many spp per step as fit (stated in
+    config).  Per-pixel RNG seeds are generated once, before any step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -137,25 +149,40 @@ def run_reference(args):
     desc = scenes.cornell_box_desc(W, H)
     flat = scenes.flatten_desc(desc)
     threads = os.cpu_count() or 1
-    spp_step = 2
+    states = ref.seed_states(W * H)
+    t0 = time.time()
+    _, states, _ = ref.pt_render(flat, desc["camera"], W, H, 1, MAX_PATH_LENGTH, rng_states=states,
+                                 threads=threads)
+    per_spp = time.time() - t0
+    spp_step = SPP_PER_STEP
+    if (args.warmup + args.steps) * per_spp * spp_step > REFERENCE_ARM_BUDGET_S:
+        spp_step = max(1, int(REFERENCE_ARM_BUDGET_S / ((args.warmup + args.steps) * per_spp)))
+    film = np.zeros((H, W, 16), np.float64)
     for _ in range(args.warmup):
-        ref.pt_render(flat, desc["camera"], W, H, 1, MAX_PATH_LENGTH, threads=threads)
+        ref.pt_render(flat, desc["camera"], W, H, spp_step, MAX_PATH_LENGTH, rng_states=states, film=film,
+                      threads=threads)
     total_seg = 0
     t0 = time.time()
     for _ in range(args.steps):
-        _, _, seg = ref.pt_render(flat, desc["camera"], W, H, spp_step, MAX_PATH_LENGTH, threads=threads)
+        film[:] = 0.0
+        _, states, seg = ref.pt_render(flat, desc["camera"], W, H, spp_step, MAX_PATH_LENGTH, rng_states=states,
+                                       film=film, threads=threads)
         total_seg += seg
     dt = time.time() - t0
     v = total_seg / dt / 1e9
+    same = spp_step == SPP_PER_STEP
+    workload = (f"Cornell box PT {W}x{H}, {spp_step} spp per step"
+                + ("" if same else f" (bounded CPU sample of the {SPP_PER_STEP} spp frame)")
+                + f", max path length {MAX_PATH_LENGTH}, 4 hero wavelengths, MIS NEE, FP64 film")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"Cornell box PT {W}x{H}, {spp_step} spp per step (bounded CPU sample of the "
-                                   f"256 spp frame), max path length {MAX_PATH_LENGTH}, 4 hero wavelengths"},
+            "config": {"workload": workload, "same_spp_as_gpu_arm": same},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{spp_step} spp of {W}x{H} per step: CPU restatement of path_tracing.cu "
-                                       f"over the reference's own BSDF/spectral code"},
+                             "sample": f"{args.steps} steps of {spp_step} spp of {W}x{H}: CPU restatement of "
+                                       f"path_tracing.cu over the reference's own BSDF/spectral code built for the "
+                                       f"host, OpenMP over rows, brute-force intersection"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -637,6 +664,10 @@ def main():
     scene, cam, keep = scenes.build(ctx, desc)
     ctx.setScene(scene)
     ctx.setOptions(max_path_length=MAX_PATH_LENGTH, max_paths_in_flight=1 << 22)
+    if world > 1:
+        # every rank its own sample streams (rank 0 keeps the reference's seed)
+        from vlr_b200 import multigpu
+        ctx.setOptions(rng_seed=multigpu.rank_seed(rank))
     stream = torch.cuda.current_stream().cuda_stream
     # launch configuration (paths in flight x blocks per SM) chosen by the
     # library's autotuner, one full step per candidate, before any timing

@@ -64,8 +64,7 @@ def pt_render(flat, camera, width, height, spp, max_path_length, rng_states=None
     """Render with the CPU restatement of the reference path tracer
     (oracle/ref_pt.inc).  Returns (film [H,W,16] float64 sum, rng_states, segments)."""
     if rng_states is None:
-        import random
-        rng_states = np.array(seed_states(width * height), np.uint64)
+        rng_states = seed_states(width * height)
     if film is None:
         film = np.zeros((height, width, 16), np.float64)
     cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
@@ -85,9 +84,17 @@ def pt_render(flat, camera, width, height, spp, max_path_length, rng_states=None
 
 def seed_states(n, seed=591842031321323413):
     """std::mt19937_64 outputs (the reference's per-pixel PCG32 seeding,
-    libVLR/context.cpp:1176-1190), generated by the 64-bit Mersenne Twister
-    recurrence."""
-    return list(_mt19937_64(seed, n))
+    libVLR/context.cpp:1176-1190) from the C++ standard library generator in
+    the host build, as a uint64 array."""
+    out = np.zeros(n, np.uint64)
+    lib().vlrref_seed_states(ctypes.c_uint64(seed), ctypes.c_uint64(n), _p(out))
+    return out
+
+
+def seed_states_py(n, seed=591842031321323413):
+    """The same outputs from the published 64-bit Mersenne Twister recurrence
+    in pure Python (slow; pins the C++ generator on small n)."""
+    return np.array(_mt19937_64(seed, n), np.uint64)
 
 
 def _mt19937_64(seed, n):

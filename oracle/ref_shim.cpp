@@ -15,6 +15,7 @@
 //   vlrref_wavelengths          -> WavelengthSamples::createWithEqualOffsets (spectrum_types.h:55-65)
 //   vlrref_bsdf_batch           -> one sample/eval/pdf triple per query (materials.cu classes)
 //   vlrref_tables               -> raw pointers to the Meng tables and CMF bins
+//   vlrref_seed_states          -> std::mt19937_64 per-pixel RNG seeds (context.cpp:1176-1190)
 #include "shared/kernel_common.h"
 
 #include <omp.h>
@@ -65,7 +66,7 @@ namespace {
     // Material ids of the BSDF batch workload.
     enum : uint32_t {
         kMatte = 0, kSpecularBRDF = 1, kMicrofacetBRDF = 2,
-        kMicrofacetBSDF = 3, kLambertianBSDF = 4, kUE4 = 5,
+        kMicrofacetBSDF = 3, kLambertianBSDF = 4, kUE4 = 5, kSpecularBSDF = 6,
     };
 
     struct Packed {
@@ -188,6 +189,15 @@ void vlrref_bsdf_batch(
             runQuery(b, query, ui, v4, p1, w3, e4, ep);
             break;
         }
+        case kSpecularBSDF: {
+            // SpecularScatteringSurfaceMaterial_setupBSDF (materials.cu:1046-1058):
+            // coefficient, exterior IOR 1, interior IOR, dispersive unless a
+            // single wavelength is selected
+            SpecularBSDF b(albedoSp.evaluate(wls), oneSp.evaluate(wls), iorSp.evaluate(wls),
+                           !wls.singleIsSelected());
+            runQuery(b, query, ui, v4, p1, w3, e4, ep);
+            break;
+        }
         default: {
             SampledSpectrum baseColor = albedoSp.evaluate(wls);
             const float roughness = std::fmax(0.01f, rx);
@@ -201,6 +211,13 @@ void vlrref_bsdf_batch(
         }
         }
     }
+}
+
+// n outputs of std::mt19937_64 seeded with `seed`: the reference's per-pixel
+// PCG32 seeding (context.cpp:618-626, 1176-1190).
+void vlrref_seed_states(uint64_t seed, uint64_t n, uint64_t* out) {
+    std::mt19937_64 gen(seed);
+    for (uint64_t i = 0; i < n; ++i) out[i] = gen();
 }
 
 // Raw table access so the extracted tables can be cross-checked against the

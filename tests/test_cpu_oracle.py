@@ -248,3 +248,12 @@ def test_treelet_oracle_keeps_the_tree_valid_and_lowers_its_sah_cost():
     # a second call on the same input gives the same tree
     och2, obx2, nr2 = lbvh.optimize_lbvh(v, prims, ch, boxes, 3)
     assert np.array_equal(och, och2) and np.array_equal(obx, obx2) and nr == nr2
+
+
+@needs_ref
+def test_seed_states_match_mt19937_64_recurrence():
+    """The oracle's per-pixel RNG seeds (std::mt19937_64 of the host build,
+    context.cpp:1176-1190) equal the published 64-bit Mersenne Twister
+    recurrence, including across the 312-word state refills."""
+    for seed in (591842031321323413, 1, 0x9E3779B97F4A7C15):
+        assert np.array_equal(ref.seed_states(1000, seed), ref.seed_states_py(1000, seed))

@@ -8,6 +8,24 @@ work as the sum."""
 import torch
 import torch.distributed as dist
 
+# The reference's seed of the per-pixel RNG streams (context.cpp:1176-1190).
+REFERENCE_SEED = 591842031321323413
+_M64 = (1 << 64) - 1
+
+
+def rank_seed(rank, base=REFERENCE_SEED):
+    """Seed of the per-pixel RNG streams of `rank`: rank 0 keeps `base` (so
+    one GPU renders exactly the reference's samples), every other rank a
+    SplitMix64 hash of base and rank, so the ranks draw independent samples
+    and their summed films hold N times the samples instead of N copies."""
+    if rank == 0:
+        return base
+    z = (base + 0x9E3779B97F4A7C15 * rank) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    z ^= z >> 31
+    return z or 1
+
 
 class _DeviceView:
     """__cuda_array_interface__ over a device allocation of doubles."""
