@@ -18,11 +18,13 @@ const char* vlrbVersion(void);
  * BSDF shading batch.
  *
  * One query = the reference's BSDF sample, then evaluate and evaluatePDF at
- * the sampled direction, for one of six BSDFs built from immediate values the
- * way the reference's setupBSDF callables build them
+ * the sampled direction, for one of seven BSDFs built from immediate values
+ * the way the reference's setupBSDF callables build them
  * (libVLR/GPU_kernels/materials.cu:584-1994).  Arrays are AoS float tuples.
  *   material: 0 Matte, 1 SpecularReflection, 2 MicrofacetReflection,
- *             3 MicrofacetScattering, 4 LambertianScattering, 5 UE4.
+ *             3 MicrofacetScattering, 4 LambertianScattering, 5 UE4,
+ *             6 SpecularScattering (dispersive ideal dielectric, exterior
+ *             IOR 1); any other id builds UE4.
  *   roughness[2]: per-axis roughness r; alpha = max(0.001, r^2) for the GGX
  *             materials, roughness = max(0.01, r.x) for UE4.
  *   ior: grey index of refraction (interior for the dielectric, eta of the
@@ -55,6 +57,13 @@ VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream);
 /* All pointers are host pointers; copies in, runs, copies out, returns when
  * done.  kernelMs (may be NULL) receives the kernel's device time. */
 VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs);
+
+/* vlrbBsdfBatchHost with options.  VLRB_BSDF_BATCH_CONTRACTED runs the copy
+ * of the kernel compiled with fused multiply-add contraction, the arithmetic
+ * the renderers' shading kernels use; without it the kernel rounds every
+ * operation like the reference's host build.  Other bits: InvalidArgument. */
+#define VLRB_BSDF_BATCH_CONTRACTED 1u
+VLRResult vlrbBsdfBatchHostEx(const VLRBBsdfBatch* batch, uint32_t flags, float* kernelMs);
 
 
 /* ------------------------------------------------------------------------
@@ -118,6 +127,16 @@ typedef struct VLRBRenderStats {
 } VLRBRenderStats;
 
 VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);
+
+/* The path tracer's per-pixel RNG states (PCG32 state words) after the last
+ * render, in pixel order (y * width + x of the rendered image), for the first
+ * `count` pixels.  Pixel i's stream starts at the i-th output of
+ * std::mt19937_64(rngSeed), as the reference seeds its per-pixel RNG buffer
+ * (context.cpp:1176-1190), and is advanced by that pixel's samples exactly as
+ * the reference's when every launch renders one sample per pixel
+ * (maxPathsInFlight = pixel count).  InvalidArgument if count exceeds the
+ * pixels or no path tracer render has seeded the states for this image. */
+VLRResult vlrbContextReadPixelRngStates(VLRContext context, uint64_t* states, uint32_t count);
 
 /* Learned path guiding of the path tracer (no counterpart in the reference).
  * With `train`, a launch records training samples at the Matte,

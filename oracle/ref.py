@@ -82,6 +82,27 @@ def pt_render(flat, camera, width, height, spp, max_path_length, rng_states=None
     return film, rng_states, seg.value
 
 
+def pt_camera_rays(flat, camera, width, height, max_path_length, rng_states=None):
+    """One frame of one sample per pixel (as pt_render) that also returns each
+    pixel's camera ray and its brute-force closest hit: (film, rng_states,
+    rays [H*W, 8] = org xyz, prim bits, dir xyz, t)."""
+    if rng_states is None:
+        rng_states = seed_states(width * height)
+    film = np.zeros((height, width, 16), np.float64)
+    cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
+                   [camera["aspect"], camera["sensitivity"], camera["fovy"], camera["lens radius"],
+                    camera["op distance"]], np.float32)
+    rays = np.zeros((width * height, 8), np.float32)
+    rc = lib().vlrref_pt_camera_rays(
+        _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),
+        _p(flat["tris"]), ctypes.c_uint32(len(flat["tris"])), _p(flat["groupMaterial"]),
+        _p(flat["groupLightInst"]), ctypes.c_uint32(len(flat["groupMaterial"])), _p(flat["mats"]),
+        ctypes.c_uint32(len(flat["mats"])), _p(cam), ctypes.c_uint32(width), ctypes.c_uint32(height),
+        ctypes.c_uint32(max_path_length), _p(rng_states), _p(film), _p(rays))
+    assert rc == 0
+    return film, rng_states, rays
+
+
 def seed_states(n, seed=591842031321323413):
     """std::mt19937_64 outputs (the reference's per-pixel PCG32 seeding,
     libVLR/context.cpp:1176-1190) from the C++ standard library generator in

@@ -48,6 +48,8 @@ def lib():
         _lib.vlrbVersion.restype = ctypes.c_char_p
         _lib.vlrbBsdfBatch.argtypes = [ctypes.POINTER(_BsdfBatch), ctypes.c_void_p]
         _lib.vlrbBsdfBatchHost.argtypes = [ctypes.POINTER(_BsdfBatch), ctypes.POINTER(ctypes.c_float)]
+        _lib.vlrbBsdfBatchHostEx.argtypes = [ctypes.POINTER(_BsdfBatch), ctypes.c_uint32,
+                                             ctypes.POINTER(ctypes.c_float)]
     return _lib
 
 
@@ -60,9 +62,10 @@ BATCH_INPUTS = ("wo", "material", "roughness", "ior", "albedo", "metallic", "u",
 BATCH_OUTPUTS = {"value": 4, "pdf": 1, "wi": 3, "evalValue": 4, "evalPdf": 1}
 
 
-def make_bsdf_batch_inputs(n, seed=0):
-    """Seeded synthetic BSDF-batch queries: material uniform over the six
-    BSDFs, wo uniform on the sphere, roughness log-uniform in [0.01, 1] per
+def make_bsdf_batch_inputs(n, seed=0, materials=6):
+    """Seeded synthetic BSDF-batch queries: material uniform over the first
+    `materials` ids (6: the six BSDFs of the shading-batch workload; 7 adds
+    SpecularScattering), wo uniform on the sphere, roughness log-uniform in [0.01, 1] per
     axis, IOR uniform in [1.3, 1.8], albedo and metallic uniform in [0, 1],
     three uniform numbers for (uComponent, uDir0, uDir1) and two for the
     wavelength offset and hero selection."""
@@ -74,7 +77,7 @@ def make_bsdf_batch_inputs(n, seed=0):
     wo /= np.linalg.norm(wo, axis=1, keepdims=True)
     return {
         "wo": np.ascontiguousarray(wo, dtype=np.float32),
-        "material": rng.integers(0, 6, n).astype(np.uint32),
+        "material": rng.integers(0, materials, n).astype(np.uint32),
         "roughness": np.exp(rng.uniform(np.log(0.01), 0.0, (n, 2))).astype(np.float32),
         "ior": rng.uniform(1.3, 1.8, n).astype(np.float32),
         "albedo": rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32),
@@ -90,8 +93,10 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-def bsdf_batch_host(inputs):
+def bsdf_batch_host(inputs, contracted=False):
     """Run the BSDF batch from host numpy arrays (copies in and out).
+    contracted: run the copy of the kernel compiled with FMA contraction (the
+    renderers' arithmetic) instead of the exactly rounded one.
     Returns (outputs dict, kernel milliseconds)."""
     n = len(inputs["material"])
     outs = {k: np.zeros((n, c) if c > 1 else n, np.float32) for k, c in BATCH_OUTPUTS.items()}
@@ -99,7 +104,8 @@ def bsdf_batch_host(inputs):
     b = _BsdfBatch(n, *[_ptr(ins[k]).value for k in BATCH_INPUTS],
                    *[_ptr(outs[k]).value for k in BATCH_OUTPUTS])
     ms = ctypes.c_float(0.0)
-    check(lib().vlrbBsdfBatchHost(ctypes.byref(b), ctypes.byref(ms)), "vlrbBsdfBatchHost")
+    check(lib().vlrbBsdfBatchHostEx(ctypes.byref(b), ctypes.c_uint32(1 if contracted else 0), ctypes.byref(ms)),
+          "vlrbBsdfBatchHostEx")
     return outs, ms.value
 
 

@@ -42,8 +42,8 @@ extern "C" VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream) 
     }
 }
 
-extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs) {
-    if (!validBatch(batch))
+static VLRResult bsdfBatchHost(const VLRBBsdfBatch* batch, uint32_t flags, float* kernelMs) {
+    if (!validBatch(batch) || (flags & ~VLRB_BSDF_BATCH_CONTRACTED))
         return VLRResult_InvalidArgument;
     if (batch->count == 0) {
         if (kernelMs) *kernelMs = 0.0f;
@@ -81,7 +81,8 @@ extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernel
         d.wi = reinterpret_cast<float*>(ob + n * 36);
         d.evalPdf = reinterpret_cast<float*>(ob + n * 48);
         float ms = 0.0f;
-        cudaError_t e = vlrb::launchBsdfBatch(d, nullptr, &ms);
+        cudaError_t e = (flags & VLRB_BSDF_BATCH_CONTRACTED) ? vlrb::launchBsdfBatchContracted(d, nullptr, &ms)
+                                                              : vlrb::launchBsdfBatch(d, nullptr, &ms);
         if (e != cudaSuccess)
             return VLRResult_InternalError;
         cudaMemcpy(batch->value, d.value, n * 16, cudaMemcpyDeviceToHost);
@@ -96,6 +97,14 @@ extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernel
         std::fprintf(stderr, "vlrbBsdfBatchHost: %s\n", ex.what());
         return VLRResult_InternalError;
     }
+}
+
+extern "C" VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs) {
+    return bsdfBatchHost(batch, 0u, kernelMs);
+}
+
+extern "C" VLRResult vlrbBsdfBatchHostEx(const VLRBBsdfBatch* batch, uint32_t flags, float* kernelMs) {
+    return bsdfBatchHost(batch, flags, kernelMs);
 }
 
 static VLRResult bvhBuildHost(const float* triVerts, uint32_t n, uint32_t treeletRounds, uint32_t* sortedCodes,

@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(256) eyeStartKernel(BptArgs a) {
     const Camera &C = S.cam;
     const uint32_t nCached = numCached(a);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.numPaths; p += gridDim.x * blockDim.x) {
-        const uint32_t pixel = p % (a.width * a.height);
+        const uint32_t pixel = pixelOfPath(p, a.width, a.height);
         const uint32_t px = pixel % a.width, py = pixel / a.width;
         PCG32 rng{ a.pb.rng[p] };
         float fx = px + rng.uniform(), fy = py + rng.uniform();
@@ -813,7 +813,7 @@ __global__ void __launch_bounds__(256) eyeFilmKernel(BptArgs a) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.numPaths; p += gridDim.x * blockDim.x) {
         S4 c = toS4(a.pb.contrib[p]);
         if (!c.allFinite()) continue;
-        const uint32_t pixel = p % (a.width * a.height);
+        const uint32_t pixel = pixelOfPath(p, a.width, a.height);
         const uint32_t fi = (pixel / a.width) * a.stride + pixel % a.width;
         filmAdd(a.film.strata + static_cast<size_t>(fi) * kNumStrata, lam, c);
     }

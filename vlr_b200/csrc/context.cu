@@ -873,9 +873,9 @@ void Context::setupCamera(const Camera* cam) {
     }
 }
 
-void Context::ensurePathBuffers(uint32_t paths) {
+void Context::ensurePathBuffers(uint32_t paths, uint32_t imageW, uint32_t imageH) {
     const uint64_t seed = options.rngSeed ? options.rngSeed : 591842031321323413ull;
-    if (paths <= pathCapacity && seed == pathSeed) return;
+    if (paths <= pathCapacity && seed == pathSeed && imageW == pathSeedW && imageH == pathSeedH) return;
     if (paths > pathCapacity) {
         if (pathCapacity > 0) {
             // keep the running totals across the reallocation
@@ -890,12 +890,33 @@ void Context::ensurePathBuffers(uint32_t paths) {
         pathCapacity = paths;
     }
     pathSeed = seed;
+    pathSeedW = imageW;
+    pathSeedH = imageH;
     paths = pathCapacity;
-    std::vector<uint64_t> seeds(paths);
-    // Per-slot PCG32 states from std::mt19937_64, slot order = pixel order for
-    // the first sample of each pixel (context.cpp:1176-1190).
-    seedPathRngs(seeds.data(), paths, seed);
+    std::vector<uint64_t> gen(paths), seeds(paths);
+    // Per-slot PCG32 states from std::mt19937_64 (context.cpp:1176-1190): the
+    // reference seeds pixel y*W+x with the generator's (y*W+x)-th output, so
+    // slot p of each full image block takes the output of the pixel it
+    // renders (pixelOfPath) and keeps that pixel's stream across launches.
+    seedPathRngs(gen.data(), paths, seed);
+    const uint32_t pixels = imageW * imageH;
+    const uint32_t fullBlocks = pixels ? paths / pixels : 0;
+    for (uint32_t p = 0; p < paths; ++p) {
+        const uint32_t block = pixels ? p / pixels : 0;
+        seeds[p] = block < fullBlocks ? gen[block * pixels + pixelOfPath(p, imageW, imageH)] : gen[p];
+    }
     ck(cudaMemcpy(pb.rng, seeds.data(), size_t(paths) * 8, cudaMemcpyHostToDevice), "seed rngs");
+}
+
+bool Context::readPixelRngStates(uint64_t* states, uint32_t count) {
+    const uint32_t pixels = imgW * imgH;
+    if (count > pixels || count > pathCapacity || pathSeedW != imgW || pathSeedH != imgH) return false;
+    std::vector<uint64_t> slots(pixels);
+    ck(cudaMemcpy(slots.data(), pb.rng, size_t(pixels) * 8, cudaMemcpyDeviceToHost), "read rngs");
+    std::vector<uint64_t> byPixel(pixels);
+    for (uint32_t p = 0; p < pixels; ++p) byPixel[pixelOfPath(p, imgW, imgH)] = slots[p];
+    std::copy(byPixel.begin(), byPixel.begin() + count, states);
+    return true;
 }
 
 void Context::ensureGuiding(uint32_t paths) {
@@ -961,7 +982,7 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
     Film fl = filmDesc();
     if (samples > 0) {
         uint32_t perLaunch = std::max<uint32_t>(1, std::min<uint32_t>(samples, options.maxPathsInFlight / pixels));
-        ensurePathBuffers(pixels * perLaunch);
+        ensurePathBuffers(pixels * perLaunch, imgW, imgH);
         uint32_t done = 0;
         while (done < samples) {
             uint32_t k = std::min(perLaunch, samples - done);

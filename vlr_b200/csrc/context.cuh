@@ -128,10 +128,15 @@ public:
     uint32_t numAccumFrames = 0;
     uint64_t generation = 1, builtGeneration = 0;
 
+    // Path tracer RNG states of the first sample's slots in pixel order
+    // (pixel y*imgW+x), count <= imgW*imgH; false if the path buffers do not
+    // hold that many.
+    bool readPixelRngStates(uint64_t* states, uint32_t count);
+
 private:
     void buildScene(cudaStream_t stream);
     void setupCamera(const Camera* cam);
-    void ensurePathBuffers(uint32_t paths);
+    void ensurePathBuffers(uint32_t paths, uint32_t imageW, uint32_t imageH);
     void ensureGuiding(uint32_t paths);
     void trainGuide(cudaStream_t stream);
 
@@ -166,6 +171,7 @@ private:
     BptBuffers bb{};
     uint32_t pathCapacity = 0;
     uint64_t pathSeed = 0;
+    uint32_t pathSeedW = 0, pathSeedH = 0;   // image layout the path RNG states were seeded for
     unsigned long long totalsBase[2] = { 0, 0 };
     uint32_t bptCapacityPaths = 0, bptCapacityVerts = 0, bptEyeCapacity = 0;
     // light tracing: light subpaths of one frame and their lens connections

@@ -39,16 +39,6 @@ __device__ __forceinline__ WLS loadWls(const PathBuffers &pb, uint32_t p) {
     return w;
 }
 
-// Pixel of path slot p: the slots of one sample cover the image in 8x4-pixel
-// tiles, one warp per tile, when it divides into them (row-major otherwise),
-// so a warp's camera rays leave neighbouring pixels in both directions.
-__device__ __forceinline__ uint32_t pixelOfPath(uint32_t p, uint32_t W, uint32_t H) {
-    const uint32_t i = p % (W * H);
-    if ((W & 7u) || (H & 3u)) return i;
-    const uint32_t tile = i >> 5, lane = i & 31u, tilesX = W >> 3;
-    return ((tile / tilesX) * 4 + (lane >> 3)) * W + (tile % tilesX) * 8 + (lane & 7u);
-}
-
 __global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, FrameParams fp) {
     const uint32_t P = fp.numPaths;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {

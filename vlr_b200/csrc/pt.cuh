@@ -18,6 +18,18 @@ enum : uint32_t {
     kCntBucket0 = 2,         // material-sorted hit queues (kNumShadeBuckets)
 };
 
+// Pixel of path slot p: the slots of one sample cover the image in 8x4-pixel
+// tiles, one warp per tile, when it divides into them (row-major otherwise),
+// so a warp's camera rays leave neighbouring pixels in both directions.
+// Slot p of every launch renders this pixel, so its RNG state is that
+// pixel's stream (seeded in pixel order, as the reference seeds them).
+VLRB_HD uint32_t pixelOfPath(uint32_t p, uint32_t W, uint32_t H) {
+    const uint32_t i = p % (W * H);
+    if ((W & 7u) || (H & 3u)) return i;
+    const uint32_t tile = i >> 5, lane = i & 31u, tilesX = W >> 3;
+    return ((tile / tilesX) * 4 + (lane >> 3)) * W + (tile % tilesX) * 8 + (lane & 7u);
+}
+
 struct ShadowRay {
     float4 org;      // xyz, w = tmax
     float4 dir;      // xyz, w = path index (bits)

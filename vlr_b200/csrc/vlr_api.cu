@@ -1391,6 +1391,14 @@ VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats) {
     API_CATCH("vlrbContextGetStats")
 }
 
+VLRResult vlrbContextReadPixelRngStates(VLRContext context, uint64_t* states, uint32_t count) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!states && count > 0) return VLRResult_InvalidArgument;
+    API_TRY
+    return c->readPixelRngStates(states, count) ? VLRResult_NoError : VLRResult_InvalidArgument;
+    API_CATCH("vlrbContextReadPixelRngStates")
+}
+
 VLRResult vlrbContextSaveOutputImages(VLRContext context, const char* pathWithoutExtension, float brightnessCoeff) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!pathWithoutExtension || c->width == 0 || c->height == 0) return VLRResult_InvalidArgument;

@@ -6,7 +6,8 @@
 
 namespace vlrb {
 
-// bsdf_batch.cu
+// bsdf_batch.cu (no FMA contraction) and bsdf_batch_contracted.cu (FMA)
 cudaError_t launchBsdfBatch(const VLRBBsdfBatch &b, cudaStream_t stream, float* kernelMs);
+cudaError_t launchBsdfBatchContracted(const VLRBBsdfBatch &b, cudaStream_t stream, float* kernelMs);
 
 } // namespace vlrb

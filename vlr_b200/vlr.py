@@ -87,6 +87,7 @@ def _api():
         "vlrContextGetOutputBufferSize": [v, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)],
         "vlrContextReadOutputBuffer": [v, v],
         "vlrbContextReadAuxBuffers": [v, v, v],
+        "vlrbContextReadPixelRngStates": [v, v, ctypes.c_uint32],
         "vlrbWriteOutputImages": [v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_float],
         "vlrbContextSaveOutputImages": [v, ctypes.c_char_p, ctypes.c_float],
         "vlrContextSetScene": [v, v],
@@ -503,6 +504,14 @@ class Context:
         p = c_void_p()
         check(_api().vlrbContextGetFilmDevicePointer(self.h, ctypes.byref(p)), "filmPtr")
         return p.value
+
+    def read_pixel_rng_states(self, count=None):
+        """Per-pixel PCG32 states of the path tracer, in pixel order."""
+        n = self.width * self.height if count is None else count
+        out = np.zeros(n, np.uint64)
+        check(_api().vlrbContextReadPixelRngStates(self.h, out.ctypes.data_as(c_void_p), ctypes.c_uint32(n)),
+              "readPixelRngStates")
+        return out
 
     def stats(self):
         s = VLRBRenderStats()
