@@ -103,6 +103,39 @@ def pt_camera_rays(flat, camera, width, height, max_path_length, rng_states=None
     return film, rng_states, rays
 
 
+def env_set(env=None, mode=0, tex_weight_rounding=0):
+    """Environment light of the following pt_render calls: env = the
+    description's {"image": HxWx4 float32, "scale", "rotation"} (None removes
+    it); mode 0 samples the full-resolution FP64 importance map the CUDA
+    build uses, mode 1 the reference's own 4x smaller FP32 map."""
+    if env is None:
+        lib().vlrref_env_set(0, None, 0, 0, None, ctypes.c_float(1.0), ctypes.c_float(0.0), 0, 0)
+        return
+    img = env.get("image")
+    const = np.array(env.get("constant", (0.0, 0.0, 0.0)), np.float32)
+    if img is not None:
+        img = np.ascontiguousarray(img, np.float32)
+        h, w = img.shape[:2]
+        ptr = _p(img)
+    else:
+        h = w = 0
+        ptr = None
+    lib().vlrref_env_set(1, ptr, ctypes.c_uint32(w), ctypes.c_uint32(h), _p(const),
+                         ctypes.c_float(env.get("scale", 1.0)), ctypes.c_float(env.get("rotation", 0.0)),
+                         ctypes.c_int(mode), ctypes.c_int(tex_weight_rounding))
+
+
+def env_unsampleable():
+    """Texels with positive luminance that the importance map can never
+    sample (zero CDF step): FP64 full-resolution map, the same map built by
+    the reference's FP32 Kahan builder, and the reference's own 4x smaller
+    FP32 map; with the positive-texel counts."""
+    v = [ctypes.c_uint64() for _ in range(5)]
+    lib().vlrref_env_unsampleable(*[ctypes.byref(x) for x in v])
+    return {"fp64_full": v[0].value, "fp32_full": v[1].value, "positive_full": v[2].value,
+            "fp32_quarter": v[3].value, "positive_quarter": v[4].value}
+
+
 def seed_states(n, seed=591842031321323413):
     """std::mt19937_64 outputs (the reference's per-pixel PCG32 seeding,
     libVLR/context.cpp:1176-1190) from the C++ standard library generator in

@@ -478,6 +478,20 @@ cudaTextureAddressMode parseWrap(const std::string &s) {
 
 } // namespace
 
+// Meng (u, v) and brightness s of a linear Rec.709 (D65) texel, the
+// reference's per-pixel conversion for light-source images in spectral mode
+// (image.cpp:542-566, xy_to_uv spectrum_types.h:382-391).
+static void envTexelUVS(const float* rgb, float* u, float* v, float* s) {
+    float c[3] = { rgb[0], rgb[1], rgb[2] }, xyz[3];
+    mulColMajor(hostColorMatrices().rec709D65ToXYZ, c, xyz);
+    const float b = xyz[0] + xyz[1] + xyz[2];
+    const float x = b > 0.0f ? xyz[0] / b : (1.0f / 3.0f);
+    const float y = b > 0.0f ? xyz[1] / b : (1.0f / 3.0f);
+    *u = 16.730260708356887f * x + 7.7801960340706f * y - 2.170152247475828f;
+    *v = -7.530081094743006f * x + 16.192422314095225f * y + 1.1125529268825947f;
+    *s = b;
+}
+
 void Context::buildScene(cudaStream_t stream) {
     if (!sceneTextures.empty()) {
         // kernels of earlier frames may still read the textures
@@ -783,31 +797,53 @@ void Context::buildScene(cudaStream_t stream) {
             if (iit != node->objects.end()) img = static_cast<const Image2D*>(iit->second);
         }
         uint32_t w = 1, h = 1;
-        std::vector<UpSpec> texels;
         std::vector<float> lum;
+        // untextured: the immediate emittance everywhere (textured: unused)
+        sg.envTexels = upload(std::vector<UpSpec>{ f.mats[envMatIndex].emit }, stream);
+        sg.envTex = 0;
         if (img && img->width > 0) {
             w = img->width;
             h = img->height;
-            texels.resize(size_t(w) * h);
             lum.resize(size_t(w) * h);
-            const ColorMatrices &M = hostColorMatrices();
-            for (size_t i = 0; i < texels.size(); ++i) {
-                float r = img->rgba[4 * i], g = img->rgba[4 * i + 1], bb2 = img->rgba[4 * i + 2];
-                texels[i] = mengUpsample(hostMengTables(), M, SpType::LightSource, ColorSp::Rec709, r, g, bb2);
-                float rgb[3] = { r, g, bb2 }, xyz[3];
-                mulColMajor(M.rec709D65ToXYZ, rgb, xyz);
-                lum[i] = std::fmax(xyz[1], 0.0f);
+            // Per texel, the reference's spectral-mode image conversion
+            // (image.cpp:542-566): Rec.709 (D65) RGB -> XYZ, b = X + Y + Z,
+            // chromaticity -> Meng (u, v), stored with s = b as halves.  The
+            // importance map's luminance is the reference's for that format
+            // (image.cpp:1010-1017): y(u, v) * s of the stored halves.
+            std::vector<__half> uvs(size_t(w) * h * 4);
+            for (size_t i = 0; i < lum.size(); ++i) {
+                float hu, hv, hs;
+                envTexelUVS(&img->rgba[4 * i], &hu, &hv, &hs);
+                uvs[4 * i + 0] = __float2half_rn(hu);
+                uvs[4 * i + 1] = __float2half_rn(hv);
+                uvs[4 * i + 2] = __float2half_rn(hs);
+                uvs[4 * i + 3] = __float2half_rn(img->rgba[4 * i + 3]);
+                const float su = __half2float(uvs[4 * i + 0]), sv = __half2float(uvs[4 * i + 1]);
+                const float sY = 0.022853819546830627f * su + 0.05077639329371236f * sv - 0.006895157122499944f;
+                lum[i] = std::fmax(sY * __half2float(uvs[4 * i + 2]), 0.0f);
             }
+            // the (u, v, s) image in a texture object the renderers fetch bilinearly
+            auto st = std::make_unique<SceneTexture>();
+            cudaChannelFormatDesc cd = cudaCreateChannelDescHalf4();
+            ck(cudaMallocArray(&st->array, &cd, w, h), "env array");
+            ck(cudaMemcpy2DToArray(st->array, 0, 0, uvs.data(), size_t(w) * 8, size_t(w) * 8, h,
+                                   cudaMemcpyHostToDevice), "env upload");
+            cudaResourceDesc rd{};
+            rd.resType = cudaResourceTypeArray;
+            rd.res.array.array = st->array;
+            cudaTextureDesc td{};
+            td.addressMode[0] = cudaAddressModeWrap;
+            td.addressMode[1] = cudaAddressModeWrap;
+            td.filterMode = cudaFilterModeLinear;
+            td.readMode = cudaReadModeElementType;
+            td.normalizedCoords = 1;
+            ck(cudaCreateTextureObject(&st->tex, &rd, &td, nullptr), "env texture");
+            sg.envTex = static_cast<unsigned long long>(st->tex);
+            sceneTextures.push_back(std::move(st));
         }
         else {
-            // Constant environment: the immediate emittance everywhere.
-            texels.push_back(f.mats[envMatIndex].emit);
-            f.mats[envMatIndex].emitScale = f.mats[envMatIndex].emitScale;
             lum.push_back(1.0f);
         }
-        // The texel radiance already carries the immediate emittance for the
-        // textured case; the descriptor's scale multiplies both.
-        sg.envTexels = upload(texels, stream);
         auto dist = std::make_unique<DeviceBuffer>();
         const size_t bRow = (size_t(h) * (w + 1) * 8 + 255) & ~size_t(255);
         const size_t bMarg = ((h + 1) * 8 + 255) & ~size_t(255);

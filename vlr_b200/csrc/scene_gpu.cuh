@@ -220,7 +220,10 @@ struct SceneGPU {
     float envRotation;
     float envLightProb;             // instProb * geomInstProb of the environment
     EnvDist env;
-    const UpSpec* envTexels;        // [h][w] upsampled radiance per texel
+    const UpSpec* envTexels;        // [1] the immediate emittance of an untextured environment
+    unsigned long long envTex;      // cudaTextureObject_t of the environment image (0: untextured):
+                                    // per texel Meng (u, v, s) + alpha in half precision, bilinear,
+                                    // repeat in u and v, normalised coordinates
     SceneBounds bounds;
     Camera cam;
     MengTables meng;
@@ -646,11 +649,19 @@ __device__ __forceinline__ float envPdfUV(const EnvDist &E, float u, float v) {
     return E.margPdf[row] * E.rowPdf[static_cast<size_t>(row) * E.w + col];
 }
 
-// Radiance of the environment at texture coordinate (u, v), nearest texel.
+// Radiance of the environment at texture coordinate (u, v), as the
+// reference's spectral build computes it (shader_nodes.cu:457-483): the
+// image is held as per-texel Meng-Simon coordinates (u, v) and brightness s
+// in half precision (image.cpp:542-566), the texture unit filters those
+// bilinearly with repeat wrapping (the node's default linear filter,
+// shader_nodes.cpp:1895-1915), and the spectrum is the one at the filtered
+// (u, v) with scale s / EqualEnergyReflectance.
 __device__ __forceinline__ S4 envRadiance(const SceneGPU &S, float u, float v, const WLS &wls) {
-    uint32_t row = min(static_cast<uint32_t>(v * S.env.h), S.env.h - 1);
-    uint32_t col = min(static_cast<uint32_t>(u * S.env.w), S.env.w - 1);
-    UpSpec t = S.envTexels[static_cast<size_t>(row) * S.env.w + col];
+    if (!S.envTex) return mengEvaluate(S.meng, S.envTexels[0], wls);
+    const float4 uvs = tex2DLod<float4>(static_cast<cudaTextureObject_t>(S.envTex), u, v, 0.0f);
+    UpSpec t;
+    mengAdjacents(S.meng, uvs.x, uvs.y, &t);
+    t.scale = uvs.z / kMengEqualEnergy;
     return mengEvaluate(S.meng, t, wls);
 }
 

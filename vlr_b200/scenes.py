@@ -219,6 +219,45 @@ def flatten_desc(desc):
             "mats": recs}
 
 
+def flatten_instanced_desc(desc):
+    """flatten_desc() of a description with instanced meshes (terrain
+    workload layout): every instance's mesh is appended in world space,
+    positions transformed as the library flattens them (s * x + t in float32,
+    in the same order), normals by the inverse scale, tangents by the scale."""
+    flat = flatten_desc(desc)
+    names = list(desc["materials"].keys())
+    pos, nrm, tan, tris, gmat, glight = ([flat["pos"]], [flat["nrm"]], [flat["tan"]], [flat["tris"]],
+                                         list(flat["groupMaterial"]), list(flat["groupLightInst"]))
+    base = len(flat["pos"])
+    for inst in desc.get("instances", []):
+        mesh = desc["instanced"][inst["mesh"]]
+        vv = mesh["verts"]
+        s = np.float32(inst["scale"])
+        t = np.array(inst["translate"], np.float32)
+        zero = np.float32(0.0)
+        p = vv[:, 0:3].astype(np.float32)
+        x = ((s * p[:, 0] + zero * p[:, 1]) + zero * p[:, 2]) + t[0]
+        y = ((zero * p[:, 0] + s * p[:, 1]) + zero * p[:, 2]) + t[1]
+        z = ((zero * p[:, 0] + zero * p[:, 1]) + s * p[:, 2]) + t[2]
+        pos.append(np.stack([x, y, z], 1).astype(np.float32))
+        nrm.append((vv[:, 3:6] * (np.float32(1.0) / s)).astype(np.float32))
+        tan.append((vv[:, 6:9] * s).astype(np.float32))
+        for idx, mname in mesh["groups"]:
+            g = len(gmat)
+            gmat.append(names.index(mname))
+            glight.append(-1)
+            tri = idx.reshape(-1, 3).astype(np.uint32) + base
+            tris.append(np.concatenate([tri, np.full((len(tri), 1), g, np.uint32)], axis=1))
+        base += len(vv)
+    out = dict(flat)
+    out.update({"pos": np.ascontiguousarray(np.concatenate(pos), np.float32),
+                "nrm": np.ascontiguousarray(np.concatenate(nrm), np.float32),
+                "tan": np.ascontiguousarray(np.concatenate(tan), np.float32),
+                "tris": np.ascontiguousarray(np.concatenate(tris), np.uint32),
+                "groupMaterial": np.array(gmat, np.int32), "groupLightInst": np.array(glight, np.int32)})
+    return out
+
+
 def _fbm(n, seed, octaves=7):
     """(n+1)x(n+1) fractional Brownian motion heights in [-1, 1] from bilinearly
     interpolated value noise, seeded."""
