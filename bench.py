@@ -365,14 +365,57 @@ def bsdf_batch_workload(hbm_peak):
     return out
 
 
-def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt")):
+TERRAIN_CPU_W, TERRAIN_CPU_H = 192, 108
+
+
+def terrain_cpu_baseline(desc, renderer, seconds_target=10.0):
+    """The reference's CPU implementation of the terrain workload's
+    integrator (CPU restatements of path_tracing.cu / lvc_bpt.cu over the
+    reference's BSDF/spectral classes, the environment light with the
+    reference's own importance map, a median-split BVH over the same 3.4 M
+    triangles), all host threads, at 1/10 of the resolution; timed over the
+    render loops only (scene and hierarchy set-up excluded, as on the GPU)."""
+    from oracle import ref
+    from vlr_b200 import scenes
+    if not ref.available():
+        return None
+    W, H = TERRAIN_CPU_W, TERRAIN_CPU_H
+    flat = scenes.flatten_instanced_desc(desc)
+    cam = dict(desc["camera"])
+    cam["aspect"] = W / H
+    threads = os.cpu_count() or 1
+    ref.env_set(desc["env"], mode=1)
+    try:
+        def run(spp):
+            if renderer == "pt":
+                _, _, seg = ref.pt_render(flat, cam, W, H, spp, 12, threads=threads)
+            else:
+                _, _, seg, _ = ref.bpt_render(flat, cam, W, H, spp, 12, W * H, threads=threads)
+            return seg, ref.last_render_seconds()
+        seg, dt = run(1)
+        spp = max(1, min(256, int(seconds_target / max(dt, 1e-3))))
+        seg, dt = run(spp)
+    finally:
+        ref.env_set(None)
+    name = "path_tracing.cu" if renderer == "pt" else "lvc_bpt.cu (one light subpath per pixel per frame)"
+    return {"value": seg / dt / 1e9, "unit": "G path segments/s", "cores": threads, "kind": "port",
+            "sample": f"{W}x{H} (1/10 of the 1920x1080 frame), {spp} spp, max depth 12, {len(flat['tris'])} "
+                      f"triangles ({seg} segments in {dt:.1f} s): CPU restatement of {name} over the reference's "
+                      f"own BSDF/spectral code"}
+
+
+def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True):
     """Path tracing and LVC-BPT on the 2,097,152-triangle terrain with 4096
     instanced icospheres under the 2048x1024 sky (FP64 CDF), 1920x1080,
-    max depth 12; device-timed segments/s after warm-up."""
+    max depth 12, one light subpath per pixel per frame for LVC-BPT;
+    device-timed segments/s after warm-up (8 and 4 spp: bounded samples of
+    the 64-spp frame), the dominant wavefront stage against the HBM
+    roofline, and the CPU restatement on the host cores beside it."""
     import torch
     from vlr_b200 import vlr as V, scenes
     W, H = 1920, 1080
     desc = scenes.terrain_scene_desc(W, H)
+    hbm_peak, peak_kind = measured_peaks()
     out = {}
     for name, renderer, spp in (("terrain_pt", V.RENDERER_PATH_TRACING, 8), ("terrain_lvc_bpt", V.RENDERER_BPT, 4)):
         if name not in names:
@@ -397,12 +440,38 @@ def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt")):
         ms = e0.elapsed_time(e1)
         seg = ctx.stats()["pathSegments"] - s0
         st = ctx.stats()
-        out[name] = {"workload": f"{'path tracing' if renderer == V.RENDERER_PATH_TRACING else 'LVC-BPT'} "
-                                 f"{W}x{H}, {spp} spp, max depth 12, sky with sun (FP64 CDF)",
-                     "triangles": st["numTriangles"], "segments_per_s": seg / (ms * 1e-3) / 1e9,
-                     "unit": "G path segments/s", "ms": ms}
-        if renderer == V.RENDERER_BPT:
-            out[name]["light_vertex_overflow"] = st["lightVertexOverflow"]
+        # per-stage device times of one more sample of the same frame
+        ctx.set_profiling(True)
+        ctx.kernel_times(reset=True)
+        q0 = ctx.stats()
+        ctx.render_samples(cam, False, 1, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        stages, _ = ctx.kernel_times(reset=True)
+        q1 = ctx.stats()
+        ctx.set_profiling(False)
+        rays = q1["pathSegments"] - q0["pathSegments"]
+        r = {"workload": f"{'path tracing' if renderer == V.RENDERER_PATH_TRACING else 'LVC-BPT'} "
+                         f"{W}x{H}, {spp} spp per timed call (bounded sample of the 64-spp frame), max depth 12, "
+                         f"sky with sun (FP64 CDF)",
+             "triangles": st["numTriangles"], "segments_per_s": seg / (ms * 1e-3) / 1e9,
+             "unit": "G path segments/s", "ms": ms,
+             "stage_ms_per_spp": {k: v["ms"] for k, v in stages.items() if v["ms"] > 0}}
+        if renderer == V.RENDERER_PATH_TRACING:
+            dom = max(("trace", "shade", "shadow"), key=lambda k: stages[k]["ms"])
+            units = rays if dom != "shadow" else q1["shadowRays"] - q0["shadowRays"]
+            gbs = STAGE_BYTES[dom] * units / (stages[dom]["ms"] * 1e-3) / 1e9
+            r["roofline"] = {"bound": "hbm", "kernel": dom + "Kernel", "achieved": gbs, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": gbs / hbm_peak, "peak_source": peak_kind,
+                             "bytes_per_unit": STAGE_BYTES[dom],
+                             "note": "algorithmic bytes of the wavefront state; BVH node traffic excluded"}
+        else:
+            r["light_vertex_overflow"] = st["lightVertexOverflow"]
+        if cpu:
+            try:
+                r["cpu_baseline"] = terrain_cpu_baseline(desc, "pt" if renderer == V.RENDERER_PATH_TRACING else "bpt")
+            except Exception as ex:  # reported, never fatal for the GPU line
+                r["cpu_baseline"] = {"error": str(ex)}
+        out[name] = r
         ctx.close()
     return out
 

@@ -82,8 +82,8 @@ typedef struct VLRBRenderOptions {
     uint32_t maxPathLength;       /* hits after which a path stops scattering (reference: 25) */
     uint32_t maxPathsInFlight;    /* path slots per launch (memory ~ 200 B each) */
     uint32_t lightPathsPerFrame;  /* light subpaths per frame of LVC-BPT and the light tracer;
-                                     0 = a quarter of the pixel count (LVC-BPT), the pixel
-                                     count (light tracing) */
+                                     0 = the pixel count (one per pixel path); the LVC-BPT
+                                     cache holds 10 vertices per light subpath */
     uint64_t rngSeed;             /* seed of the per-path RNG states, 0 = the reference's
                                      591842031321323413 (context.cpp:1176-1190) */
     uint32_t consistentDielectricPdf;  /* 0: MicrofacetScattering pdf exactly as the reference,

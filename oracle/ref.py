@@ -82,6 +82,39 @@ def pt_render(flat, camera, width, height, spp, max_path_length, rng_states=None
     return film, rng_states, seg.value
 
 
+LIGHT_SEED = 459182033132123413
+
+
+def bpt_render(flat, camera, width, height, frames, max_path_length, num_light_paths, state=None, film=None,
+               threads=0):
+    """Render `frames` LVC-BPT frames with the CPU restatement of the
+    reference's lvc_bpt.cu (oracle/ref_bpt.inc); the environment of env_set
+    applies.  state carries the eye RNG states (per pixel), the light RNG
+    states (per light subpath, seeded from std::mt19937_64(459182033132123413)
+    as the reference seeds them) and the per-frame wavelength generator's
+    draws across calls.  Returns (film [H,W,16] float64 sum, state, segments,
+    light vertices stored)."""
+    if state is None:
+        state = {"eye": seed_states(width * height), "light": seed_states(num_light_paths, LIGHT_SEED),
+                 "wl": np.zeros(1, np.uint64)}
+    if film is None:
+        film = np.zeros((height, width, 16), np.float64)
+    cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
+                   [camera["aspect"], camera["sensitivity"], camera["fovy"], camera["lens radius"],
+                    camera["op distance"]], np.float32)
+    seg, nlv = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib().vlrref_bpt_render(
+        _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),
+        _p(flat["tris"]), ctypes.c_uint32(len(flat["tris"])), _p(flat["groupMaterial"]),
+        _p(flat["groupLightInst"]), ctypes.c_uint32(len(flat["groupMaterial"])), _p(flat["mats"]),
+        ctypes.c_uint32(len(flat["mats"])), _p(cam), ctypes.c_uint32(width), ctypes.c_uint32(height),
+        ctypes.c_uint32(frames), ctypes.c_uint32(max_path_length), ctypes.c_uint32(num_light_paths),
+        ctypes.c_int(threads), _p(state["eye"]), _p(state["light"]), _p(state["wl"]), _p(film),
+        ctypes.byref(seg), ctypes.byref(nlv))
+    assert rc == 0
+    return film, state, seg.value, nlv.value
+
+
 def pt_camera_rays(flat, camera, width, height, max_path_length, rng_states=None):
     """One frame of one sample per pixel (as pt_render) that also returns each
     pixel's camera ray and its brute-force closest hit: (film, rng_states,
@@ -134,6 +167,14 @@ def env_unsampleable():
     lib().vlrref_env_unsampleable(*[ctypes.byref(x) for x in v])
     return {"fp64_full": v[0].value, "fp32_full": v[1].value, "positive_full": v[2].value,
             "fp32_quarter": v[3].value, "positive_quarter": v[4].value}
+
+
+def last_render_seconds():
+    """Wall time of the last pt_render / bpt_render loop, scene set-up
+    (BVH build) excluded."""
+    f = lib().vlrref_last_render_seconds
+    f.restype = ctypes.c_double
+    return f()
 
 
 def seed_states(n, seed=591842031321323413):

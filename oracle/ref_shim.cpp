@@ -238,3 +238,4 @@ void vlrref_tables(const void** grid, const void** points, const float** cmf16, 
 }
 
 #include "ref_pt.inc"
+#include "ref_bpt.inc"

@@ -1032,12 +1032,15 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
             fp.blocksPerSM = options.blocksPerSM;
             if (renderer == VLRRenderer_BPT) {
                 // One frame per launch: all paths of a frame share its
-                // wavelength samples.  Light subpaths per frame default to a
-                // quarter of the pixel count and the cache holds one vertex
-                // per pixel (overflow is counted, see vlrbContextGetStats).
+                // wavelength samples.  Light subpaths per frame default to
+                // one per pixel path (the pixel count), and the cache holds
+                // ten vertices per light subpath, the reference's ratio
+                // (500,000 subpaths, 5,000,000 vertices: context.h:303,
+                // context.cpp:628); overflow is counted, see vlrbContextGetStats.
                 const uint32_t lightPaths = options.lightPathsPerFrame ? options.lightPathsPerFrame
-                                                                       : std::max<uint32_t>(1, pixels / 4);
-                const uint32_t capacity = std::max<uint32_t>(pixels, lightPaths);
+                                                                       : std::max<uint32_t>(1, pixels);
+                const uint32_t capacity = static_cast<uint32_t>(
+                    std::min<uint64_t>(uint64_t(10) * lightPaths, 0xFFFFFFFFull / 2));
                 if (bptCapacityPaths < lightPaths || bptCapacityVerts < capacity || bptEyeCapacity < pixels) {
                     bptCapacityPaths = lightPaths;
                     bptCapacityVerts = capacity;
