@@ -11,6 +11,8 @@
  *   VLRImmediateSpectrum      public_types.h:69-74
  *   VLRPoint3D ... Quaternion public_types.h:76-94
  *   VLRVertex (44 bytes)      public_types.h:107-112
+ *   VLR_PROCESS_CLASS_LIST    public_types.h:120-146 (the API's classes, in the
+ *                             order vlr.h and vlrcpp.h expand them)
  */
 #ifndef VLRB_PUBLIC_TYPES_H
 #define VLRB_PUBLIC_TYPES_H
@@ -111,5 +113,27 @@ struct VLRVertex {
 #if !defined(__cplusplus)
 typedef struct VLRVertex VLRVertex;
 #endif
+
+/* The classes of the API.  A user defines VLR_PROCESS_CLASS(Name) and expands
+ * the list (vlr.h declares a handle type per class, vlrcpp.h a holder). */
+#define VLR_PROCESS_CLASS_LIST() \
+    VLR_PROCESS_CLASS(Object); \
+    VLR_PROCESS_CLASS(ParameterInfo); \
+    VLR_PROCESS_CLASS(Queryable); \
+    VLR_PROCESS_CLASS(Image2D); \
+    VLR_PROCESS_CLASS(LinearImage2D); \
+    VLR_PROCESS_CLASS(BlockCompressedImage2D); \
+    VLR_PROCESS_CLASS(ShaderNode); \
+    VLR_PROCESS_CLASS(SurfaceMaterial); \
+    VLR_PROCESS_CLASS(Transform); \
+    VLR_PROCESS_CLASS(StaticTransform); \
+    VLR_PROCESS_CLASS(Node); \
+    VLR_PROCESS_CLASS(SurfaceNode); \
+    VLR_PROCESS_CLASS(TriangleMeshSurfaceNode); \
+    VLR_PROCESS_CLASS(PointSurfaceNode); \
+    VLR_PROCESS_CLASS(ParentNode); \
+    VLR_PROCESS_CLASS(InternalNode); \
+    VLR_PROCESS_CLASS(Scene); \
+    VLR_PROCESS_CLASS(Camera)
 
 #endif /* VLRB_PUBLIC_TYPES_H */

@@ -2,23 +2,27 @@
  *
  * Every function here replaces the reference entry point of the same name in
  * libVLR/include/vlr/vlr.h (line numbers given per block) with the same
- * signature, argument meaning and VLRResult error codes, so code written
- * against the reference (including its vlrcpp.h C++ wrapper) links against
- * this library unchanged.  Implementation: vlr_b200/csrc/vlr_api.cpp.
+ * signature, argument meaning and VLRResult error codes, at the same path
+ * (include/vlr/vlr.h, beside public_types.h, basic_types.h and vlrcpp.h), so
+ * code written against the reference, C or its vlrcpp.h C++ wrapper,
+ * compiles and links against this library unchanged.
+ * Implementation: vlr_b200/csrc/vlr_api.cu.
  *
  * Supported surface (everything else validates its arguments and returns
  * VLRResult_InvalidArgument for features this library does not render):
  *   context, output buffer (glTexID must be 0: no graphics interop),
- *   scenes, internal nodes, static transforms, triangle meshes,
- *   materials Matte, SpecularReflection, SpecularScattering,
+ *   scenes, internal nodes, static transforms, triangle meshes, point
+ *   nodes, materials Matte, SpecularReflection, SpecularScattering,
  *   MicrofacetReflection, MicrofacetScattering, LambertianScattering, UE4,
- *   DiffuseEmitter, EnvironmentEmitter; shader node EnvironmentTexture and
- *   immediate spectra; the Perspective camera; renderers PathTracing and BPT.
+ *   Multi, DiffuseEmitter, DirectionalEmitter, PointEmitter,
+ *   EnvironmentEmitter; shader nodes Image2DTexture, EnvironmentTexture and
+ *   immediate spectra; the Perspective and Equirectangular cameras;
+ *   renderers PathTracing, LightTracing and BPT.
  */
 #ifndef VLRB_VLR_H
 #define VLRB_VLR_H
 
-#include "vlr_public_types.h"
+#include "public_types.h"
 #include <cuda.h>
 
 #if defined(__cplusplus)
@@ -39,30 +43,14 @@ enum VLRResult {
 typedef enum VLRResult VLRResult;
 #endif
 
-/* Opaque handles (vlr.h:46-58, class list public_types.h:120-146). */
-#define VLRB_HANDLE(name) \
+/* Opaque handles (vlr.h:46-58): the context and every class of the list in
+ * public_types.h (VLR_PROCESS_CLASS_LIST). */
+#define VLR_PROCESS_CLASS(name) \
     typedef struct VLR##name##_API* VLR##name; \
     typedef const struct VLR##name##_API* VLR##name##Const
-VLRB_HANDLE(Context);
-VLRB_HANDLE(Object);
-VLRB_HANDLE(ParameterInfo);
-VLRB_HANDLE(Queryable);
-VLRB_HANDLE(Image2D);
-VLRB_HANDLE(LinearImage2D);
-VLRB_HANDLE(BlockCompressedImage2D);
-VLRB_HANDLE(ShaderNode);
-VLRB_HANDLE(SurfaceMaterial);
-VLRB_HANDLE(Transform);
-VLRB_HANDLE(StaticTransform);
-VLRB_HANDLE(Node);
-VLRB_HANDLE(SurfaceNode);
-VLRB_HANDLE(TriangleMeshSurfaceNode);
-VLRB_HANDLE(PointSurfaceNode);
-VLRB_HANDLE(ParentNode);
-VLRB_HANDLE(InternalNode);
-VLRB_HANDLE(Scene);
-VLRB_HANDLE(Camera);
-#undef VLRB_HANDLE
+VLR_PROCESS_CLASS(Context);
+VLR_PROCESS_CLASS_LIST();
+#undef VLR_PROCESS_CLASS
 #define VLR_TYPEDEF_DONE
 
 /* vlr.h:64 */

@@ -5,7 +5,7 @@
 #ifndef VLRB_VLRB_H
 #define VLRB_VLRB_H
 
-#include "vlr.h"
+#include "vlr/vlr.h"
 
 #if defined(__cplusplus)
 extern "C" {

@@ -25,7 +25,7 @@ def _lib():
 
 def header_functions():
     names = []
-    for h in ("vlr.h", "vlrb.h"):
+    for h in ("vlr/vlr.h", "vlrb.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         names += re.findall(r"^(?:VLRResult|const char\*)\s+(vlr\w+)\(", text, re.M)
     return names

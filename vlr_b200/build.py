@@ -52,6 +52,7 @@ def _compile(src, force):
     obj = os.path.join(OBJ, name + ".o")
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + [GEN]
     headers += glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    headers += glob.glob(os.path.join(HERE, "..", "include", "vlr", "*.h"))
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _newest([src] + headers):
         return obj, None
     cmd = [NVCC] + COMMON + (["-fmad=false"] if name in NO_FMA else []) + ["-c", src, "-o", obj]
