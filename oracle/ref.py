@@ -169,6 +169,22 @@ def env_unsampleable():
             "fp32_quarter": v[3].value, "positive_quarter": v[4].value}
 
 
+def pt_render_fp32_films(flat, camera, width, height, spp, max_path_length, rng_states=None, threads=0):
+    """pt_render that also feeds every contribution to two FP32 films: the
+    reference's own SpectrumStorage (FP32 Kahan pairs per stratum, summed per
+    sample) and a plain FP32 sum.  Returns (film64 [H,W,16], kahan_sum
+    [H,W,16], plain [H,W,16], rng_states)."""
+    kahan = np.zeros((height, width, 32), np.float32)
+    plain = np.zeros((height, width, 16), np.float32)
+    lib().vlrref_pt_set_fp32_films(_p(kahan), _p(plain))
+    try:
+        film, states, _ = pt_render(flat, camera, width, height, spp, max_path_length, rng_states=rng_states,
+                                    threads=threads)
+    finally:
+        lib().vlrref_pt_set_fp32_films(None, None)
+    return film, kahan[..., :16].copy(), plain, states
+
+
 def last_render_seconds():
     """Wall time of the last pt_render / bpt_render loop, scene set-up
     (BVH build) excluded."""

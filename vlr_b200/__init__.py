@@ -13,7 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvlr_b200.so")
 _lib = None
 
-# VLRResult codes (include/vlr.h)
+# VLRResult codes (include/vlr/vlr.h)
 NO_ERROR = 0
 INVALID_CONTEXT = 1
 INVALID_INSTANCE = 2

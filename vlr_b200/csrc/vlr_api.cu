@@ -1,4 +1,4 @@
-// The VLR C API (include/vlr.h) over the host object model.
+// The VLR C API (include/vlr/vlr.h) over the host object model.
 //
 // Error behaviour follows the reference's C layer (libVLR/vlr.cpp:13-34):
 // a null handle is VLRResult_InvalidArgument, a handle of the wrong kind is
