@@ -124,6 +124,8 @@ typedef struct VLRBRenderStats {
     uint64_t frames;              /* samples per pixel rendered since context creation */
     uint32_t lightVertexOverflow; /* LVC-BPT cache appends dropped for lack of capacity */
     uint32_t numTriangles;
+    uint32_t bvhMaxDepth;         /* internal nodes on the deepest root-to-leaf path of the scene's
+                                     hierarchy; never above the traversal stack (64) */
 } VLRBRenderStats;
 
 VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);

@@ -257,3 +257,64 @@ def test_seed_states_match_mt19937_64_recurrence():
     recurrence, including across the 312-word state refills."""
     for seed in (591842031321323413, 1, 0x9E3779B97F4A7C15):
         assert np.array_equal(ref.seed_states(1000, seed), ref.seed_states_py(1000, seed))
+
+
+def _max_leaf_depth(ch):
+    """Internal nodes on the deepest root-to-leaf path."""
+    n1 = len(ch) // 2
+    if n1 == 0:
+        return 0
+    depth = np.zeros(n1, np.int64)
+    best = 0
+    order = [0]
+    for x in order:                       # breadth first: parents before children
+        for c in (ch[2 * x], ch[2 * x + 1]):
+            if c >= 0:
+                depth[c] = depth[x] + 1
+                order.append(c)
+            else:
+                best = max(best, depth[x] + 1)
+    return best
+
+
+def test_lbvh_depth_stays_within_the_traversal_stack():
+    """The traversal keeps one stack entry per tree level (64 entries).  In
+    the Karras hierarchy every level splits at a longer common prefix of the
+    30-bit Morton code extended by the index, so a path has at most
+    30 + ceil(log2 n) internal nodes.  Inputs that reach for that bound:
+    centroids spaced by powers of two (one new Morton bit per level), each
+    repeated 64 times (index tie-break levels below), near-equal centroids,
+    and a uniform cloud.  The restructured trees of the same inputs stay
+    within the stack too (the build falls back to the plain LBVH when one
+    would not)."""
+    rng = np.random.default_rng(11)
+    pts = np.array([[2.0 ** -i, 2.0 ** -j, 2.0 ** -k] for i in range(11) for j in range(0, 11, 5)
+                    for k in range(0, 11, 5)])
+    cases = [pts, np.repeat(pts, 64, axis=0), np.zeros((4096, 3)), rng.uniform(-1, 1, (20000, 3))]
+    for c in cases:
+        n = len(c)
+        v = (c[:, None, :] + 1e-4 * rng.normal(size=(n, 3, 3))).astype(np.float32).reshape(n, 9)
+        codes, prims, ch, boxes = lbvh.build_lbvh(v)
+        d = _max_leaf_depth(ch)
+        assert d <= 30 + int(np.ceil(np.log2(n))) and d <= 64, (n, d)
+        och, obx, _ = lbvh.optimize_lbvh(v, prims, ch, boxes, 3)
+        assert _max_leaf_depth(och) <= 64
+
+
+@needs_ref
+def test_fp64_film_against_the_reference_fp32_kahan_film():
+    """The same contributions summed three ways by the CPU path tracer:
+    FP64 (the CUDA renderers' film), the reference's own FP32 SpectrumStorage
+    (Kahan pairs per stratum) and a plain FP32 sum.  On the Cornell box at
+    1024 spp the Kahan film stays within 2e-7 of FP64 per stratum and the
+    plain FP32 sum drifts further; at 512x512 and 4096 spp the figures are
+    1.1e-7 and 4.1e-6 (python -m oracle.film_precision)."""
+    from vlr_b200 import scenes
+    W = H = 32
+    desc = scenes.cornell_box_desc(W, H)
+    f64, kahan, plain, _ = ref.pt_render_fp32_films(scenes.flatten_desc(desc), desc["camera"], W, H, 1024, 8)
+    lit = f64 > 0
+    k_err = np.abs(kahan.astype(np.float64) - f64)[lit] / f64[lit]
+    p_err = np.abs(plain.astype(np.float64) - f64)[lit] / f64[lit]
+    assert k_err.max() < 2e-7, k_err.max()
+    assert p_err.max() > k_err.max()

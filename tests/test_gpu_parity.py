@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import vlr_b200 as V
-from oracle import ref, lbvh
+from oracle import ref, lbvh, triangle
 
 pytestmark = pytest.mark.gpu
 needs_ref = pytest.mark.skipif(not ref.available(), reason="reference host build (oracle/_ref) not built")
@@ -1071,37 +1071,30 @@ def _trace(v, rays, rounds, any_hit):
     return hits[:, 0], hits[:, 3].view(np.uint32)
 
 
-def _brute_force(v, rays):
-    """Closest hit per ray over every triangle (float64 Moller-Trumbore)."""
-    tri = v.reshape(-1, 3, 3).astype(np.float64)
-    a, e1, e2 = tri[:, 0], tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
-    best_t = np.full(len(rays), np.inf)
-    best = np.full(len(rays), 0xFFFFFFFF, np.uint32)
-    for i, r in enumerate(rays.astype(np.float64)):
-        o, tmax, d = r[0:3], r[3], r[4:7]
-        p = np.cross(d, e2)
-        det = np.einsum("ij,ij->i", e1, p)
-        with np.errstate(divide="ignore", invalid="ignore"):
-            inv = 1.0 / det
-            s = o - a
-            u = np.einsum("ij,ij->i", s, p) * inv
-            q = np.cross(s, e1)
-            w = (q @ d) * inv
-            t = np.einsum("ij,ij->i", e2, q) * inv
-        ok = (det != 0) & (u >= 0) & (u <= 1) & (w >= 0) & (u + w <= 1) & (t > 0) & (t < tmax)
-        if ok.any():
-            j = np.argmin(np.where(ok, t, np.inf))
-            best_t[i], best[i] = t[j], j
-    return best_t, best
+def _check_against_brute_force(v, rays):
+    """Closest and first hits through the plain LBVH and the restructured
+    hierarchy against the watertight test applied to every triangle
+    (oracle/triangle.py, the same float32 operations): the same hit/miss
+    answer for every ray (no hit lost, none invented), t bit-identical, the
+    same triangle wherever the closest t is unique."""
+    ref_t, ref_p, unique = triangle.closest_hits(v.reshape(-1, 3, 3), rays)
+    hit = ref_p != 0xFFFFFFFF
+    for rounds in (0, 3):
+        t, p = _trace(v, rays, rounds, False)
+        assert np.array_equal(p != 0xFFFFFFFF, hit), (rounds, np.flatnonzero((p != 0xFFFFFFFF) != hit)[:10])
+        assert np.array_equal(t[hit], ref_t[hit]), rounds
+        assert np.array_equal(p[hit & unique], ref_p[hit & unique]), rounds
+        _, a = _trace(v, rays, rounds, True)
+        assert np.array_equal(a != 0xFFFFFFFF, hit), rounds
+    return hit
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 37, 3000, 40000])
 def test_traversal_matches_brute_force(n):
-    """Closest and first hits through the plain LBVH and the restructured
-    hierarchy (vlrbTraceRaysHost) against a brute-force search over every
-    triangle: no hit lost, the same closest triangle for every ray the brute
-    force resolves away from float ties, the same hit/miss answer for the
-    any-hit query, and both hierarchies agree."""
+    """Triangle soups of 1 to 40,000 triangles, rays from random origins in
+    random directions (a tenth with an axis-parallel component, a third
+    shortened) and aimed at triangle centroids: no hit lost against the
+    brute-force search, t bit-identical (see _check_against_brute_force)."""
     rng = np.random.default_rng(500 + n)
     scale = np.exp(rng.uniform(-3, 0, (n, 1, 1)))
     v = (rng.uniform(-1, 1, (n, 1, 3)) + 0.2 * scale * rng.normal(0, 1, (n, 3, 3))).astype(np.float32).reshape(n, 9)
@@ -1114,21 +1107,69 @@ def test_traversal_matches_brute_force(n):
     d[: m // 10, 1] = 0.0                                  # axis-parallel components
     rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
     rays[:, 3] = np.where(np.arange(m) % 3 == 0, 0.8, 3.4e38)   # some short rays
-    t0, p0 = _trace(v, rays, 0, False)
-    t3, p3 = _trace(v, rays, 3, False)
-    ref_t, ref_p = _brute_force(v, rays)
-    hit = ref_p != 0xFFFFFFFF
+    hit = _check_against_brute_force(v, rays)
     assert hit.sum() >= m // 4
-    for t, p in ((t0, p0), (t3, p3)):
-        assert np.sum(hit & (p == 0xFFFFFFFF)) <= 1
-        assert np.mean((p != 0xFFFFFFFF) == hit) >= 0.999
-        resolved = hit & (np.abs(t - ref_t) <= 1e-4 * np.maximum(ref_t, 1e-3))
-        assert np.mean(resolved[hit]) >= 0.995
-    same = p0 == p3
-    assert np.mean(same) >= 0.999
-    assert np.array_equal(t0[same], t3[same])
-    _, a3 = _trace(v, rays, 3, True)
-    assert np.mean((a3 != 0xFFFFFFFF) == hit) >= 0.999
+
+
+def _icosphere(subdivisions):
+    """Closed triangle mesh of a sphere of radius 0.75: every edge is shared
+    by two triangles that hold its two vertices as the same float32 values."""
+    t = (1.0 + 5 ** 0.5) / 2
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                p = verts[a] + verts[b]
+                verts.append(p / np.linalg.norm(p))
+                mid[key] = len(verts) - 1
+            return mid[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    vs = np.array(verts, np.float32) * np.float32(0.75)
+    return vs, np.array(faces, np.int64)
+
+
+def test_closed_mesh_leaks_no_ray():
+    """Watertightness: rays from the centre of a closed icosphere (1,280
+    triangles) aimed exactly at its vertices (direction = the vertex, so the
+    ray passes through the shared vertex; several have zero direction
+    components and start on box faces) and at its edges' midpoints, plus
+    random directions from random interior points, all hit the mesh in both
+    hierarchies, and t equals the brute-force search bit for bit.  A float32
+    Moller-Trumbore test lets 332 of the 2,562 vertex and edge rays through."""
+    vs, faces = _icosphere(3)
+    v = vs[faces].reshape(-1, 9)
+    rng = np.random.default_rng(9)
+    edges = np.unique(np.sort(np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]]), axis=1), axis=0)
+    dirs = [vs.astype(np.float32),                                   # through each vertex from the centre
+            (vs[edges[:, 0]] + vs[edges[:, 1]]).astype(np.float32)]  # towards each edge's midpoint
+    rays = []
+    for d in dirs:
+        r = np.zeros((len(d), 8), np.float32)
+        r[:, 3] = 3.4e38
+        r[:, 4:7] = d
+        rays.append(r)
+    m = 2000
+    r = np.zeros((m, 8), np.float32)
+    r[:, 0:3] = rng.uniform(-0.3, 0.3, (m, 3))
+    d = rng.normal(size=(m, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    r[:, 3] = 3.4e38
+    rays.append(r)
+    rays = np.concatenate(rays)
+    hit = _check_against_brute_force(v, rays)
+    assert hit.all(), np.flatnonzero(~hit)[:10]
 
 
 def test_guide_buffers_hold_first_hit_albedo_and_camera_space_normal():

@@ -183,7 +183,7 @@ extern "C" VLRResult vlrbTraceRaysHost(const float* triVerts, uint32_t n, uint32
         for (int i = 0; i < 9; ++i) { off[i] = total; total += a256(sizes[i]); }
         off[9] = total;
         total += 256;
-        const size_t scratchBytes = std::max(vlrb::lbvhScratchBytes(n), vlrb::lbvhOptimizeScratchBytes(n));
+        const size_t scratchBytes = vlrb::lbvhTraversableScratchBytes(n);
         DevBuf out, scratch;
         if (out.alloc(total) != cudaSuccess || scratch.alloc(scratchBytes) != cudaSuccess)
             return VLRResult_InternalError;
@@ -195,8 +195,8 @@ extern "C" VLRResult vlrbTraceRaysHost(const float* triVerts, uint32_t n, uint32
                              reinterpret_cast<int32_t*>(b + off[3]), reinterpret_cast<float*>(b + off[4]),
                              reinterpret_cast<vlrb::BvhNode*>(b + off[5]), reinterpret_cast<vlrb::BvhTri*>(b + off[6]) };
         uint32_t* flags = reinterpret_cast<uint32_t*>(b + off[9]);
-        vlrb::lbvhBuild(reinterpret_cast<const float*>(b + off[0]), n, scratch.p, &lo, nullptr);
-        vlrb::lbvhOptimize(n, treeletRounds, scratch.p, &lo, nullptr, nullptr);
+        vlrb::lbvhBuildTraversable(reinterpret_cast<const float*>(b + off[0]), n, treeletRounds, scratch.p, &lo,
+                                   nullptr, nullptr);
         const vlrb::Bvh bvh{ lo.nodes, lo.tris, n, flags };
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);

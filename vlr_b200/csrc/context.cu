@@ -774,9 +774,9 @@ void Context::buildScene(cudaStream_t stream) {
         LbvhOutput lo{ reinterpret_cast<uint32_t*>(b + off[0]), reinterpret_cast<uint32_t*>(b + off[1]),
                        reinterpret_cast<int32_t*>(b + off[2]), reinterpret_cast<float*>(b + off[3]),
                        reinterpret_cast<BvhNode*>(b + off[4]), reinterpret_cast<BvhTri*>(b + off[5]) };
-        lbvhScratch.resize(std::max(lbvhScratchBytes(numTris), lbvhOptimizeScratchBytes(numTris)));
-        lbvhBuild(dVerts, numTris, lbvhScratch.ptr, &lo, stream);
-        lbvhOptimize(numTris, options.bvhTreeletRounds, lbvhScratch.ptr, &lo, nullptr, stream);
+        lbvhScratch.resize(lbvhTraversableScratchBytes(numTris));
+        bvhMaxDepth = lbvhBuildTraversable(dVerts, numTris, options.bvhTreeletRounds, lbvhScratch.ptr, &lo, nullptr,
+                                           stream);
         auto flag = std::make_unique<DeviceBuffer>();
         flag->resize(256);
         ck(cudaMemsetAsync(flag->ptr, 0, 4, stream), "bvh flag");

@@ -111,6 +111,7 @@ public:
                      reinterpret_cast<uint32_t*>(static_cast<char*>(film.ptr) + size_t(width) * height * kNumStrata * 8) };
     }
     uint32_t numTriangles() const { return sg.numTris; }
+    uint32_t bvhDepth() const { return bvhMaxDepth; }
     uint32_t guideSamplesRecorded() const;
 
     CUcontext cuContext;
@@ -161,6 +162,7 @@ private:
     };
     std::vector<std::unique_ptr<SceneTexture>> sceneTextures;
     DeviceBuffer film, output, pathMem, lbvhScratch, bptMem, auxMem;
+    uint32_t bvhMaxDepth = 0;          // deepest leaf of the scene's hierarchy (internal nodes on its path)
     AuxBuffers aux{};
     uint32_t auxSamples = 0;       // guide samples accumulated since the buffers were cleared
     uint64_t auxSeed = 0;

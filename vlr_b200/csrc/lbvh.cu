@@ -270,11 +270,10 @@ __global__ void packTrisKernel(const float* verts, const uint32_t* sortedPrims, 
     if (i >= n) return;
     uint32_t p = sortedPrims[i];
     V3 a = loadVertex(verts, p, 0), b = loadVertex(verts, p, 1), c = loadVertex(verts, p, 2);
-    V3 e1 = b - a, e2 = c - a;
     BvhTri t;
     t.v0 = make_float4(a.x, a.y, a.z, __uint_as_float(p));
-    t.e1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
-    t.e2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+    t.v1 = make_float4(b.x, b.y, b.z, 0.0f);
+    t.v2 = make_float4(c.x, c.y, c.z, 0.0f);
     tris[i] = t;
 }
 
@@ -592,6 +591,24 @@ void lbvhBuild(const float* verts, uint32_t n, void* scratch, LbvhOutput* out, c
     ck(cudaGetLastError(), "launch");
 }
 
+// Leaf depth (internal nodes on the root path) by walking the parent links
+// up; the maximum over all leaves lands in *maxDepth.  A walk longer than n
+// steps (a malformed tree) stops there and reports n + 1.
+__global__ void leafDepthKernel(const int32_t* parentOfNode, const int32_t* parentOfLeaf, uint32_t n,
+                                uint32_t* maxDepth) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t d = 0;
+    if (i < n) {
+        int node = parentOfLeaf[i];
+        while (node >= 0 && d <= n) {
+            ++d;
+            node = parentOfNode[node];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xFFFFFFFFu, d, o));
+    if ((threadIdx.x & 31u) == 0 && d > 0) atomicMax(maxDepth, d);
+}
+
 size_t lbvhOptimizeScratchBytes(uint32_t n) {
     return 5 * align256(size_t(n) * 4) + 256;
 }
@@ -622,6 +639,45 @@ void lbvhOptimize(uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out, u
         gamma *= 2;
     }
     ck(cudaGetLastError(), "treelet launch");
+}
+
+uint32_t lbvhMaxLeafDepth(uint32_t n, const int32_t* children, void* scratch, cudaStream_t stream) {
+    if (n < 2) return 0;
+    char* s = static_cast<char*>(scratch);
+    auto take = [&](size_t bytes) { char* p = s; s += align256(bytes); return p; };
+    int32_t* parentOfNode = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    int32_t* parentOfLeaf = reinterpret_cast<int32_t*>(take(size_t(n) * 4));
+    uint32_t* maxDepth = reinterpret_cast<uint32_t*>(take(4));
+    const uint32_t tb = 256;
+    ck(cudaMemsetAsync(parentOfLeaf, 0xFF, size_t(n) * 4, stream), "leaf parents");
+    ck(cudaMemsetAsync(parentOfNode, 0xFF, size_t(n) * 4, stream), "node parents");
+    ck(cudaMemsetAsync(maxDepth, 0, 4, stream), "depth");
+    parentsKernel<<<(n - 1 + tb - 1) / tb, tb, 0, stream>>>(children, static_cast<int>(n), parentOfNode, parentOfLeaf);
+    leafDepthKernel<<<(n + tb - 1) / tb, tb, 0, stream>>>(parentOfNode, parentOfLeaf, n, maxDepth);
+    ck(cudaGetLastError(), "depth launch");
+    uint32_t depth = 0;
+    ck(cudaMemcpyAsync(&depth, maxDepth, 4, cudaMemcpyDeviceToHost, stream), "depth readback");
+    ck(cudaStreamSynchronize(stream), "depth sync");
+    return depth;
+}
+
+size_t lbvhTraversableScratchBytes(uint32_t n) {
+    const size_t a = lbvhScratchBytes(n), b = lbvhOptimizeScratchBytes(n);
+    return a > b ? a : b;
+}
+
+uint32_t lbvhBuildTraversable(const float* verts, uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out,
+                              uint32_t* restructuredDev, cudaStream_t stream) {
+    lbvhBuild(verts, n, scratch, out, stream);
+    if (rounds == 0 || n < 3) return lbvhMaxLeafDepth(n, out->children, scratch, stream);
+    lbvhOptimize(n, rounds, scratch, out, restructuredDev, stream);
+    const uint32_t depth = lbvhMaxLeafDepth(n, out->children, scratch, stream);
+    if (depth <= static_cast<uint32_t>(kTraversalStack)) return depth;
+    // Restructuring deepened a path past the traversal stack: use the plain
+    // LBVH, whose depth the key bits bound (at most 30 + 32 levels).
+    lbvhBuild(verts, n, scratch, out, stream);
+    if (restructuredDev) ck(cudaMemsetAsync(restructuredDev, 0, 4, stream), "treelet counter");
+    return lbvhMaxLeafDepth(n, out->children, scratch, stream);
 }
 
 } // namespace vlrb

@@ -30,4 +30,19 @@ size_t lbvhOptimizeScratchBytes(uint32_t n);
 void lbvhOptimize(uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out, uint32_t* restructuredDev,
                   cudaStream_t stream);
 
+// Largest number of internal nodes on a root-to-leaf path of the hierarchy
+// in `children` (synchronises `stream`).  scratch: lbvhOptimizeScratchBytes(n).
+uint32_t lbvhMaxLeafDepth(uint32_t n, const int32_t* children, void* scratch, cudaStream_t stream);
+
+// The hierarchy the traversal walks: lbvhBuild, then `rounds` of
+// lbvhOptimize; if restructuring left a leaf deeper than kTraversalStack
+// levels, the plain LBVH is built again instead.  Its depth is bounded by the
+// key: each level of the Karras hierarchy splits at a longer common prefix of
+// the 30-bit Morton code extended by the 32-bit index, so no path holds more
+// than 62 internal nodes and the traversal stack (one entry per level) cannot
+// overflow.  Returns the maximum leaf depth (synchronises `stream`).
+size_t lbvhTraversableScratchBytes(uint32_t n);
+uint32_t lbvhBuildTraversable(const float* verts, uint32_t n, uint32_t rounds, void* scratch, LbvhOutput* out,
+                              uint32_t* restructuredDev, cudaStream_t stream);
+
 } // namespace vlrb

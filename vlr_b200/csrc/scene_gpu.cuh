@@ -418,6 +418,7 @@ __device__ __forceinline__ float hashUniform(uint64_t seed, uint32_t prim) {
 // from the path's RNG state mixed with the primitive, so it does not advance
 // the path's stream and a ray meets each triangle with one decision.
 struct StochasticAlpha {
+    static constexpr bool kNeedsBarycentrics = true;
     const SceneGPU* S;
     uint64_t seed;
     __device__ __forceinline__ bool operator()(uint32_t prim, float b1, float b2) const {
@@ -430,6 +431,7 @@ struct StochasticAlpha {
 // visibility is the product of (1 - alpha) over the surfaces the segment
 // crosses; an intersection ends the ray once that product reaches 0.
 struct AlphaVisibility {
+    static constexpr bool kNeedsBarycentrics = true;
     const SceneGPU* S;
     float visibility;
     __device__ __forceinline__ bool operator()(uint32_t prim, float b1, float b2) {

@@ -1387,6 +1387,7 @@ VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats) {
     stats->frames = s.frames;
     stats->lightVertexOverflow = s.lightVertexOverflow;
     stats->numTriangles = c->numTriangles();
+    stats->bvhMaxDepth = c->bvhDepth();
     return VLRResult_NoError;
     API_CATCH("vlrbContextGetStats")
 }

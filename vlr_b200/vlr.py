@@ -44,7 +44,8 @@ class VLRBAutotuneTrial(ctypes.Structure):
 
 class VLRBRenderStats(ctypes.Structure):
     _fields_ = [("pathSegments", ctypes.c_uint64), ("shadowRays", ctypes.c_uint64), ("frames", ctypes.c_uint64),
-                ("lightVertexOverflow", ctypes.c_uint32), ("numTriangles", ctypes.c_uint32)]
+                ("lightVertexOverflow", ctypes.c_uint32), ("numTriangles", ctypes.c_uint32),
+                ("bvhMaxDepth", ctypes.c_uint32)]
 
 
 class VLRBGuidingOptions(ctypes.Structure):
