@@ -192,9 +192,10 @@ def run_reference(args):
 RMSE_W = RMSE_H = 1024
 RMSE_BLOCK = 8
 RMSE_TARGET = 0.01
-RMSE_REF_SPP = 4096
+RMSE_REF_SPP = 16384
 RMSE_CHUNK_SPP = 16
 RMSE_CAP_S = 40.0
+RMSE_PIXEL_TARGET = 0.10
 
 
 class _FilmView:
@@ -215,13 +216,17 @@ def _cmf_y():
 
 def time_to_rmse():
     """Device time until the image is within RMSE_TARGET of an FP64 plain-PT
-    reference (RMSE_REF_SPP spp, independent RNG seed), for plain and for
-    guided path tracing with online training included in the time.  Error:
-    RMSE of RMSE_BLOCK^2-pixel block means of CIE Y, relative to the
-    reference mean (block means keep the reference's own noise well below
-    the target).  A method that has not reached the target after RMSE_CAP_S
-    seconds reports its error there and an extrapolated time assuming error
-    ~ 1/sqrt(time)."""
+    reference (RMSE_REF_SPP spp in two independently seeded halves), for
+    plain and for guided path tracing with online training included in the
+    time.  Error: RMSE of RMSE_BLOCK^2-pixel block means of CIE Y, relative
+    to the reference mean; beside it the per-pixel relative RMSE of CIE Y at
+    every checkpoint and the time to RMSE_PIXEL_TARGET per pixel (a per-pixel
+    1% needs far more samples than either method renders in the cap).  The
+    reference's own variance, a quarter of the halves' mean squared
+    difference, is subtracted from every squared error, per block and per
+    pixel.  A method that has not reached a target after RMSE_CAP_S seconds
+    reports its error there and an extrapolated time assuming error ~
+    1/sqrt(time)."""
     import torch
     from vlr_b200 import vlr as V, scenes
     W, H, b = RMSE_W, RMSE_H, RMSE_BLOCK
@@ -242,9 +247,11 @@ def time_to_rmse():
             ctx.setGuiding(enabled=True, train=True, recordBounces=1, warmupLaunches=1, trainInterval=4)
         return ctx, cam, keep
 
-    def blocks(ctx):
+    def pixels(ctx):
         f = torch.as_tensor(_FilmView(ctx.film_device_ptr(), W * H * 16), device="cuda").view(H, W, 16)
-        y = f @ cy
+        return f @ cy
+
+    def blocks(y):
         return y.view(H // b, b, W // b, b).mean(dim=(1, 3))
 
     # the reference in two independent halves: their difference measures the
@@ -252,20 +259,26 @@ def time_to_rmse():
     halves = []
     for seed in (0x9E3779B97F4A7C15, 0xD1B54A32D192ED03):
         ctx, cam, keep = make(False, seed)
-        ctx.render_samples(cam, True, RMSE_REF_SPP // 2)
-        halves.append(blocks(ctx) / (RMSE_REF_SPP // 2))
+        for k in range(RMSE_REF_SPP // 2 // 1024):
+            ctx.render_samples(cam, k == 0, 1024)
+        halves.append(pixels(ctx) / (RMSE_REF_SPP // 2))
         torch.cuda.synchronize()
         ctx.close()
-    ref = 0.5 * (halves[0] + halves[1])
-    ref_var = (torch.mean((halves[0] - halves[1]) ** 2) / 4).item()
+    ref_px = 0.5 * (halves[0] + halves[1])
+    ref_var_px = (torch.mean((halves[0] - halves[1]) ** 2) / 4).item()
+    ref = blocks(ref_px)
+    ref_var = (torch.mean((blocks(halves[0]) - blocks(halves[1])) ** 2) / 4).item()
     ref_mean = ref.mean().item()
     out = {"scene": "Cornell box, 20,022-triangle GGX dielectric sphere (IOR 1.5, roughness 0.02), light 0.1x area",
            "resolution": [W, H], "max_path_length": MAX_PATH_LENGTH, "target": RMSE_TARGET,
            "error": f"RMSE of {b}x{b}-pixel block means of CIE Y / reference mean",
+           "pixel_error": "RMSE of per-pixel CIE Y / reference mean (curve entries' fourth value)",
+           "pixel_target": RMSE_PIXEL_TARGET,
            "reference": f"plain PT, {RMSE_REF_SPP} spp in two independently seeded halves, FP64 film; "
                         f"the reference's own variance (a quarter of the halves' mean squared difference) is "
                         f"subtracted from each squared error",
            "reference_noise": None,
+           "reference_pixel_noise": None,
            "dielectric_pdf": "consistent (the reference's MicrofacetScattering pdf is 0 for exits: "
                              "NEE double counting and fireflies)",
            "guided_config": "hash grid 16x2x2^19, 3x64 BF16 MLP, 8 vMF lobes, Adam lr 1e-2, 2^18 samples per "
@@ -273,6 +286,7 @@ def time_to_rmse():
                             "one warm-up launch of 16 spp, then one step every 4 launches (64 spp); training time "
                             "included"}
     out["reference_noise"] = math.sqrt(ref_var) / ref_mean
+    out["reference_pixel_noise"] = math.sqrt(ref_var_px) / ref_mean
     for name, guided in (("plain", False), ("guided", True)):
         ctx, cam, keep = make(guided, 0)
         stream = torch.cuda.current_stream()
@@ -281,6 +295,7 @@ def time_to_rmse():
         n = 0
         curve = []
         reached = None
+        pixel_reached = None
         while t < RMSE_CAP_S:
             e0.record(stream)
             ctx.render_samples(cam, n == 0, RMSE_CHUNK_SPP, stream=stream.cuda_stream)
@@ -288,16 +303,24 @@ def time_to_rmse():
             e1.synchronize()
             t += e0.elapsed_time(e1) * 1e-3
             n += RMSE_CHUNK_SPP
-            mse = torch.mean((blocks(ctx) / n - ref) ** 2).item()
+            y = pixels(ctx) / n
+            mse = torch.mean((blocks(y) - ref) ** 2).item()
             err = math.sqrt(max(mse - ref_var, 0.0)) / ref_mean
+            mse_px = torch.mean((y - ref_px) ** 2).item()
+            err_px = math.sqrt(max(mse_px - ref_var_px, 0.0)) / ref_mean
+            if pixel_reached is None and err_px <= RMSE_PIXEL_TARGET:
+                pixel_reached = t
             if n in (16, 64, 256, 1024, 4096, 8192) or err <= RMSE_TARGET:
-                curve.append([n, round(t, 4), err])
+                curve.append([n, round(t, 4), err, err_px])
             if err <= RMSE_TARGET:
                 reached = t
                 break
-        r = {"seconds": reached, "spp": n, "error_at_end": err, "seconds_at_end": t, "curve": curve}
+        r = {"seconds": reached, "spp": n, "error_at_end": err, "pixel_error_at_end": err_px,
+             "seconds_at_end": t, "seconds_to_pixel_target": pixel_reached, "curve": curve}
         if reached is None:
             r["seconds_extrapolated"] = t * (err / RMSE_TARGET) ** 2
+        if pixel_reached is None:
+            r["seconds_to_pixel_target_extrapolated"] = t * (err_px / RMSE_PIXEL_TARGET) ** 2
         if guided:
             r["guiding"] = ctx.guiding_stats()
         seg = ctx.stats()["pathSegments"]
@@ -307,6 +330,9 @@ def time_to_rmse():
     tp = out["plain"]["seconds"] or out["plain"]["seconds_extrapolated"]
     tg = out["guided"]["seconds"] or out["guided"]["seconds_extrapolated"]
     out["guided_over_plain"] = tg / tp
+    pp = out["plain"]["seconds_to_pixel_target"] or out["plain"]["seconds_to_pixel_target_extrapolated"]
+    pg = out["guided"]["seconds_to_pixel_target"] or out["guided"]["seconds_to_pixel_target_extrapolated"]
+    out["guided_over_plain_pixel"] = pg / pp
     return out
 
 
@@ -440,11 +466,13 @@ def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True):
         ms = e0.elapsed_time(e1)
         seg = ctx.stats()["pathSegments"] - s0
         st = ctx.stats()
-        # per-stage device times of one more sample of the same frame
+        # per-stage device times of one more call of the same size (stage
+        # events serialise the stages a little: they sum to slightly more than
+        # the timed call), reported per spp
         ctx.set_profiling(True)
         ctx.kernel_times(reset=True)
         q0 = ctx.stats()
-        ctx.render_samples(cam, False, 1, stream=stream.cuda_stream)
+        ctx.render_samples(cam, False, spp, stream=stream.cuda_stream)
         torch.cuda.synchronize()
         stages, _ = ctx.kernel_times(reset=True)
         q1 = ctx.stats()
@@ -455,7 +483,7 @@ def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True):
                          f"sky with sun (FP64 CDF)",
              "triangles": st["numTriangles"], "segments_per_s": seg / (ms * 1e-3) / 1e9,
              "unit": "G path segments/s", "ms": ms,
-             "stage_ms_per_spp": {k: v["ms"] for k, v in stages.items() if v["ms"] > 0}}
+             "stage_ms_per_spp": {k: v["ms"] / spp for k, v in stages.items() if v["ms"] > 0}}
         if renderer == V.RENDERER_PATH_TRACING:
             dom = max(("trace", "shade", "shadow"), key=lambda k: stages[k]["ms"])
             units = rays if dom != "shadow" else q1["shadowRays"] - q0["shadowRays"]
@@ -586,6 +614,7 @@ WORKLOADS = {
     "glossy_guided": lambda: {"glossy_guided": glossy_guided_workload()},
     "light_tracing": lambda: {"light_tracing": light_tracing_workload()},
     "denoise": lambda: {"denoise": denoise_workload()},
+    "time_to_rmse": lambda: {"time_to_rmse": time_to_rmse()},
 }
 
 
@@ -852,6 +881,18 @@ def main():
             except Exception as ex:  # reported, never fatal for the GPU line
                 base = {"error": str(ex)}
         launches_per_step = launches / args.steps
+        # the metric's own targets, each on the workload it is stated for
+        targets = {}
+        tpw = workloads.get("terrain_pt") if isinstance(workloads, dict) else None
+        if tpw:
+            targets["terrain_pt_segments_per_s"] = {
+                "value": tpw["segments_per_s"], "target": 2.0, "unit": UNIT, "higher_is_better": True,
+                "workload": f"{tpw['workload']}, {tpw['triangles']} triangles"}
+        if isinstance(rmse, dict) and "guided_over_plain" in rmse:
+            targets["guided_over_plain_time_to_1pct"] = {
+                "value": rmse["guided_over_plain"], "target": 0.5, "unit": "ratio of device seconds",
+                "higher_is_better": False, "workload": rmse["scene"],
+                "per_pixel_ratio": rmse.get("guided_over_plain_pixel")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -873,6 +914,7 @@ def main():
             "gpu_launches": int(launches),
             "gpu_launches_per_step": launches_per_step,
             "clocks": clocks.summary(),
+            "targets": targets,
             "time_to_rmse": rmse,
             "workloads": workloads,
         }
