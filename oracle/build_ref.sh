@@ -39,6 +39,22 @@ sed -E \
     -e 's/^([[:space:]]*)(float DiscretizedSpectrumTemplate<float, NumStrataForStorage>::integralCMF);/\1template <> \2 = 0.0f;/' \
     "$REF/libVLR/shared/spectrum_types.cpp" > "$MIR/shared/spectrum_types.cpp"
 
+# FP64 oracle copy (ref_shim64.cpp): the patched file without the FP32
+# Meng-Simon tables and the FP32 explicit instantiations, which clash with the
+# FP64 ones once every float is compiled as double.
+python3 - "$MIR/shared/spectrum_types.cpp" "$MIR/shared/spectrum_types64.cpp" <<'PYEOF'
+import sys
+lines = open(sys.argv[1]).read().split("\n")
+def table_start(real):
+    key = "UpsampledSpectrumTemplate<%s, NumSpectralSamples>::spectrum_grid_cell_t" % real
+    i = next(k for k, l in enumerate(lines) if key in l)
+    return i - 1 if lines[i - 1].strip() == "template <>" else i
+a, b = table_start("float"), table_start("double")
+assert a < b
+out = [l for l in lines[:a] + lines[b:] if not (l.strip().startswith("template class") and "<float," in l)]
+open(sys.argv[2], "w").write("\n".join(out))
+PYEOF
+
 ln -s "$REF/libVLR/include/vlr" "$MIR/include/vlr"
 ln -s "$REF/libVLR/include/vlr" "$MIR/include/VLR"
 ln -s "$REF/libVLR/GPU_kernels/materials.cu" "$MIR/GPU_kernels/materials.cu"
@@ -56,3 +72,10 @@ FLAGS=(-std=c++20 -O2 -fPIC -fopenmp -DVLR_USE_SPECTRAL_RENDERING -mlzcnt -mpopc
 "$CXX" -shared -fopenmp -o "$OUT/libvlrref.so" \
     "$OUT/obj/ref_shim.o" "$OUT/obj/spectrum_base.o" "$OUT/obj/spectrum_types.o"
 echo "built $OUT/libvlrref.so"
+
+# The FP64 oracle: the same reference sources with every float compiled as
+# double (ref_shim64.cpp), in a library of its own; -Bsymbolic keeps its
+# classes bound to themselves when both libraries are loaded.
+"$CXX" "${FLAGS[@]}" -I "$HERE" -x c++ -c "$HERE/ref_shim64.cpp" -o "$OUT/obj/ref_shim64.o"
+"$CXX" -shared -fopenmp -Wl,-Bsymbolic -o "$OUT/libvlrref64.so" "$OUT/obj/ref_shim64.o"
+echo "built $OUT/libvlrref64.so"

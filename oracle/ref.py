@@ -40,6 +40,31 @@ def bsdf_batch(inputs, threads=0):
     return outs
 
 
+REF64_LIB = os.path.join(HERE, "_ref", "libvlrref64.so")
+_lib64 = None
+
+
+def available64():
+    return os.path.exists(REF64_LIB)
+
+
+def bsdf_batch64(inputs, threads=0):
+    """The same batch through the FP64 build of the reference's BSDF and
+    spectral classes (oracle/ref_shim64.cpp: every float of the reference
+    sources compiled as double; FP32 inputs widened exactly).  Returns
+    float64 outputs."""
+    global _lib64
+    if _lib64 is None:
+        _lib64 = ctypes.CDLL(REF64_LIB)
+        _lib64.vlrref64_init()
+    n = len(inputs["material"])
+    ins = [np.ascontiguousarray(inputs[k]) for k in BATCH_INPUTS]
+    outs = {k: np.zeros((n, c) if c > 1 else n, np.float64) for k, c in BATCH_OUTPUTS.items()}
+    _lib64.vlrref64_bsdf_batch(ctypes.c_int64(n), ctypes.c_int(threads), *[_p(a) for a in ins],
+                               *[_p(outs[k]) for k in BATCH_OUTPUTS])
+    return outs
+
+
 def upsample(sp_type, color_space, e0, e1, e2):
     out = (ctypes.c_uint32 * 3)()
     lib().vlrref_upsample(sp_type, color_space, ctypes.c_float(e0), ctypes.c_float(e1),

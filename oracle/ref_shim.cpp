@@ -63,44 +63,14 @@ using namespace vlr;
 using namespace vlr::shared;
 
 namespace {
-    // Material ids of the BSDF batch workload.
-    enum : uint32_t {
-        kMatte = 0, kSpecularBRDF = 1, kMicrofacetBRDF = 2,
-        kMicrofacetBSDF = 3, kLambertianBSDF = 4, kUE4 = 5, kSpecularBSDF = 6,
-    };
-
-    struct Packed {
-        uint32_t w[3];
-    };
-
     inline UpsampledSpectrum unpack(const uint32_t p[3]) {
         UpsampledSpectrum s;
         std::memcpy(&s, p, sizeof(UpsampledSpectrum));
         return s;
     }
-
-    template <typename BSDFType>
-    void runQuery(const BSDFType &bsdf, const BSDFQuery &query, const float u[3],
-                  float* value4, float* pdf, float* wi3, float* evalValue4, float* evalPdf) {
-        BSDFQueryResult result;
-        result.dirPDF = 0.0f;
-        result.dirLocal = Vector3D(0.0f, 0.0f, 0.0f);
-        const float uDir[2] = { u[1], u[2] };
-        SampledSpectrum fs = bsdf.sampleInternal(query, u[0], uDir, &result);
-        if (!(result.dirPDF > 0.0f)) {
-            for (int i = 0; i < 4; ++i) { value4[i] = 0.0f; evalValue4[i] = 0.0f; }
-            *pdf = 0.0f; *evalPdf = 0.0f;
-            wi3[0] = wi3[1] = wi3[2] = 0.0f;
-            return;
-        }
-        for (int i = 0; i < 4; ++i) value4[i] = fs[i];
-        *pdf = result.dirPDF;
-        wi3[0] = result.dirLocal.x; wi3[1] = result.dirLocal.y; wi3[2] = result.dirLocal.z;
-        SampledSpectrum ev = bsdf.evaluateInternal(query, result.dirLocal);
-        for (int i = 0; i < 4; ++i) evalValue4[i] = ev[i];
-        *evalPdf = bsdf.evaluatePDFInternal(query, result.dirLocal);
-    }
 }
+
+#include "ref_bsdf_batch.inc"
 
 extern "C" {
 
@@ -136,81 +106,7 @@ void vlrref_bsdf_batch(
     const float* wo, const uint32_t* mat, const float* rough, const float* ior,
     const float* rgb, const float* metallic, const float* u, const float* wl,
     float* value, float* pdf, float* wi, float* evalValue, float* evalPdf) {
-    if (numThreads > 0)
-        omp_set_num_threads(numThreads);
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < n; ++i) {
-        float wlPDF;
-        WavelengthSamples wls = WavelengthSamples::createWithEqualOffsets(wl[2 * i + 0], wl[2 * i + 1], &wlPDF);
-        const Vector3D dirLocal(wo[3 * i + 0], wo[3 * i + 1], wo[3 * i + 2]);
-        BSDFQuery query(dirLocal, Normal3D(0.0f, 0.0f, 1.0f), TransportMode::Radiance,
-                        DirectionType::All(), wls);
-        const float* ui = u + 3 * i;
-        float* v4 = value + 4 * i;
-        float* p1 = pdf + i;
-        float* w3 = wi + 3 * i;
-        float* e4 = evalValue + 4 * i;
-        float* ep = evalPdf + i;
-
-        UpsampledSpectrum albedoSp(SpectrumType::Reflectance, ColorSpace::Rec709_D65,
-                                   rgb[3 * i + 0], rgb[3 * i + 1], rgb[3 * i + 2]);
-        UpsampledSpectrum iorSp(SpectrumType::IndexOfRefraction, ColorSpace::Rec709_D65,
-                                ior[i], ior[i], ior[i]);
-        UpsampledSpectrum oneSp(SpectrumType::IndexOfRefraction, ColorSpace::Rec709_D65, 1.0f, 1.0f, 1.0f);
-        UpsampledSpectrum zeroSp(SpectrumType::IndexOfRefraction, ColorSpace::Rec709_D65, 0.0f, 0.0f, 0.0f);
-        const float rx = rough[2 * i + 0], ry = rough[2 * i + 1];
-        const float alphaX = std::fmax(0.001f, rx * rx);
-        const float alphaY = std::fmax(0.001f, ry * ry);
-
-        switch (mat[i]) {
-        case kMatte: {
-            MatteBRDF b(albedoSp.evaluate(wls), 0.0f);
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        case kSpecularBRDF: {
-            SpecularBRDF b(albedoSp.evaluate(wls), iorSp.evaluate(wls), zeroSp.evaluate(wls));
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        case kMicrofacetBRDF: {
-            MicrofacetBRDF b(iorSp.evaluate(wls), zeroSp.evaluate(wls), alphaX, alphaY, 0.0f);
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        case kMicrofacetBSDF: {
-            MicrofacetBSDF b(albedoSp.evaluate(wls), oneSp.evaluate(wls), iorSp.evaluate(wls),
-                             alphaX, alphaY, 0.0f);
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        case kLambertianBSDF: {
-            LambertianBSDF b(albedoSp.evaluate(wls), 0.04f);
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        case kSpecularBSDF: {
-            // SpecularScatteringSurfaceMaterial_setupBSDF (materials.cu:1046-1058):
-            // coefficient, exterior IOR 1, interior IOR, dispersive unless a
-            // single wavelength is selected
-            SpecularBSDF b(albedoSp.evaluate(wls), oneSp.evaluate(wls), iorSp.evaluate(wls),
-                           !wls.singleIsSelected());
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        default: {
-            SampledSpectrum baseColor = albedoSp.evaluate(wls);
-            const float roughness = std::fmax(0.01f, rx);
-            const float m = metallic[i];
-            const float specular = 0.5f;
-            SampledSpectrum diffuseColor = baseColor * (1 - m);
-            SampledSpectrum specularF0Color = lerp(0.08f * specular * SampledSpectrum::One(), baseColor, m);
-            DiffuseAndSpecularBRDF b(diffuseColor, specularF0Color, roughness);
-            runQuery(b, query, ui, v4, p1, w3, e4, ep);
-            break;
-        }
-        }
-    }
+    bsdfBatchQueries(n, numThreads, wo, mat, rough, ior, rgb, metallic, u, wl, value, pdf, wi, evalValue, evalPdf);
 }
 
 // n outputs of std::mt19937_64 seeded with `seed`: the reference's per-pixel

@@ -318,3 +318,24 @@ def test_fp64_film_against_the_reference_fp32_kahan_film():
     p_err = np.abs(plain.astype(np.float64) - f64)[lit] / f64[lit]
     assert k_err.max() < 2e-7, k_err.max()
     assert p_err.max() > k_err.max()
+
+
+@pytest.mark.skipif(not ref.available64(), reason="FP64 oracle (oracle/_ref/libvlrref64.so) not built")
+def test_fp64_oracle_is_the_reference_algorithm_in_double():
+    """The FP64 oracle runs the reference's own BSDF code in double: on every
+    BSDF its results differ from the FP32 build's (it is not the FP32 code)
+    by FP32 rounding only, a median norm-wise difference below 1e-4 per
+    output, and it samples the same lobes (the same zero/non-zero pattern)."""
+    import vlr_b200 as V
+    inp = V.make_bsdf_batch_inputs(1 << 15, seed=77, materials=7)
+    r32, r64 = ref.bsdf_batch(inp), ref.bsdf_batch64(inp)
+    mat = inp["material"]
+    assert np.any(r32["value"].astype(np.float64) != r64["value"])
+    for k in ("value", "pdf", "wi", "evalValue", "evalPdf"):
+        a, b = r32[k].astype(np.float64), r64[k]
+        a2, b2 = a.reshape(len(mat), -1), b.reshape(len(mat), -1)
+        assert np.mean(np.any(a2 != 0, axis=1) == np.any(b2 != 0, axis=1)) > 0.999, k
+        for m in range(7):
+            sel = mat == m
+            d = np.abs(a2[sel] - b2[sel]).max(axis=1) / np.maximum(np.abs(b2[sel]).max(axis=1), 1e-30)
+            assert np.median(d) < 1e-4, (k, m, np.median(d))
