@@ -430,13 +430,15 @@ def terrain_cpu_baseline(desc, renderer, seconds_target=10.0):
                       f"own BSDF/spectral code"}
 
 
-def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True):
+def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True, paths_in_flight=0):
     """Path tracing and LVC-BPT on the 2,097,152-triangle terrain with 4096
     instanced icospheres under the 2048x1024 sky (FP64 CDF), 1920x1080,
     max depth 12, one light subpath per pixel per frame for LVC-BPT;
     device-timed segments/s after warm-up (8 and 4 spp: bounded samples of
     the 64-spp frame), the dominant wavefront stage against the HBM
-    roofline, and the CPU restatement on the host cores beside it."""
+    roofline, and the CPU restatement on the host cores beside it.
+    paths_in_flight > 0 fixes the launch size instead of autotuning it (a
+    smaller device footprint, for profiling)."""
     import torch
     from vlr_b200 import vlr as V, scenes
     W, H = 1920, 1080
@@ -452,7 +454,9 @@ def terrain_workloads(names=("terrain_pt", "terrain_lvc_bpt"), cpu=True):
         ctx.setScene(scene)
         ctx.setRenderer(renderer)
         ctx.setOptions(max_path_length=12, max_paths_in_flight=1 << 22)
-        if renderer == V.RENDERER_PATH_TRACING:
+        if paths_in_flight:
+            ctx.setOptions(max_paths_in_flight=paths_in_flight)
+        elif renderer == V.RENDERER_PATH_TRACING:
             ctx.autotune(cam, spp)      # launch configuration for this workload's frame
         ctx.render_samples(cam, True, 2)
         torch.cuda.synchronize()
@@ -607,14 +611,16 @@ def denoise_workload():
 
 
 WORKLOADS = {
-    "bsdf_batch": lambda: {"bsdf_batch": bsdf_batch_workload(measured_peaks()[0])},
-    "terrain_pt": lambda: terrain_workloads(("terrain_pt",)),
-    "terrain_lvc_bpt": lambda: terrain_workloads(("terrain_lvc_bpt",)),
-    "multi_scene_batch": lambda: {"multi_scene_batch": batch_workload()},
-    "glossy_guided": lambda: {"glossy_guided": glossy_guided_workload()},
-    "light_tracing": lambda: {"light_tracing": light_tracing_workload()},
-    "denoise": lambda: {"denoise": denoise_workload()},
-    "time_to_rmse": lambda: {"time_to_rmse": time_to_rmse()},
+    "bsdf_batch": lambda a: {"bsdf_batch": bsdf_batch_workload(measured_peaks()[0])},
+    "terrain_pt": lambda a: terrain_workloads(("terrain_pt",), cpu=not a.no_cpu_baseline,
+                                              paths_in_flight=a.paths_in_flight),
+    "terrain_lvc_bpt": lambda a: terrain_workloads(("terrain_lvc_bpt",), cpu=not a.no_cpu_baseline,
+                                                   paths_in_flight=a.paths_in_flight),
+    "multi_scene_batch": lambda a: {"multi_scene_batch": batch_workload()},
+    "glossy_guided": lambda a: {"glossy_guided": glossy_guided_workload()},
+    "light_tracing": lambda a: {"light_tracing": light_tracing_workload()},
+    "denoise": lambda a: {"denoise": denoise_workload()},
+    "time_to_rmse": lambda a: {"time_to_rmse": time_to_rmse()},
 }
 
 
@@ -742,7 +748,7 @@ def main():
     if args.workload:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        print(json.dumps(WORKLOADS[args.workload]()), flush=True)
+        print(json.dumps(WORKLOADS[args.workload](args)), flush=True)
         return
 
     import torch
