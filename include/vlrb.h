@@ -140,6 +140,15 @@ VLRResult vlrbContextGetStats(VLRContext context, VLRBRenderStats* stats);
  * pixels or no path tracer render has seeded the states for this image. */
 VLRResult vlrbContextReadPixelRngStates(VLRContext context, uint64_t* states, uint32_t count);
 
+/* The path tracer's queue lengths in its last launch (no counterpart in the
+ * reference, whose OptiX launch keeps no queues): 16 words per bounce for the
+ * first `bounces` bounces (at most 65): [0] rays traced, [1] shadow rays
+ * appended, [2 + k] hits appended to the shading queue of BSDF kind k (0
+ * Matte, 1 SpecularReflection, 2 MicrofacetReflection, 3
+ * MicrofacetScattering, 4 LambertianScattering, 5 UE4, 6 SpecularScattering,
+ * 7 emitter without BSDF), [10] misses; the rest 0. */
+VLRResult vlrbContextReadBounceCounters(VLRContext context, uint32_t* counters, uint32_t bounces);
+
 /* Learned path guiding of the path tracer (no counterpart in the reference).
  * With `train`, a launch records training samples at the Matte,
  * LambertianScattering and UE4 vertices of its first `recordBounces` bounces

@@ -210,6 +210,21 @@ def pt_render_fp32_films(flat, camera, width, height, spp, max_path_length, rng_
     return film, kahan[..., :16].copy(), plain, states
 
 
+def pt_render_census(flat, camera, width, height, spp, max_path_length, rng_states=None, threads=0):
+    """pt_render that also counts, per bounce, the rays traced and where they
+    ended: [64, 16] uint64 in the layout of the CUDA path tracer's queue
+    counters ([0] rays, [2 + k] hits on BSDF kind k, [10] misses).  Returns
+    (film, rng_states, census)."""
+    census = np.zeros((64, 16), np.uint64)
+    lib().vlrref_pt_set_census(_p(census))
+    try:
+        film, states, _ = pt_render(flat, camera, width, height, spp, max_path_length, rng_states=rng_states,
+                                    threads=threads)
+    finally:
+        lib().vlrref_pt_set_census(None)
+    return film, states, census
+
+
 def last_render_seconds():
     """Wall time of the last pt_render / bpt_render loop, scene set-up
     (BVH build) excluded."""

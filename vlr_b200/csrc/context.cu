@@ -955,6 +955,13 @@ bool Context::readPixelRngStates(uint64_t* states, uint32_t count) {
     return true;
 }
 
+bool Context::readBounceCounters(uint32_t* counters, uint32_t bounces) {
+    if (!pb.counters || bounces > kMaxBounces + 1) return false;
+    ck(cudaMemcpy(counters, pb.counters, size_t(bounces) * kCountersPerBounce * 4, cudaMemcpyDeviceToHost),
+       "read counters");
+    return true;
+}
+
 void Context::ensureGuiding(uint32_t paths) {
     const GuidingOptions &g = guiding;
     if (!guideNet || guideNet->net.log2Table != g.log2TableSize) {

@@ -133,6 +133,10 @@ public:
     // (pixel y*imgW+x), count <= imgW*imgH; false if the path buffers do not
     // hold that many.
     bool readPixelRngStates(uint64_t* states, uint32_t count);
+    // The path tracer's queue counters of its last launch, kCountersPerBounce
+    // words per bounce (pt.cuh: rays traced, shadow rays, then one hit queue
+    // per BSDF kind and the miss queue) for the first `bounces` bounces.
+    bool readBounceCounters(uint32_t* counters, uint32_t bounces);
 
 private:
     void buildScene(cudaStream_t stream);

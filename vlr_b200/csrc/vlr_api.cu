@@ -1400,6 +1400,14 @@ VLRResult vlrbContextReadPixelRngStates(VLRContext context, uint64_t* states, ui
     API_CATCH("vlrbContextReadPixelRngStates")
 }
 
+VLRResult vlrbContextReadBounceCounters(VLRContext context, uint32_t* counters, uint32_t bounces) {
+    CHECK_HANDLE(c, Context, kindContext, context);
+    if (!counters || bounces == 0) return VLRResult_InvalidArgument;
+    API_TRY
+    return c->readBounceCounters(counters, bounces) ? VLRResult_NoError : VLRResult_InvalidArgument;
+    API_CATCH("vlrbContextReadBounceCounters")
+}
+
 VLRResult vlrbContextSaveOutputImages(VLRContext context, const char* pathWithoutExtension, float brightnessCoeff) {
     CHECK_HANDLE(c, Context, kindContext, context);
     if (!pathWithoutExtension || c->width == 0 || c->height == 0) return VLRResult_InvalidArgument;

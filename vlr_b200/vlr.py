@@ -89,6 +89,7 @@ def _api():
         "vlrContextReadOutputBuffer": [v, v],
         "vlrbContextReadAuxBuffers": [v, v, v],
         "vlrbContextReadPixelRngStates": [v, v, ctypes.c_uint32],
+        "vlrbContextReadBounceCounters": [v, v, ctypes.c_uint32],
         "vlrbWriteOutputImages": [v, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_float],
         "vlrbContextSaveOutputImages": [v, ctypes.c_char_p, ctypes.c_float],
         "vlrContextSetScene": [v, v],
@@ -512,6 +513,14 @@ class Context:
         out = np.zeros(n, np.uint64)
         check(_api().vlrbContextReadPixelRngStates(self.h, out.ctypes.data_as(c_void_p), ctypes.c_uint32(n)),
               "readPixelRngStates")
+        return out
+
+    def read_bounce_counters(self, bounces=16):
+        """Queue lengths of the path tracer's last launch, [bounces, 16]
+        (vlrbContextReadBounceCounters)."""
+        out = np.zeros((bounces, 16), np.uint32)
+        check(_api().vlrbContextReadBounceCounters(self.h, out.ctypes.data_as(c_void_p), ctypes.c_uint32(bounces)),
+              "readBounceCounters")
         return out
 
     def stats(self):
