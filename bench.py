@@ -630,8 +630,11 @@ def batch_workload():
     1024x768, 1920x1080}; 1-64 spp; odd scenes guided with online training),
     each context's paths in flight and blocks per SM chosen by the
     autotuner.  Rendered once as plain per-scene launches one after another,
-    then as one CUDA graph of all scenes replayed (vlrbRenderBatch*); reports
-    aggregate segments/s and per-scene frame latency p50/p99 for both."""
+    then as one CUDA graph of all scenes replayed (vlrbRenderBatch*), then
+    as one graph whose plain scenes render in a single persistent kernel
+    launch beside the guided scenes' launches (VLRB_BATCH_PERSISTENT);
+    reports aggregate segments/s and per-scene frame latency p50/p99 for
+    each."""
     import torch
     from vlr_b200 import vlr as V, scenes
     rng = np.random.default_rng(2024)
@@ -694,6 +697,25 @@ def batch_workload():
     g_ms = t0.elapsed_time(t1) / reps
     g_seg = (sum(c.stats()["pathSegments"] for c, *_ in items) - seg0) / reps
     batch.close()
+    # one graph: the plain scenes in one persistent kernel launch
+    pbatch = V.RenderBatch([(ctx, cam, spp, True) for ctx, cam, keep, spp, W, H in items], persistent=True)
+    pbatch.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    seg0 = sum(c.stats()["pathSegments"] for c, *_ in items)
+    p_lat, p_lat_plain = [], []
+    t0 = ev()
+    t0.record(stream)
+    for _ in range(reps):
+        pbatch.launch(stream.cuda_stream)
+        times = pbatch.item_times()
+        p_lat += times
+        p_lat_plain += [t for k, t in enumerate(times) if k % 2 == 0]
+    t1 = ev()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    p_ms = t0.elapsed_time(t1) / reps
+    p_seg = (sum(c.stats()["pathSegments"] for c, *_ in items) - seg0) / reps
+    pbatch.close()
     out = {"workload": "32 seeded terrain/instance scenes, 1k-2M triangles (log-uniform), 256^2..1920x1080, "
                        "1-64 spp, half guided, autotuned launch configuration",
            "triangles": [int(c.stats()["numTriangles"]) for c, *_ in items],
@@ -703,6 +725,14 @@ def batch_workload():
            "graph_batch": {"segments_per_s": g_seg / (g_ms * 1e-3) / 1e9, "ms": g_ms,
                            "latency_ms_p50": float(np.percentile(g_lat, 50)),
                            "latency_ms_p99": float(np.percentile(g_lat, 99))},
+           "persistent_batch": {"segments_per_s": p_seg / (p_ms * 1e-3) / 1e9, "ms": p_ms,
+                                "latency_ms_p50": float(np.percentile(p_lat, 50)),
+                                "latency_ms_p99": float(np.percentile(p_lat, 99)),
+                                "plain_latency_ms_p50": float(np.percentile(p_lat_plain, 50)),
+                                "plain_latency_ms_p99": float(np.percentile(p_lat_plain, 99)),
+                                "note": "16 plain scenes in one persistent kernel launch (pixels from one "
+                                        "counter, smallest work first), 16 guided scenes as their own launch "
+                                        "sequences beside it, all in one replayed CUDA graph"},
            "unit": "G path segments/s"}
     for ctx, *_ in items:
         ctx.close()

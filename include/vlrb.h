@@ -335,6 +335,18 @@ typedef struct VLRBBatchItem {
 typedef struct VLRBRenderBatch_API* VLRBRenderBatch;
 VLRResult vlrbRenderBatchCreate(const VLRBBatchItem* items, uint32_t numItems, CUstream stream,
                                 VLRBRenderBatch* batch);
+/* flags: VLRB_BATCH_PERSISTENT renders the plain (unguided) items in ONE
+ * persistent kernel launch instead of one launch sequence each: every SM
+ * stays busy with pixels taken from one counter over all those items, laid
+ * out smallest work (pixels x samples) first, each pixel's samples drawn from
+ * its own RNG stream one after another (the images equal the path tracer's at
+ * one sample per pixel per launch).  Guided items keep their own launch
+ * sequences beside it.  itemMs of a persistent item is the time from the
+ * kernel's start to the end of the item's last pixel.  Persistent items do
+ * not fill the denoiser's guide buffers. */
+#define VLRB_BATCH_PERSISTENT 1u
+VLRResult vlrbRenderBatchCreateEx(const VLRBBatchItem* items, uint32_t numItems, CUstream stream, uint32_t flags,
+                                  VLRBRenderBatch* batch);
 VLRResult vlrbRenderBatchLaunch(VLRBRenderBatch batch, CUstream stream);
 VLRResult vlrbRenderBatchItemTimes(VLRBRenderBatch batch, float* itemMs);
 VLRResult vlrbRenderBatchDestroy(VLRBRenderBatch batch);

@@ -955,6 +955,22 @@ bool Context::readPixelRngStates(uint64_t* states, uint32_t count) {
     return true;
 }
 
+bool Context::persistentScene(uint32_t spp, PersistentScene* out) const {
+    const uint32_t pixels = imgW * imgH;
+    if (pixels == 0 || pathCapacity < pixels || pathSeedW != imgW || pathSeedH != imgH) return false;
+    out->scene = sg;
+    out->rng = pb.rng;
+    out->film = filmDesc();
+    out->totals = pb.totals;
+    out->width = imgW;
+    out->height = imgH;
+    out->stride = width;
+    out->spp = spp;
+    out->maxPathLength = options.maxPathLength;
+    out->firstUnit = 0;
+    return true;
+}
+
 bool Context::readBounceCounters(uint32_t* counters, uint32_t bounces) {
     if (!pb.counters || bounces > kMaxBounces + 1) return false;
     ck(cudaMemcpy(counters, pb.counters, size_t(bounces) * kCountersPerBounce * 4, cudaMemcpyDeviceToHost),
@@ -1199,7 +1215,8 @@ std::vector<AutotuneTrial> Context::autotune(cudaStream_t stream, const Camera* 
     return trials;
 }
 
-RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : items(std::move(its)) {
+RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream, bool persistentMode)
+    : items(std::move(its)), persistent(persistentMode) {
     for (const BatchItem &it : items) {
         if (!it.ctx || !it.cam || it.samples == 0) throw std::runtime_error("batch item without context, camera or samples");
         if (it.ctx->renderer != VLRRenderer_PathTracing) throw std::runtime_error("batch rendering is path tracing only");
@@ -1209,8 +1226,25 @@ RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : item
     evBegin.resize(n);
     evEnd.resize(n);
     evJoin.resize(n);
+    // Each item's stream gets a priority by its work (pixels x samples): the
+    // smallest items the highest, so the block scheduler starts their kernels
+    // first and short frames are not held behind long ones.  The captured
+    // nodes keep their stream's priority (instantiated with node priorities).
+    int leastPrio = 0, greatestPrio = 0;
+    ck(cudaDeviceGetStreamPriorityRange(&leastPrio, &greatestPrio), "priority range");
+    std::vector<uint32_t> byWork(n);
+    for (size_t i = 0; i < n; ++i) byWork[i] = static_cast<uint32_t>(i);
+    auto itemWork = [&](uint32_t i) {
+        const Context* c = items[i].ctx;
+        return uint64_t(c->width) * c->height * items[i].samples;
+    };
+    std::stable_sort(byWork.begin(), byWork.end(), [&](uint32_t a, uint32_t b) { return itemWork(a) < itemWork(b); });
+    std::vector<int> prio(n, leastPrio);
+    const int levels = leastPrio - greatestPrio + 1;
+    for (size_t r = 0; r < n; ++r)
+        prio[byWork[r]] = greatestPrio + static_cast<int>(r * levels / n);
     for (size_t i = 0; i < n; ++i) {
-        ck(cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking), "batch stream");
+        ck(cudaStreamCreateWithPriority(&streams[i], cudaStreamNonBlocking, prio[i]), "batch stream");
         ck(cudaEventCreate(&evBegin[i]), "event");
         ck(cudaEventCreate(&evEnd[i]), "event");
         ck(cudaEventCreateWithFlags(&evJoin[i], cudaEventDisableTiming), "event");
@@ -1227,14 +1261,55 @@ RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : item
         it.ctx->timer.enabled = profiling;
     }
     ck(cudaStreamSynchronize(stream), "batch warm-up");
+    slotOfItem.assign(n, ~0u);
+    if (persistent) {
+        for (size_t i = 0; i < n; ++i) {
+            const Context* c = items[i].ctx;
+            if (!(c->guiding.enabled || c->guiding.train)) plainOrder.push_back(static_cast<uint32_t>(i));
+        }
+        auto cost = [&](uint32_t i) { return uint64_t(items[i].ctx->imgW) * items[i].ctx->imgH * items[i].samples; };
+        std::stable_sort(plainOrder.begin(), plainOrder.end(), [&](uint32_t a, uint32_t b) { return cost(a) < cost(b); });
+        std::vector<PersistentScene> ps(plainOrder.size());
+        unsigned long long units = 0;
+        for (size_t k = 0; k < plainOrder.size(); ++k) {
+            BatchItem &it = items[plainOrder[k]];
+            if (!it.ctx->persistentScene(it.samples, &ps[k]))
+                throw std::runtime_error("batch item without path buffers for its image");
+            ps[k].firstUnit = units;
+            units += uint64_t(ps[k].width) * ps[k].height;
+            maps = maps || it.ctx->shadingNeedsMaps();
+            slotOfItem[plainOrder[k]] = static_cast<uint32_t>(k);
+        }
+        if (!ps.empty()) {
+            scenesBuf.resize(ps.size() * sizeof(PersistentScene));
+            ck(cudaMemcpy(scenesBuf.ptr, ps.data(), ps.size() * sizeof(PersistentScene), cudaMemcpyHostToDevice),
+               "persistent scenes");
+            countersBuf.resize(persistentCounterBytes(static_cast<uint32_t>(ps.size())));
+            work = persistentWorkDesc(scenesBuf.as<PersistentScene>(), static_cast<uint32_t>(ps.size()), units,
+                                      countersBuf.ptr);
+            grid = persistentGrid(items[plainOrder[0]].ctx->numSMs, maps);
+            ck(cudaStreamCreateWithFlags(&pStream, cudaStreamNonBlocking), "persistent stream");
+            ck(cudaEventCreateWithFlags(&pJoin, cudaEventDisableTiming), "event");
+        }
+    }
     // Captured on a stream of its own: the caller's may be the legacy default
     // stream, which cannot be captured.  Launches go to the caller's stream.
     ck(cudaStreamCreateWithFlags(&captureStream, cudaStreamNonBlocking), "capture stream");
     ck(cudaStreamBeginCapture(captureStream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         ck(cudaEventRecord(fork, captureStream), "fork");
+        if (!plainOrder.empty()) {
+            ck(cudaStreamWaitEvent(pStream, fork, 0), "wait fork");
+            for (uint32_t i : plainOrder)
+                if (items[i].firstFrame) items[i].ctx->clearFilm(pStream);
+            persistentPtLaunch(work, maps, grid, pStream);
+            for (uint32_t i : plainOrder) items[i].ctx->convertFilm(pStream);
+            ck(cudaEventRecord(pJoin, pStream), "join");
+            ck(cudaStreamWaitEvent(captureStream, pJoin, 0), "wait join");
+        }
         for (size_t i = 0; i < n; ++i) {
             BatchItem &it = items[i];
+            if (slotOfItem[i] != ~0u) continue;
             ck(cudaStreamWaitEvent(streams[i], fork, 0), "wait fork");
             ck(cudaEventRecordWithFlags(evBegin[i], streams[i], cudaEventRecordExternal), "begin");
             const bool profiling = it.ctx->timer.enabled;
@@ -1255,7 +1330,7 @@ RenderBatch::RenderBatch(std::vector<BatchItem> its, cudaStream_t stream) : item
         throw;
     }
     ck(cudaStreamEndCapture(captureStream, &graph), "end capture");
-    ck(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+    ck(cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority), "instantiate");
 }
 
 RenderBatch::~RenderBatch() {
@@ -1267,6 +1342,8 @@ RenderBatch::~RenderBatch() {
     for (auto e : evJoin) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
     if (captureStream) cudaStreamDestroy(captureStream);
+    if (pStream) cudaStreamDestroy(pStream);
+    if (pJoin) cudaEventDestroy(pJoin);
 }
 
 void RenderBatch::launch(cudaStream_t stream) {
@@ -1280,7 +1357,19 @@ void RenderBatch::launch(cudaStream_t stream) {
 
 void RenderBatch::itemTimes(std::vector<float>* ms) const {
     ms->resize(items.size());
+    std::vector<unsigned long long> ends(plainOrder.size());
+    unsigned long long start = 0;
+    if (!plainOrder.empty()) {
+        // the persistent items: each scene's last pixel against the launch's start
+        ck(cudaStreamSynchronize(pStream), "sync");
+        ck(cudaMemcpy(&start, work.startNs, 8, cudaMemcpyDeviceToHost), "start stamp");
+        ck(cudaMemcpy(ends.data(), work.endNs, ends.size() * 8, cudaMemcpyDeviceToHost), "end stamps");
+    }
     for (size_t i = 0; i < items.size(); ++i) {
+        if (slotOfItem[i] != ~0u) {
+            (*ms)[i] = static_cast<float>(double(ends[slotOfItem[i]] - start) * 1e-6);
+            continue;
+        }
         ck(cudaEventSynchronize(evEnd[i]), "sync");
         ck(cudaEventElapsedTime(&(*ms)[i], evBegin[i], evEnd[i]), "elapsed");
     }

@@ -138,6 +138,14 @@ public:
     // per BSDF kind and the miss queue) for the first `bounces` bounces.
     bool readBounceCounters(uint32_t* counters, uint32_t bounces);
 
+    // For a persistent batch launch (after a render of this image): the
+    // scene, path RNG states, film and totals, rendering `spp` samples per
+    // pixel; false when the path buffers do not hold one slot per pixel.
+    bool persistentScene(uint32_t spp, PersistentScene* out) const;
+    bool shadingNeedsMaps() const { return sg.geomMaps != nullptr || sg.hasScalarTextures != 0; }
+    void clearFilm(cudaStream_t stream) { filmClear(filmDesc(), stream); }
+    void convertFilm(cudaStream_t stream) { filmToRGBA(filmDesc(), output.as<float4>(), stream); }
+
 private:
     void buildScene(cudaStream_t stream);
     void setupCamera(const Camera* cam);
@@ -206,7 +214,10 @@ struct BatchItem {
 
 class RenderBatch {
 public:
-    RenderBatch(std::vector<BatchItem> items, cudaStream_t stream);
+    // persistent: the plain (unguided) items render in one persistent kernel
+    // launch (pt_persistent.cu), laid out smallest work (pixels x samples)
+    // first; guided items keep their own launch sequences beside it.
+    RenderBatch(std::vector<BatchItem> items, cudaStream_t stream, bool persistent = false);
     ~RenderBatch();
     RenderBatch(const RenderBatch &) = delete;
     RenderBatch &operator=(const RenderBatch &) = delete;
@@ -222,6 +233,16 @@ private:
     cudaStream_t captureStream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // persistent mode
+    bool persistent = false;
+    std::vector<uint32_t> plainOrder;        // item indices in the order of the persistent layout
+    std::vector<uint32_t> slotOfItem;        // item -> position in plainOrder, or ~0u
+    DeviceBuffer scenesBuf, countersBuf;
+    PersistentWork work{};
+    bool maps = false;
+    int grid = 0;
+    cudaStream_t pStream = nullptr;
+    cudaEvent_t pJoin = nullptr;
 };
 
 } // namespace api

@@ -20,6 +20,7 @@
 #include "guide_mlp.cuh"
 #include "tables.cuh"
 #include "wavefront.cuh"
+#include "pt_shade.cuh"
 
 #include <random>
 #include <stdexcept>
@@ -43,45 +44,18 @@ __global__ void __launch_bounds__(256) cameraKernel(SceneGPU S, PathBuffers pb, 
     const uint32_t P = fp.numPaths;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
         const uint32_t pixel = pixelOfPath(p, fp.width, fp.height);
-        const uint32_t px = pixel % fp.width, py = pixel / fp.width;
         PCG32 rng{ pb.rng[p] };
-        float jx = rng.uniform(), jy = rng.uniform();
-        float fx = px + jx, fy = py + jy;
-        float selectWLPDF;
-        float wo = rng.uniform(), ws = rng.uniform();
-        WLS wls = WLS::equalOffsets(wo, ws, &selectWLPDF);
-        // PerspectiveCamera_sample (cameras.cu:42-74)
-        const Camera &C = S.cam;
-        float lx, ly;
-        float l0 = rng.uniform(), l1 = rng.uniform();
-        concentricDisk(l0, l1, &lx, &ly);
-        V3 orgLocal(C.lensRadius * lx, C.lensRadius * ly, 0.0f);
-        V3 gn = normalize(C.forward);
-        Frame camFrame;
-        camFrame.z = gn;
-        camFrame.x = normalize(C.right);
-        camFrame.y = cross(camFrame.z, camFrame.x);
-        V3 lensPos = C.right * orgLocal.x + C.up * orgLocal.y + C.forward * orgLocal.z + C.position;
-        float areaPDF = C.lensRadius > 0.0f ? 1.0f / (kPi * C.lensRadius * C.lensRadius) : 1.0f;
-        // the camera's IDF sample (cameras.cu:142-155 perspective, :272-288
-        // equirectangular); the density is per pixel
-        float u0 = fx / fp.width, u1 = fy / fp.height;
-        float dirPDF;
-        V3 dirLocal = cameraSampleDir(C, C.lensRadius * lx, C.lensRadius * ly, u0, u1, &dirPDF);
-        dirPDF *= static_cast<float>(fp.width * fp.height);
-        V3 rayDir = camFrame.fromLocal(dirLocal);
-        S4 We0(C.sensitivity);
-        S4 alpha = (We0 * S4::one()) * (lensCos(C, rayDir, gn) / (areaPDF * dirPDF * selectWLPDF));
+        const CameraRay cr = cameraSample(S, pixel % fp.width, pixel / fp.width, fp.width, fp.height, rng);
         pb.rng[p] = rng.state;
-        pb.lambda[p] = make_float4(wls.lambda[0], wls.lambda[1], wls.lambda[2], wls.lambda[3]);
-        pb.flags[p] = wls.selected;
-        pb.alpha[p] = toF4(alpha);
+        pb.lambda[p] = make_float4(cr.wls.lambda[0], cr.wls.lambda[1], cr.wls.lambda[2], cr.wls.lambda[3]);
+        pb.flags[p] = cr.wls.selected;
+        pb.alpha[p] = toF4(cr.alpha);
         pb.contrib[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-        pb.initImportance[p] = alpha.importance(wls.selected);
-        pb.prevDirPDF[p] = dirPDF;
+        pb.initImportance[p] = cr.initImportance;
+        pb.prevDirPDF[p] = cr.dirPDF;
         pb.prevType[p] = dir::Acquisition | dir::LowFreq;
-        pb.rayOrg[p] = make_float4(lensPos.x, lensPos.y, lensPos.z, FLT_MAX);
-        pb.rayDir[p] = make_float4(rayDir.x, rayDir.y, rayDir.z, 0.0f);
+        pb.rayOrg[p] = make_float4(cr.org.x, cr.org.y, cr.org.z, FLT_MAX);
+        pb.rayDir[p] = make_float4(cr.dir.x, cr.dir.y, cr.dir.z, 0.0f);
         pb.active[0][p] = p;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) bounceCounters(pb, 0)[kCntActive] = P;
@@ -116,32 +90,9 @@ __global__ void __launch_bounds__(256) traceKernel(SceneGPU S, PathBuffers pb, F
 __device__ __forceinline__ void shadeMiss(const SceneGPU &S, const PathBuffers &pb, uint32_t p, const WLS &wls,
                                           uint32_t pathLength, S4 &contrib) {
     if (S.envInst < 0) return;
-    float4 d4 = pb.rayDir[p];
-    V3 direction(d4.x, d4.y, d4.z);
-    float phi, theta;
-    toPolarYUp(direction, &theta, &phi);
-    float posPhi = phi;
-    phi += S.envRotation;
-    phi = phi - floorf(phi / (2 * kPi)) * 2 * kPi;
-    float tu = phi / (2 * kPi), tv = theta / kPi;
-    float uvPDF = envPdfUV(S.env, tu, tv);
-    float hypAreaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
-    const MatDesc &m = S.mats[S.envMaterial];
-    // EnvironmentEDF: emittance pi*E, directional factor 1/pi for the
-    // direction facing the scene (materials.cu:2830-2893).
-    S4 E = envRadiance(S, tu, tv, wls) * m.emitScale;
-    S4 spEmittance = kPi * E;
-    (void)posPhi;
-    if (!spEmittance.hasNonZero()) return;
-    S4 Le = spEmittance * (1.0f / kPi);
-    float MIS = 1.0f;
-    uint32_t prevType = pb.prevType[p];
-    if (!dir::isDelta(prevType) && pathLength > 1) {
-        float bsdfPDF = pb.prevDirPDF[p];
-        float lightPDF = S.envLightProb * hypAreaPDF * 1.0f / 1.0f;
-        MIS = (bsdfPDF * bsdfPDF) / (lightPDF * lightPDF + bsdfPDF * bsdfPDF);
-    }
-    contrib += toS4(pb.alpha[p]) * Le * MIS;
+    const float4 d4 = pb.rayDir[p];
+    envMissContribution(S, V3(d4.x, d4.y, d4.z), wls, toS4(pb.alpha[p]), PrevFromBuffers{ &pb, p }, pathLength,
+                        contrib);
 }
 
 __device__ __forceinline__ float4* recField(const GuideFrame &gf, uint32_t P, uint32_t b, uint32_t f) {
@@ -236,19 +187,8 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
         V3 dirOutLocal = sp.frame.toLocal(-rayDir);
         S4 alpha = toS4(pb.alpha[p]);
         // implicit light sampling
-        S4 spEmittance = emittance(S.meng, mat, wls);
-        if (spEmittance.hasNonZero()) {
-            S4 Le = spEmittance * edfEval(mat.emitter, dirOutLocal);
-            float MIS = 1.0f;
-            if (!dir::isDelta(pb.prevType[p]) && pathLength > 1) {
-                float bsdfPDF = pb.prevDirPDF[p];
-                float dist2 = (sp.position - rayOrg).sqLength();
-                float lightPDF = __ldg(S.geomLightPdfArea + sp.geomInst) * hypAreaPDF * dist2 /
-                                 fabsf(dirOutLocal.z);
-                MIS = (bsdfPDF * bsdfPDF) / (lightPDF * lightPDF + bsdfPDF * bsdfPDF);
-            }
-            contrib += alpha * Le * MIS;
-        }
+        implicitEmission(S, mat, wls, sp, dirOutLocal, rayOrg, hypAreaPDF, PrevFromBuffers{ &pb, p }, pathLength,
+                         alpha, contrib);
         alpha *= bsdfScale;   // a Multi material's component choice (after the emission)
         // The record of the previous vertex closes after this vertex's
         // emission: light reached directly from there is NEE's job, and the
@@ -275,89 +215,15 @@ __global__ void __launch_bounds__(256, 3) shadeKernel(SceneGPU S, PathBuffers pb
             if (guided) loadMixture(gf, P, p, mix);
         }
         // next-event estimation
-        if (bsdfHasNonDelta(bsdf) && S.lightInsts.n > 0) {
-            float uLight = rng.uniform();
-            float instProb, uInst;
-            uint32_t li = S.lightInsts.sample(uLight, &instProb, &uInst);
-            float ue0 = rng.uniform(), ue1 = rng.uniform();
-            LightSample ls;
-            float lightProb;
-            S4 M;
-            bool ok = true;
-            if (static_cast<int32_t>(li) == S.envInst) {
-                // sampleInfiniteSphere (infinite_sphere.cu:60-114)
-                float groupProb, uPrim;
-                S.instGroups[li].sample(uInst, &groupProb, &uPrim);
-                lightProb = instProb * groupProb;
-                float uu, vv, uvPDF;
-                envSampleUV(S.env, ue0, ue1, &uu, &vv, &uvPDF);
-                float phi = 2 * kPi * uu, theta = kPi * vv;
-                float posPhi = phi - S.envRotation;
-                posPhi = posPhi - floorf(posPhi / (2 * kPi)) * 2 * kPi;
-                V3 dirE = dirFromPolarYUp(posPhi, theta);
-                ls.sp.position = dirE;
-                ls.sp.gn = -dirE;
-                ls.sp.frame.z = -dirE;
-                ls.sp.atInfinity = true;
-                ls.areaPDF = uvPDF / (2 * kPi * kPi * sinf(theta));
-                ls.delta = false;
-                ls.isPoint = false;
-                ls.material = S.envMaterial;
-                M = kPi * envRadiance(S, uu, vv, wls) * S.mats[S.envMaterial].emitScale;
-                ok = uvPDF > 0.0f;
-            }
-            else {
-                float groupProb, uPrim;
-                uint32_t g = S.instGroups[li].sample(uInst, &groupProb, &uPrim);
-                lightProb = instProb * groupProb;
-                uint32_t grp = __ldg(S.instFirstGroup + li) + g;
-                sampleTriangleGroup(S, grp, uPrim, ue0, ue1, &ls);
-                M = emittance(S.meng, S.mats[ls.material], wls);
-            }
-            if (ok && M.hasNonZero()) {
-                // testVisibility (light_transport_common.h:147-177)
-                V3 shadowDir;
-                float dist2;
-                if (ls.sp.atInfinity) { shadowDir = normalize(ls.sp.position); dist2 = 1.0f; }
-                else {
-                    V3 dv = ls.sp.position - sp.position;
-                    dist2 = dv.sqLength();
-                    shadowDir = dv / sqrtf(dist2);
-                }
-                bool front = dot(sp.gn, shadowDir) > 0;
-                V3 sOrg = offsetRayOrigin(sp.position, front ? sp.gn : -sp.gn);
-                float tmax = FLT_MAX;
-                if (!ls.sp.atInfinity) {
-                    bool lfront = -dot(ls.sp.gn, shadowDir) > 0;
-                    V3 lPt = offsetRayOrigin(ls.sp.position, lfront ? ls.sp.gn : -ls.sp.gn);
-                    tmax = (lPt - sOrg).length() * 0.9999f;
-                }
-                float recSqDist = 1.0f / dist2;
-                V3 dirL = ls.sp.atInfinity ? V3(0.0f, 0.0f, 1.0f) : ls.sp.frame.toLocal(-shadowDir);
-                V3 dirSn = sp.frame.toLocal(shadowDir);
-                S4 Le = M * edfEval(S.mats[ls.material].emitter, dirL);
-                float lightPDF = lightProb * ls.areaPDF;
-                S4 fs = bsdfEval(bsdf, q, gnLocal, dirSn, nullptr);
-                float cosLight = ls.isPoint ? 1.0f : absDot(-shadowDir, ls.sp.gn);
-                float dirPdfV = bsdfPDF(bsdf, q, dirSn, nullptr);
-                if constexpr (kGuide) {
-                    if (guided) dirPdfV = 0.5f * dirPdfV + 0.5f * guide::mixturePdf(mix, shadowDir);
-                }
-                float bsdfPdfV = dirPdfV * cosLight * recSqDist;
-                float MIS = 1.0f;
-                if (!ls.delta && !isinf(lightPDF))
-                    MIS = (lightPDF * lightPDF) / (lightPDF * lightPDF + bsdfPdfV * bsdfPdfV);
-                float G = absDot(dirSn, gnLocal) * cosLight * recSqDist;
-                float scalar = G * MIS / lightPDF;
-                S4 c = alpha * Le * fs * scalar;
-                if (c.hasNonZero()) {
-                    uint32_t slot = appendSlot(ctr + kCntShadow, 0u);
-                    ShadowRay sr;
-                    sr.org = make_float4(sOrg.x, sOrg.y, sOrg.z, tmax);
-                    sr.dir = make_float4(shadowDir.x, shadowDir.y, shadowDir.z, __uint_as_float(p));
-                    sr.contrib = toF4(c);
-                    pb.shadow[slot] = sr;
-                }
+        {
+            NeeRay nr;
+            if (neeSample<kGuide>(S, sp, bsdf, q, gnLocal, wls, alpha, rng, guided, mix, &nr)) {
+                uint32_t slot = appendSlot(ctr + kCntShadow, 0u);
+                ShadowRay sr;
+                sr.org = make_float4(nr.org.x, nr.org.y, nr.org.z, nr.tmax);
+                sr.dir = make_float4(nr.dir.x, nr.dir.y, nr.dir.z, __uint_as_float(p));
+                sr.contrib = toF4(nr.contrib);
+                pb.shadow[slot] = sr;
             }
         }
         // BSDF sampling (guided kinds: one-sample MIS of BSDF and mixture)

@@ -161,6 +161,40 @@ void launchTraceSorted(const SceneGPU &scene, const PathBuffers &pb, const Frame
                        cudaStream_t stream);
 
 void filmToRGBA(const Film &film, float4* out, cudaStream_t stream);
+
+// One scene of a persistent batch launch (pt_persistent.cu): a rendered
+// context's scene, RNG states, film and statistics, and how much to render.
+struct PersistentScene {
+    SceneGPU scene;
+    uint64_t* rng;                 // path-slot RNG states: slot p renders pixel pixelOfPath(p)
+    Film film;
+    unsigned long long* totals;    // running [segments, shadow rays] of the context
+    uint32_t width, height;        // the image
+    uint32_t stride;               // film row length in pixels
+    uint32_t spp;                  // samples per pixel of this launch
+    uint32_t maxPathLength;
+    unsigned long long firstUnit;  // pixels of the scenes laid out before this one
+};
+
+// The batch of one persistent launch and its device counters.
+struct PersistentWork {
+    const PersistentScene* scenes;   // device array
+    uint32_t numScenes;
+    unsigned long long totalUnits;   // pixels of all scenes
+    unsigned long long* next;        // next pixel to hand out
+    unsigned long long* startNs;     // global timer at the launch's start
+    uint32_t* pixelsDone;            // per scene
+    unsigned long long* endNs;       // global timer when each scene's last pixel finished
+};
+
+size_t persistentCounterBytes(uint32_t numScenes);
+PersistentWork persistentWorkDesc(const PersistentScene* devScenes, uint32_t numScenes,
+                                  unsigned long long totalUnits, void* counters);
+// Blocks of the persistent grid: every SM filled to the kernel's occupancy.
+int persistentGrid(int numSMs, bool maps);
+// Resets the counters and launches (maps: the normal-map / scalar-texture
+// shading variant).  Enqueued on `stream`; capturable.
+void persistentPtLaunch(const PersistentWork &w, bool maps, int grid, cudaStream_t stream);
 void filmClear(const Film &film, cudaStream_t stream);
 void filmAddFrames(const Film &film, uint32_t samples, cudaStream_t stream);
 

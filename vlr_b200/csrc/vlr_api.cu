@@ -1282,7 +1282,12 @@ struct VLRBRenderBatch_API {
 
 VLRResult vlrbRenderBatchCreate(const VLRBBatchItem* items, uint32_t numItems, CUstream stream,
                                 VLRBRenderBatch* batch) {
-    if (!items || numItems == 0 || !batch) return VLRResult_InvalidArgument;
+    return vlrbRenderBatchCreateEx(items, numItems, stream, 0u, batch);
+}
+
+VLRResult vlrbRenderBatchCreateEx(const VLRBBatchItem* items, uint32_t numItems, CUstream stream, uint32_t flags,
+                                  VLRBRenderBatch* batch) {
+    if (!items || numItems == 0 || !batch || (flags & ~VLRB_BATCH_PERSISTENT)) return VLRResult_InvalidArgument;
     std::vector<api::BatchItem> its;
     for (uint32_t i = 0; i < numItems; ++i) {
         CHECK_HANDLE(c, Context, kindContext, items[i].context);
@@ -1294,10 +1299,11 @@ VLRResult vlrbRenderBatchCreate(const VLRBBatchItem* items, uint32_t numItems, C
     }
     API_TRY
     auto* b = new VLRBRenderBatch_API;
-    b->impl.reset(new api::RenderBatch(std::move(its), reinterpret_cast<cudaStream_t>(stream)));
+    b->impl.reset(new api::RenderBatch(std::move(its), reinterpret_cast<cudaStream_t>(stream),
+                                       (flags & VLRB_BATCH_PERSISTENT) != 0));
     *batch = b;
     return VLRResult_NoError;
-    API_CATCH("vlrbRenderBatchCreate")
+    API_CATCH("vlrbRenderBatchCreateEx")
 }
 
 VLRResult vlrbRenderBatchLaunch(VLRBRenderBatch batch, CUstream stream) {

@@ -133,6 +133,8 @@ def _api():
         "vlrbContextGetStats": [v, ctypes.POINTER(VLRBRenderStats)],
         "vlrbContextSetGuiding": [v, ctypes.POINTER(VLRBGuidingOptions)],
         "vlrbRenderBatchCreate": [ctypes.POINTER(VLRBBatchItem), ctypes.c_uint32, v, ctypes.POINTER(c_void_p)],
+        "vlrbRenderBatchCreateEx": [ctypes.POINTER(VLRBBatchItem), ctypes.c_uint32, v, ctypes.c_uint32,
+                                    ctypes.POINTER(c_void_p)],
         "vlrbRenderBatchLaunch": [v, v],
         "vlrbRenderBatchItemTimes": [v, ctypes.POINTER(ctypes.c_float)],
         "vlrbRenderBatchDestroy": [v],
@@ -530,16 +532,19 @@ class Context:
 
 
 class RenderBatch:
-    """vlrbRenderBatch*: items = [(context, camera, samples, first_frame)]."""
+    """vlrbRenderBatch*: items = [(context, camera, samples, first_frame)];
+    persistent: the plain items in one persistent kernel launch
+    (VLRB_BATCH_PERSISTENT)."""
 
-    def __init__(self, items, stream=0):
+    def __init__(self, items, stream=0, persistent=False):
         self.n = len(items)
         arr = (VLRBBatchItem * self.n)()
         for i, (ctx, cam, spp, first) in enumerate(items):
             arr[i] = VLRBBatchItem(ctx.h.value if hasattr(ctx.h, "value") else ctx.h, cam.h.value
                                    if hasattr(cam.h, "value") else cam.h, spp, first)
         self.h = c_void_p()
-        check(_api().vlrbRenderBatchCreate(arr, self.n, c_void_p(stream), ctypes.byref(self.h)), "batchCreate")
+        check(_api().vlrbRenderBatchCreateEx(arr, self.n, c_void_p(stream), ctypes.c_uint32(1 if persistent else 0),
+                                             ctypes.byref(self.h)), "batchCreate")
 
     def launch(self, stream=0):
         check(_api().vlrbRenderBatchLaunch(self.h, c_void_p(stream)), "batchLaunch")
