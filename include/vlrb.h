@@ -85,7 +85,10 @@ typedef struct VLRBRenderOptions {
                                      0 = the pixel count (one per pixel path); the LVC-BPT
                                      cache holds 10 vertices per light subpath */
     uint64_t rngSeed;             /* seed of the per-path RNG states, 0 = the reference's
-                                     591842031321323413 (context.cpp:1176-1190) */
+                                     591842031321323413 (context.cpp:1176-1190); any other
+                                     seed also gives LVC-BPT's and the light tracer's light
+                                     subpaths and per-frame wavelengths their own seed
+                                     (otherwise the reference's 459182033132123413) */
     uint32_t consistentDielectricPdf;  /* 0: MicrofacetScattering pdf exactly as the reference,
                                      which is 0 for every transmission out of the medium
                                      (materials.cu:1448-1513), so MIS double-counts NEE

@@ -955,6 +955,17 @@ bool Context::readPixelRngStates(uint64_t* states, uint32_t count) {
     return true;
 }
 
+uint64_t Context::lightSeedOf(uint64_t rngSeed) {
+    // the reference's constant (context.cpp:618-626) unless the caller chose
+    // its own seed: then one derived from it (SplitMix64), so contexts or
+    // ranks with different seeds also draw different light subpaths
+    if (rngSeed == 0 || rngSeed == 591842031321323413ull) return 459182033132123413ull;
+    uint64_t z = rngSeed + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 bool Context::persistentScene(uint32_t spp, PersistentScene* out) const {
     const uint32_t pixels = imgW * imgH;
     if (pixels == 0 || pathCapacity < pixels || pathSeedW != imgW || pathSeedH != imgH) return false;
@@ -1064,7 +1075,13 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                                                                        : std::max<uint32_t>(1, pixels);
                 const uint32_t capacity = static_cast<uint32_t>(
                     std::min<uint64_t>(uint64_t(10) * lightPaths, 0xFFFFFFFFull / 2));
-                if (bptCapacityPaths < lightPaths || bptCapacityVerts < capacity || bptEyeCapacity < pixels) {
+                const uint64_t lightSeed = lightSeedOf(options.rngSeed);
+                const bool reseed = bptLightSeed != lightSeed;
+                if (reseed) {
+                    bptLightSeed = lightSeed;
+                    bptRng.seed(lightSeed);
+                }
+                if (bptCapacityPaths < lightPaths || bptCapacityVerts < capacity || bptEyeCapacity < pixels || reseed) {
                     bptCapacityPaths = lightPaths;
                     bptCapacityVerts = capacity;
                     bptEyeCapacity = pixels;
@@ -1072,7 +1089,7 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                     carveBptBuffers(bptMem.ptr, lightPaths, pixels, capacity, &lightPb, &bb);
                     std::vector<uint64_t> seeds(lightPaths);
                     // The reference seeds its light-path RNGs from this generator (context.cpp:618-626).
-                    seedPathRngs(seeds.data(), lightPaths, 459182033132123413ull);
+                    seedPathRngs(seeds.data(), lightPaths, lightSeed);
                     ck(cudaMemcpy(lightPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
                     ck(cudaMemset(lightPb.totals, 0, 16), "totals");
                 }
@@ -1097,14 +1114,16 @@ void Context::render(cudaStream_t stream, const Camera* cam, bool firstFrame, ui
                 const uint32_t frames = std::max<uint32_t>(
                     1u, std::min<uint32_t>(samples - done, options.maxPathsInFlight / lightPaths));
                 const uint32_t slots = lightPaths * frames;
-                if (ltCapacity < slots) {
+                const uint64_t lightSeed = lightSeedOf(options.rngSeed);
+                if (ltCapacity < slots || ltLightSeed != lightSeed) {
+                    ltLightSeed = lightSeed;
                     ltCapacity = slots;
                     const size_t pathBytes = pathBufferBytes(slots);
                     ltMem.resize(pathBytes + ltConnectionBytes(slots));
                     carvePathBuffers(ltMem.ptr, slots, &ltPb);
                     ltConn = ltMem.as<char>() + pathBytes;
                     std::vector<uint64_t> seeds(slots);
-                    seedPathRngs(seeds.data(), slots, 459182033132123413ull);
+                    seedPathRngs(seeds.data(), slots, lightSeed);
                     ck(cudaMemcpy(ltPb.rng, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice), "seed light rngs");
                     ck(cudaMemset(ltPb.totals, 0, 16), "totals");
                 }

@@ -182,6 +182,8 @@ private:
     PathBuffers pb{};
     PathBuffers lightPb{};
     std::mt19937_64 bptRng{ 459182033132123413ull };
+    uint64_t bptLightSeed = 459182033132123413ull, ltLightSeed = 459182033132123413ull;
+    static uint64_t lightSeedOf(uint64_t rngSeed);
     BptBuffers bb{};
     uint32_t pathCapacity = 0;
     uint64_t pathSeed = 0;
