@@ -339,6 +339,10 @@ def time_to_rmse():
 # ---- the other scope-table workloads, reported beside the headline line
 BATCH_BYTES_PER_QUERY = 116     # in: wo 12, material 4, roughness 8, ior 4, albedo 12, metallic 4, u 12,
                                 # wavelength u 8; out: value 16, pdf 4, wi 12, eval value 16, eval pdf 4
+# ncu, one launch of the 2^20-query batch (--set full): DRAM bytes read +
+# written, FMA-pipe and issue-active fractions; the kernel is issue/latency
+# bound inside the GGX BSDFs, so these stand beside its HBM fraction.
+BATCH_NCU = {"dram_bytes": 161.8e6 + 76.6e6, "fma_pipe": 0.179, "issue": 0.365}
 
 
 def bsdf_batch_workload(hbm_peak):
@@ -370,10 +374,26 @@ def bsdf_batch_workload(hbm_peak):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / iters
     gbs = n * BATCH_BYTES_PER_QUERY / (ms * 1e-3) / 1e9
-    out = {"workload": "BSDF shading batch, 2^20 queries, six BSDFs uniform, 4 hero wavelengths",
+    # end to end through the host-buffer entry (vlrbBsdfBatchHost: device
+    # buffers, H2D copy of the inputs, the kernel, D2H copy of the outputs),
+    # host-clock timed since the call returns when its results are home
+    host_inp = VB.make_bsdf_batch_inputs(n, seed=100)
+    VB.bsdf_batch_host(host_inp)
+    reps = 8
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        VB.bsdf_batch_host(host_inp)
+    e2e_s = (time.perf_counter() - t0) / reps
+    out = {"workload": "BSDF shading batch, 2^20 queries, seven BSDFs uniform, 4 hero wavelengths",
            "queries_per_s": n / (ms * 1e-3), "ms_per_batch": ms,
+           "e2e": {"value": n / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * 52,
+                   "note": "vlrbBsdfBatchHost from pageable host arrays, host-clock timed"},
            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
-                        "bytes_per_query": BATCH_BYTES_PER_QUERY}}
+                        "bytes_per_query": BATCH_BYTES_PER_QUERY,
+                        "fp32_pipe_active": BATCH_NCU["fma_pipe"], "issue_active": BATCH_NCU["issue"],
+                        "traffic": BATCH_NCU["dram_bytes"],
+                        "ncu_source": "dram__bytes_read.sum + dram__bytes_write.sum, FMA pipe and issue-active "
+                                      "fractions of one launch of this workload"}}
     from oracle import ref
     if ref.available():
         m = 1 << 16
