@@ -55,7 +55,10 @@ typedef struct VLRBBsdfBatch {
 VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream);
 
 /* All pointers are host pointers; copies in, runs, copies out, returns when
- * done.  kernelMs (may be NULL) receives the kernel's device time. */
+ * done.  kernelMs (may be NULL) receives the kernel's device time.  The
+ * device buffers and stream it uses are kept per device between calls (grown
+ * to the largest batch so far, released at process exit), and calls are
+ * serialised; pinned host arrays copy at the link's full rate. */
 VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs);
 
 /* vlrbBsdfBatchHost with options.  VLRB_BSDF_BATCH_CONTRACTED runs the copy

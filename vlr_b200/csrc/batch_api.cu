@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <exception>
+#include <map>
+#include <mutex>
 
 namespace {
 
@@ -42,6 +44,30 @@ extern "C" VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream) 
     }
 }
 
+// Device side of the host-buffer entry, kept per device between calls (grown
+// to the largest batch, never freed: the driver releases it at exit), with
+// its own stream and timing events.  Calls are serialised by the mutex.
+struct HostBatchState {
+    void* in = nullptr;
+    void* out = nullptr;
+    size_t inBytes = 0, outBytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+static std::mutex g_hostBatchMutex;
+static std::map<int, HostBatchState> g_hostBatch;
+
+static cudaError_t growDevice(void** p, size_t* have, size_t want) {
+    if (*have >= want) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    const cudaError_t e = cudaMalloc(p, want);
+    if (e == cudaSuccess) *have = want;
+    return e;
+}
+
 static VLRResult bsdfBatchHost(const VLRBBsdfBatch* batch, uint32_t flags, float* kernelMs) {
     if (!validBatch(batch) || (flags & ~VLRB_BSDF_BATCH_CONTRACTED))
         return VLRResult_InvalidArgument;
@@ -51,19 +77,30 @@ static VLRResult bsdfBatchHost(const VLRBBsdfBatch* batch, uint32_t flags, float
     }
     try {
         const size_t n = static_cast<size_t>(batch->count);
+        std::lock_guard<std::mutex> lock(g_hostBatchMutex);
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess) return VLRResult_InternalError;
+        HostBatchState &st = g_hostBatch[device];
+        if (!st.stream) {
+            if (cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreate(&st.e0) != cudaSuccess || cudaEventCreate(&st.e1) != cudaSuccess)
+                return VLRResult_InternalError;
+        }
         // Inputs: wo 3, material 1 (u32), roughness 2, ior 1, albedo 3,
         // metallic 1, u 3, wavelengthU 2  -> 16 words per query.
         // Outputs: value 4, pdf 1, wi 3, evalValue 4, evalPdf 1 -> 13 words.
-        DevBuf in, out;
-        if (in.alloc(n * 16 * 4) != cudaSuccess || out.alloc(n * 13 * 4) != cudaSuccess)
+        if (growDevice(&st.in, &st.inBytes, n * 16 * 4) != cudaSuccess ||
+            growDevice(&st.out, &st.outBytes, n * 13 * 4) != cudaSuccess)
             return VLRResult_InternalError;
-        char* ib = static_cast<char*>(in.p);
-        char* ob = static_cast<char*>(out.p);
+        char* ib = static_cast<char*>(st.in);
+        char* ob = static_cast<char*>(st.out);
+        cudaStream_t s = st.stream;
         VLRBBsdfBatch d = *batch;
         size_t off = 0;
+        cudaError_t e = cudaSuccess;
         auto place = [&](const void* src, size_t words, const void** dst) {
             *dst = ib + off;
-            cudaMemcpy(ib + off, src, n * words * 4, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(ib + off, src, n * words * 4, cudaMemcpyHostToDevice, s);
             off += n * words * 4;
         };
         place(batch->wo, 3, reinterpret_cast<const void**>(&d.wo));
@@ -80,17 +117,20 @@ static VLRResult bsdfBatchHost(const VLRBBsdfBatch* batch, uint32_t flags, float
         d.pdf = reinterpret_cast<float*>(ob + n * 32);
         d.wi = reinterpret_cast<float*>(ob + n * 36);
         d.evalPdf = reinterpret_cast<float*>(ob + n * 48);
-        float ms = 0.0f;
-        cudaError_t e = (flags & VLRB_BSDF_BATCH_CONTRACTED) ? vlrb::launchBsdfBatchContracted(d, nullptr, &ms)
-                                                              : vlrb::launchBsdfBatch(d, nullptr, &ms);
+        if (e != cudaSuccess) return VLRResult_InternalError;
+        cudaEventRecord(st.e0, s);
+        e = (flags & VLRB_BSDF_BATCH_CONTRACTED) ? vlrb::launchBsdfBatchContracted(d, s, nullptr)
+                                                 : vlrb::launchBsdfBatch(d, s, nullptr);
+        cudaEventRecord(st.e1, s);
         if (e != cudaSuccess)
             return VLRResult_InternalError;
-        cudaMemcpy(batch->value, d.value, n * 16, cudaMemcpyDeviceToHost);
-        cudaMemcpy(batch->evalValue, d.evalValue, n * 16, cudaMemcpyDeviceToHost);
-        cudaMemcpy(batch->pdf, d.pdf, n * 4, cudaMemcpyDeviceToHost);
-        cudaMemcpy(batch->wi, d.wi, n * 12, cudaMemcpyDeviceToHost);
-        e = cudaMemcpy(batch->evalPdf, d.evalPdf, n * 4, cudaMemcpyDeviceToHost);
-        if (kernelMs) *kernelMs = ms;
+        const struct { void* dst; const void* src; size_t bytes; } back[5] = {
+            { batch->value, d.value, n * 16 }, { batch->evalValue, d.evalValue, n * 16 },
+            { batch->pdf, d.pdf, n * 4 }, { batch->wi, d.wi, n * 12 }, { batch->evalPdf, d.evalPdf, n * 4 } };
+        for (const auto &b : back)
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b.dst, b.src, b.bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && kernelMs) e = cudaEventElapsedTime(kernelMs, st.e0, st.e1);
         return e == cudaSuccess ? VLRResult_NoError : VLRResult_InternalError;
     }
     catch (const std::exception &ex) {
