@@ -93,13 +93,15 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-def bsdf_batch_host(inputs, contracted=False):
+def bsdf_batch_host(inputs, contracted=False, outputs=None):
     """Run the BSDF batch from host numpy arrays (copies in and out).
     contracted: run the copy of the kernel compiled with FMA contraction (the
-    renderers' arithmetic) instead of the exactly rounded one.
+    renderers' arithmetic) instead of the exactly rounded one.  outputs: host
+    arrays to write (e.g. pinned), else new ones.
     Returns (outputs dict, kernel milliseconds)."""
     n = len(inputs["material"])
-    outs = {k: np.zeros((n, c) if c > 1 else n, np.float32) for k, c in BATCH_OUTPUTS.items()}
+    outs = outputs if outputs is not None else \
+        {k: np.zeros((n, c) if c > 1 else n, np.float32) for k, c in BATCH_OUTPUTS.items()}
     ins = {k: np.ascontiguousarray(inputs[k]) for k in BATCH_INPUTS}
     b = _BsdfBatch(n, *[_ptr(ins[k]).value for k in BATCH_INPUTS],
                    *[_ptr(outs[k]).value for k in BATCH_OUTPUTS])
