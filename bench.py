@@ -776,12 +776,12 @@ def batch_workload():
 #          + next-queue append 4 + shadow ray 48                      = 412 B / hit
 #   shadow: shadow ray 48 + contribution read-modify-write 32        = 80 B / shadow ray
 STAGE_BYTES = {"trace": 56, "shade": 412, "shadow": 80}
-# DRAM bytes per path segment measured on this workload at the autotuned
-# launch configuration (2^25 paths in flight, 32 blocks per SM):
-# dram__bytes_read.sum + dram__bytes_write.sum summed over the 16 launches of
-# each stage in one 256-spp step (ncu, one pass), divided by that step's
-# 149,354,856 segments.
-STAGE_DRAM_BYTES_PER_SEGMENT = {"trace": 82.6, "shade": 426.9, "shadow": 44.3}
+# DRAM bytes per path segment of each stage: dram__bytes_read.sum +
+# dram__bytes_write.sum over the 8 bounces of one launch of this workload at
+# 2^22 paths in flight (ncu, one pass), divided by that launch's segments
+# (one sixteenth of a 256-spp step); the bench's own launches (2^25 paths)
+# keep less path state in L2 and measured 1.19x these figures.
+STAGE_DRAM_BYTES_PER_SEGMENT = {"trace": 69.0, "shade": 357.7, "shadow": 38.2}
 
 
 def main():
@@ -916,7 +916,8 @@ def main():
                 "peak_source": peak_kind,
                 "stage_ms_per_step": {k: v["ms"] / 2 for k, v in stages.items()}}
     roofline["traffic"] = STAGE_DRAM_BYTES_PER_SEGMENT[dominant] * rays / max(st["launches"], 1)
-    roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum per segment on this workload"
+    roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per segment of this workload "
+                                  "captured at 2^22 paths in flight, scaled by this launch's segments")
 
     workloads = None
     if rank == 0 and world == 1 and not args.no_workloads:
