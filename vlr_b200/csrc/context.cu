@@ -758,6 +758,9 @@ void Context::buildScene(cudaStream_t stream) {
     sg.bounds.hi = f.hi;
     sg.bounds.center = (f.lo + f.hi) * 0.5f;
     sg.bounds.worldRadius = (f.hi - sg.bounds.center).length();
+    // A scene without extent (no geometry, or one point) still needs a disc
+    // for the environment's light subpaths and its density: a unit radius.
+    if (!(sg.bounds.worldRadius > 0.0f)) sg.bounds.worldRadius = 1.0f;
     sg.bounds.worldDiscArea = kPi * sg.bounds.worldRadius * sg.bounds.worldRadius;
 
     // ---- BVH
