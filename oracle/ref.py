@@ -30,6 +30,17 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _camera_array(camera):
+    """The restatements' camera record: position, orientation (x, y, z, w),
+    aspect, sensitivity, fovy, lens radius, op distance, kind (0
+    perspective, 1 equirectangular), h angle, v angle."""
+    equi = camera.get("type", "Perspective") == "Equirectangular"
+    return np.array(list(camera["position"]) + list(camera["orientation"]) +
+                    [camera.get("aspect", 1.0), camera["sensitivity"], camera.get("fovy", 1.0),
+                     0.0 if equi else camera["lens radius"], camera.get("op distance", 1.0),
+                     1.0 if equi else 0.0, camera.get("h angle", 0.0), camera.get("v angle", 0.0)], np.float32)
+
+
 def bsdf_batch(inputs, threads=0):
     """Run the reference BSDF classes over a batch (see vlrref_bsdf_batch)."""
     n = len(inputs["material"])
@@ -92,9 +103,7 @@ def pt_render(flat, camera, width, height, spp, max_path_length, rng_states=None
         rng_states = seed_states(width * height)
     if film is None:
         film = np.zeros((height, width, 16), np.float64)
-    cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
-                   [camera["aspect"], camera["sensitivity"], camera["fovy"], camera["lens radius"],
-                    camera["op distance"]], np.float32)
+    cam = _camera_array(camera)
     seg = ctypes.c_uint64()
     rc = lib().vlrref_pt_render(
         _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),
@@ -124,9 +133,7 @@ def bpt_render(flat, camera, width, height, frames, max_path_length, num_light_p
                  "wl": np.zeros(1, np.uint64)}
     if film is None:
         film = np.zeros((height, width, 16), np.float64)
-    cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
-                   [camera["aspect"], camera["sensitivity"], camera["fovy"], camera["lens radius"],
-                    camera["op distance"]], np.float32)
+    cam = _camera_array(camera)
     seg, nlv = ctypes.c_uint64(), ctypes.c_uint64()
     rc = lib().vlrref_bpt_render(
         _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),
@@ -147,9 +154,7 @@ def pt_camera_rays(flat, camera, width, height, max_path_length, rng_states=None
     if rng_states is None:
         rng_states = seed_states(width * height)
     film = np.zeros((height, width, 16), np.float64)
-    cam = np.array(list(camera["position"]) + list(camera["orientation"]) +
-                   [camera["aspect"], camera["sensitivity"], camera["fovy"], camera["lens radius"],
-                    camera["op distance"]], np.float32)
+    cam = _camera_array(camera)
     rays = np.zeros((width * height, 8), np.float32)
     rc = lib().vlrref_pt_camera_rays(
         _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),

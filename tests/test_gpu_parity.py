@@ -755,6 +755,40 @@ def test_equirectangular_camera_renderers_agree(angles):
     assert np.all(z < 6), z.max()
 
 
+@needs_ref
+@pytest.mark.parametrize("angles", [(2 * np.pi, np.pi), (np.pi, 0.5 * np.pi)])
+def test_equirectangular_camera_same_seed_as_the_oracle(angles):
+    """The equirectangular camera against the CPU restatement of
+    path_tracing.cu with EquirectangularCamera_sample and its IDF
+    (cameras.cu:226-288): same seeds, one sample per pixel per launch, 4
+    frames of the Cornell box (GGX metal and glass) seen from inside: RNG
+    state identical on at least 99% of pixels and, on those, CIE Y within
+    1e-4 on 99% and the total within 1e-3."""
+    from vlr_b200 import vlr as VV, scenes
+    W, H = 64, 32
+    desc = scenes.cornell_box_desc(W, H)
+    desc["camera"] = {"type": "Equirectangular", "position": (0.0, 1.4, 0.8),
+                      "orientation": VV.quat_rotate_y(np.pi), "sensitivity": 1.0,
+                      "h angle": float(angles[0]), "v angle": float(angles[1])}
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = scenes.build(ctx, desc)
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=8, max_paths_in_flight=W * H)
+    ctx.render_samples(cam, True, 4)
+    g_states = ctx.read_pixel_rng_states()
+    gy = _y_of(ctx.read_film()).ravel()
+    ctx.close()
+    cfilm, c_states, _ = ref.pt_render(scenes.flatten_desc(desc), desc["camera"], W, H, 4, 8,
+                                       rng_states=ref.seed_states(W * H))
+    cy = _y_of(cfilm).ravel()
+    same = g_states == c_states
+    assert same.mean() >= 0.99, same.mean()
+    rel = (np.abs(gy - cy) / np.maximum(np.abs(cy), 1e-3 * cy.mean()))[same]
+    assert np.mean(rel <= 1e-4) >= 0.99, np.mean(rel <= 1e-4)
+    assert abs(gy[same].sum() / cy[same].sum() - 1) < 1e-3, gy[same].sum() / cy[same].sum()
+
+
 def test_shrunk_preview_fills_the_top_left_region():
     """vlrContextRender's shrinkCoeff (context.cpp:1414): a first frame with
     shrinkCoeff 2 renders the image at half size into the film's top-left
