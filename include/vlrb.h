@@ -266,9 +266,10 @@ VLRResult vlrbBvhBuildOptimizedHost(const float* triVerts, uint32_t n, uint32_t 
  *   tris[n x 48 bytes]       triangles in sorted order.
  * Work is enqueued on `stream`.  One scratch per device: calls on the same
  * device must not overlap (serialise them on one stream or synchronise
- * between them).  The first call on a device does a one-time set-up; make it
- * before any stream capture.  No scratch byte needs an initial value.  The
- * set-up is kept for the process: no cudaDeviceReset between calls.  For
+ * between them).  The first call on a device does a one-time set-up (it
+ * looks up the scratch's device address, which loads this library's device
+ * code).  No scratch byte needs an initial value.  The set-up is kept for the
+ * process: no cudaDeviceReset between calls.  For
  * n == 1 children, nodeBoxes and nodes are not written and may be NULL.
  * ---------------------------------------------------------------------- */
 #define VLRB_BVH_NO_ALLOC_MAX_TRIANGLES 65536u

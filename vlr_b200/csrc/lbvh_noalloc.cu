@@ -20,7 +20,7 @@
 //     parent links, arrival counters) before using it;
 //   * the first call on a device performs a one-time set-up for that device
 //     (the symbol lookup below, which makes the runtime load this file's
-//     device code): make that first call before any stream capture begins;
+//     device code);
 //   * the looked-up address is kept for the life of the process, so a
 //     device reset (cudaDeviceReset) between calls is not supported: the
 //     reset unloads the module and the kept address no longer points at it.
