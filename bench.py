@@ -342,7 +342,7 @@ BATCH_BYTES_PER_QUERY = 116     # in: wo 12, material 4, roughness 8, ior 4, alb
 # ncu, one launch of the 2^20-query batch (--set full): DRAM bytes read +
 # written, FMA-pipe and issue-active fractions; the kernel is issue/latency
 # bound inside the GGX BSDFs, so these stand beside its HBM fraction.
-BATCH_NCU = {"dram_bytes": 161.8e6 + 76.6e6, "fma_pipe": 0.179, "issue": 0.365}
+BATCH_NCU = {"dram_bytes": 177.8e6 + 93.7e6, "fma_pipe": 0.243, "issue": 0.480}
 
 
 def bsdf_batch_workload(hbm_peak):

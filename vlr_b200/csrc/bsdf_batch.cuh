@@ -181,7 +181,10 @@ __device__ __forceinline__ void shadeQueryOfKind(uint32_t kind, const BsdfBatchA
 }
 
 // Queries arrive in random material order.  One launch of persistent warps;
-// each warp takes a tile of kWarpTile consecutive queries at a time: it reads
+// each warp owns an equal contiguous share of the queries (every resident
+// warp busy, balanced by count: the kernel is latency-bound, so the number
+// of warps in flight matters more than the sort's fill) and works through
+// it in tiles of at most kWarpTile queries: for each tile it reads
 // the tile's material ids (coalesced), counting-sorts the tile's indices by
 // BSDF kind into its own shared-memory list (ballot + popcount, no block
 // barrier), each kind's run padded to a multiple of 32, then shades 32 sorted
@@ -197,28 +200,33 @@ constexpr int kWarpTilePerLane = kWarpTile / 32;
 constexpr uint32_t kBatchKinds = 7;
 constexpr int kWarpSlots = ((kWarpTile + kBatchKinds * 31) + 31) / 32 * 32;
 constexpr uint16_t kBatchPad = 0xFFFFu;
+constexpr int64_t kMinWarpQueries = 64;   // fewer warps than resident for small batches
 
 __global__ void __launch_bounds__(kBatchThreads, 3) bsdfBatchKernel(BsdfBatchArgs a) {
     __shared__ uint16_t sIdx[kBatchWarps][kWarpSlots];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lanesBelow = (1u << lane) - 1u;
     uint16_t* idx = sIdx[warp];
-    const int64_t numTiles = (a.n + kWarpTile - 1) / kWarpTile;
     const int64_t warpId = static_cast<int64_t>(blockIdx.x) * kBatchWarps + warp;
     const int64_t numWarps = static_cast<int64_t>(gridDim.x) * kBatchWarps;
-    for (int64_t tile = warpId; tile < numTiles; tile += numWarps) {
-        const int64_t base = tile * kWarpTile;
-        const int count = static_cast<int>(a.n - base < kWarpTile ? a.n - base : kWarpTile);
+    // shares in multiples of 8 queries: every share starts on a 32-byte
+    // sector of every input and output array (4, 8, 12 and 16 B per query)
+    const int64_t per = ((a.n + numWarps - 1) / numWarps + 7) & ~int64_t(7);
+    const int64_t start = warpId * per < a.n ? warpId * per : a.n;
+    const int64_t end = start + per < a.n ? start + per : a.n;
+    for (int64_t base = start; base < end; base += kWarpTile) {
+        const int count = static_cast<int>(end - base < kWarpTile ? end - base : kWarpTile);
         // material kinds of this lane's 16 queries, 3 bits each (7 = none)
-        uint64_t packed = 0;
+        uint64_t packed = ~0ull;     // kind 7 (none) in every unread slot
         uint32_t counts[kBatchKinds];
 #pragma unroll
         for (uint32_t k = 0; k < kBatchKinds; ++k) counts[k] = 0;
 #pragma unroll
         for (int j = 0; j < kWarpTilePerLane; ++j) {
+            if (j * 32 >= count) break;
             const int li = j * 32 + static_cast<int>(lane);
             const uint32_t kind = li < count ? batchKind(__ldg(a.mat + base + li)) : kBatchKinds;
-            packed |= static_cast<uint64_t>(kind) << (3 * j);
+            packed &= ~(static_cast<uint64_t>(7u ^ kind) << (3 * j));
 #pragma unroll
             for (uint32_t k = 0; k < kBatchKinds; ++k) counts[k] += __popc(__ballot_sync(0xFFFFFFFFu, kind == k));
         }
@@ -233,6 +241,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) bsdfBatchKernel(BsdfBatchArg
         for (uint32_t k = 0; k < kBatchKinds; ++k) fill[k] = off[k];
 #pragma unroll
         for (int j = 0; j < kWarpTilePerLane; ++j) {
+            if (j * 32 >= count) break;
             const uint32_t kind = static_cast<uint32_t>(packed >> (3 * j)) & 7u;
 #pragma unroll
             for (uint32_t k = 0; k < kBatchKinds; ++k) {
@@ -275,11 +284,11 @@ inline cudaError_t launch(const VLRBBsdfBatch &b, cudaStream_t stream, float* ke
     MengTables ht = hostMengTables();
     a.oneIOR = mengUpsample(ht, hm, SpType::IOR, ColorSp::Rec709, 1.0f, 1.0f, 1.0f);
     a.zeroIOR = mengUpsample(ht, hm, SpType::IOR, ColorSp::Rec709, 0.0f, 0.0f, 0.0f);
-    // Persistent grid: every resident CTA slot of every SM, warp tiles
-    // strided over all warps.
-    const int64_t numTiles = (b.count + kWarpTile - 1) / kWarpTile;
+    // Persistent grid: every resident CTA slot of every SM (fewer for small
+    // batches, at least kMinWarpQueries queries per warp).
     const int64_t resident = static_cast<int64_t>(numSMs) * perSM;
-    const int64_t needed = (numTiles + kBatchWarps - 1) / kBatchWarps;
+    const int64_t warpsWanted = (b.count + kMinWarpQueries - 1) / kMinWarpQueries;
+    const int64_t needed = (warpsWanted + kBatchWarps - 1) / kBatchWarps;
     const int blocks = static_cast<int>(needed < resident ? needed : resident);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (kernelMs) {
