@@ -188,6 +188,59 @@ def env_set(env=None, mode=0, tex_weight_rounding=0):
                          ctypes.c_int(mode), ctypes.c_int(tex_weight_rounding))
 
 
+def points_set(points=None, color_space=1, intensity=(1.0, 1.0, 1.0), scale=1.0):
+    """Point emitters of the following pt_render calls: one PointSurfaceNode
+    with a PointEmitter material, its points an (n, 9) array of world-space
+    position, normal and tangent; intensity in color space `color_space`
+    (0 Rec709 sRGB gamma, 1 Rec709 linear, 2 XYZ, 3 xyY).  The node is the
+    light instance after the meshes' instances.  None removes it."""
+    if points is None:
+        lib().vlrref_pt_set_points(None, ctypes.c_uint32(0), ctypes.c_int32(1), None, ctypes.c_float(1.0))
+        return
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 9)
+    inten = np.array(intensity, np.float32)
+    lib().vlrref_pt_set_points(_p(pts), ctypes.c_uint32(len(pts)), ctypes.c_int32(color_space), _p(inten),
+                               ctypes.c_float(scale))
+
+
+def texture_set(material=-1, rgba=None, uv=None, nearest=False, color_space=1, weight_rounding=0):
+    """Image2DTexture on the albedo of Matte material `material` (index in
+    the flattened material records) for the following pt_render calls: an
+    (h, w, 4) float image (row 0 at v = 0) in color space `color_space`,
+    nearest or linear filtering, repeat wrapping, and the scene's per-vertex
+    texture coordinates (flatten_desc's "uv").  weight_rounding: how the
+    linear filter's weights are held in 8 fractional bits, 0 rounded to
+    nearest, 1 rounded down (shared with the environment texture).
+    material = -1 removes it."""
+    if material < 0 or rgba is None:
+        lib().vlrref_pt_set_texture(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0,
+                                    ctypes.c_int32(1), None, ctypes.c_uint32(0), ctypes.c_int(0))
+        return
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    tc = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    lib().vlrref_pt_set_texture(ctypes.c_int32(material), _p(img), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                                ctypes.c_int(1 if nearest else 0), ctypes.c_int32(color_space), _p(tc),
+                                ctypes.c_uint32(len(tc)), ctypes.c_int(weight_rounding))
+
+
+def normal_map_set(group=-1, rgba=None, uv=None, nearest=False, directx=False, coeff=1.0):
+    """Normal map (Image2DTexture read through its xyz plug, (n + 1) / 2 per
+    texel) on geometry group `group` of the following pt_render calls,
+    DirectX or OpenGL convention, the bump coefficient as the kernels receive
+    it, the scene's per-vertex texture coordinates.  group = -1 removes it."""
+    if group < 0 or rgba is None:
+        lib().vlrref_pt_set_normal_map(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0, 0,
+                                       ctypes.c_float(1.0), None, ctypes.c_uint32(0))
+        return
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    tc = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    lib().vlrref_pt_set_normal_map(ctypes.c_int32(group), _p(img), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                                   ctypes.c_int(1 if nearest else 0), ctypes.c_int(1 if directx else 0),
+                                   ctypes.c_float(coeff), _p(tc), ctypes.c_uint32(len(tc)))
+
+
 def env_unsampleable():
     """Texels with positive luminance that the importance map can never
     sample (zero CDF step): FP64 full-resolution map, the same map built by

@@ -339,3 +339,122 @@ def test_fp64_oracle_is_the_reference_algorithm_in_double():
             sel = mat == m
             d = np.abs(a2[sel] - b2[sel]).max(axis=1) / np.maximum(np.abs(b2[sel]).max(axis=1), 1e-30)
             assert np.median(d) < 1e-4, (k, m, np.median(d))
+
+
+def _point_lit_desc(W, H):
+    """The Cornell box description with every material diffuse and the
+    ceiling light turned into a plain Matte quad (the scene the point-light
+    tests light with one point at (0, 2.4, 0))."""
+    from vlr_b200 import scenes
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    desc["materials"]["light"] = ("Matte", {"albedo": ("Rec709(D65)", 0.8, 0.8, 0.8)})
+    return desc
+
+
+BULB = np.array([[0.0, 2.4, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0]], np.float32)
+
+
+@needs_ref
+def test_oracle_point_emitter_is_linear_in_its_intensity():
+    """The oracle's point emitter (samplePoint, point.cu:38-80, with the
+    reference's PointEDF, materials.cu:2194-2250): with the same seeds,
+    doubling the PointEmitter's scale doubles every film value exactly
+    (the light enters each path's contribution as one factor, and the
+    Russian roulette does not see it); without the point the box has no
+    light at all; the LVC-BPT restatement refuses point emitters."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = _point_lit_desc(W, H)
+    flat = scenes.flatten_desc(desc)
+    films = []
+    try:
+        for scale in (1.0, 2.0):
+            ref.points_set(BULB, 1, (4.0, 4.0, 4.0), scale)
+            f, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
+            films.append(f)
+        with pytest.raises(AssertionError):
+            ref.bpt_render(flat, desc["camera"], W, H, 1, 6, W * H)
+    finally:
+        ref.points_set(None)
+    assert np.isfinite(films[0]).all() and films[0].sum() > 0
+    assert np.array_equal(films[1], 2 * films[0])
+    dark, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
+    assert dark.sum() == 0.0
+
+
+def _poster_desc(W, H, albedo=("Rec709(D65)", 0.5, 0.5, 0.5)):
+    """The diffuse Cornell box with its back wall split off as a "poster"
+    material (u left to right, v bottom to top across the wall)."""
+    from vlr_b200 import scenes
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    desc["materials"]["poster"] = ("Matte", {"albedo": albedo})
+    mesh = desc["meshes"][0]
+    verts = mesh["verts"].copy()
+    verts[4:8, 9:11] = [[0, 0], [1, 0], [1, 1], [0, 1]]
+    mesh["verts"] = verts
+    groups = [(np.array([0, 1, 2, 0, 2, 3, 8, 9, 10, 8, 10, 11], np.uint32), "white"),
+              (np.array([4, 5, 6, 4, 6, 7], np.uint32), "poster")]
+    mesh["groups"] = groups + mesh["groups"][1:]
+    return desc
+
+
+@needs_ref
+def test_oracle_texture_of_a_constant_is_the_immediate_colour():
+    """The oracle's Image2DTexture albedo (shader_nodes.cu:410-445, the
+    texture unit restated): a point-sampled texture holding the immediate
+    linear colour everywhere gives the same film, bit for bit, with the same
+    seeds; a black texture darkens the image (the poster reflects nothing);
+    the LVC-BPT restatement refuses textures."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = _poster_desc(W, H)
+    flat = scenes.flatten_desc(desc)
+    poster = list(desc["materials"]).index("poster")
+    films = []
+    for value in (None, 0.5, 0.0):
+        if value is not None:
+            ref.texture_set(poster, np.full((3, 5, 4), value, np.float32), flat["uv"], nearest=True)
+        try:
+            f, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
+            if value == 0.0:
+                with pytest.raises(AssertionError):
+                    ref.bpt_render(flat, desc["camera"], W, H, 1, 6, W * H)
+        finally:
+            ref.texture_set()
+        films.append(f)
+    assert np.array_equal(films[0], films[1])
+    assert films[2].sum() < films[0].sum()
+
+
+@needs_ref
+def test_oracle_normal_map_of_the_vertex_normal_changes_nothing():
+    """The oracle's normal map (shader_nodes.cu:349-391 with
+    applyBumpMapping, renderer_common.h:554-576): a map that stores the
+    untilted normal (0, 0, 1) leaves the film unchanged bit for bit (the
+    bump is skipped when the mapped normal has no tangential part), while a
+    tilted one changes it; the LVC-BPT restatement refuses normal maps."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = scenes.floor_desc(W, H)
+    flat = scenes.flatten_desc(desc)
+    films = []
+    for n in (None, (0.0, 0.0, 1.0), (0.3, 0.4, np.sqrt(0.75))):
+        if n is not None:
+            rgba = np.ones((2, 2, 4), np.float32)
+            rgba[..., :3] = (np.array(n) + 1) / 2
+            ref.normal_map_set(0, rgba, flat["uv"], nearest=True, coeff=17 / 16)
+        try:
+            f, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 4, rng_states=ref.seed_states(W * H))
+            if n is not None and n[0] != 0.0:
+                with pytest.raises(AssertionError):
+                    ref.bpt_render(flat, desc["camera"], W, H, 1, 4, W * H)
+        finally:
+            ref.normal_map_set()
+        films.append(f)
+    assert films[0].sum() > 0
+    assert np.array_equal(films[0], films[1])
+    assert not np.array_equal(films[0], films[2])

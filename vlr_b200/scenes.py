@@ -176,8 +176,9 @@ MAT_DTYPE = np.dtype([("type", "<i4"), ("colorSpace", "<i4", 3), ("spectra", "<f
 def flatten_desc(desc):
     """World-space arrays of a description with identity transforms, in the
     layout of the oracle's path tracer: positions, normals, tangents,
-    triangles (i0, i1, i2, group), group material, group light instance
-    (each emitting mesh is one light instance), material records."""
+    texture coordinates, triangles (i0, i1, i2, group), group material, group
+    light instance (each emitting mesh is one light instance), material
+    records."""
     names = list(desc["materials"].keys())
     recs = np.zeros(len(names), MAT_DTYPE)
     for i, name in enumerate(names):
@@ -193,12 +194,13 @@ def flatten_desc(desc):
             recs[i]["spectra"][k] = (e0, e1, e2)
         for k, slot in enumerate(FLOAT_SLOTS.get(typ, ())):
             recs[i]["params"][k] = float(params.get(slot, FLOAT_DEFAULTS[slot]))
-    pos, nrm, tan, tris, gmat, glight = [], [], [], [], [], []
+    pos, nrm, tan, uv, tris, gmat, glight = [], [], [], [], [], [], []
     base = 0
     n_light_inst = 0
     for mesh in desc["meshes"]:
         vv = mesh["verts"]
         pos.append(vv[:, 0:3]); nrm.append(vv[:, 3:6]); tan.append(vv[:, 6:9])
+        uv.append(vv[:, 9:11] if vv.shape[1] >= 11 else np.zeros((len(vv), 2), np.float32))
         emitting = False
         for idx, mname in mesh["groups"]:
             g = len(gmat)
@@ -215,6 +217,7 @@ def flatten_desc(desc):
             "nrm": np.ascontiguousarray(np.concatenate(nrm), np.float32),
             "tan": np.ascontiguousarray(np.concatenate(tan), np.float32),
             "tris": np.ascontiguousarray(np.concatenate(tris), np.uint32),
+            "uv": np.ascontiguousarray(np.concatenate(uv), np.float32),
             "groupMaterial": np.array(gmat, np.int32), "groupLightInst": np.array(glight, np.int32),
             "mats": recs}
 
@@ -472,3 +475,29 @@ def build_instanced(ctx, desc):
         scene.set_environment(em, env.get("rotation", 0.0))
         keep += [img, tex, em]
     return scene, cam, keep
+
+
+def floor_desc(W, H, light_at=(1.2, -1.2)):
+    """Description of the lit-floor scene: a 4 x 4 white floor at y = 0 (u
+    along +x, v along +z; tangent +x) and a 1 x 1 downward-facing light at
+    height 2 over `light_at` (x, z), seen by a camera at height 0.9 looking
+    straight down (40-degree field of view)."""
+    uvs = [(0, 0), (0, 1), (1, 1), (1, 0)]
+
+    def quad(corners, n, t):
+        return np.array([list(p) + list(n) + list(t) + list(uv) for p, uv in zip(corners, uvs)], np.float32)
+
+    lx, lz = light_at
+    idx = np.array([0, 1, 2, 0, 2, 3], np.uint32)
+    return {
+        "materials": {"floor": ("Matte", {"albedo": ("Rec709(D65)", 0.8, 0.8, 0.8)}),
+                      "light": ("DiffuseEmitter", {"emittance": ("Rec709(D65)", 10.0, 10.0, 10.0)})},
+        "meshes": [{"verts": quad([(-2, 0, -2), (-2, 0, 2), (2, 0, 2), (2, 0, -2)], (0, 1, 0), (1, 0, 0)),
+                    "groups": [(idx, "floor")]},
+                   {"verts": quad([(lx - .5, 2, lz - .5), (lx + .5, 2, lz - .5), (lx + .5, 2, lz + .5),
+                                   (lx - .5, 2, lz + .5)], (0, -1, 0), (1, 0, 0)),
+                    "groups": [(idx, "light")]}],
+        "camera": {"position": (0.0, 0.9, 0.0), "orientation": (np.sqrt(0.5), 0.0, 0.0, np.sqrt(0.5)),
+                   "aspect": W / H, "sensitivity": 1.0, "fovy": 40 * np.pi / 180, "lens radius": 0.0,
+                   "op distance": 1.0},
+    }
