@@ -208,9 +208,9 @@ def texture_set(material=-1, rgba=None, uv=None, nearest=False, color_space=1, w
     the flattened material records) for the following pt_render calls: an
     (h, w, 4) float image (row 0 at v = 0) in color space `color_space`,
     nearest or linear filtering, repeat wrapping, and the scene's per-vertex
-    texture coordinates (flatten_desc's "uv").  weight_rounding: how the
-    linear filter's weights are held in 8 fractional bits, 0 rounded to
-    nearest, 1 rounded down (shared with the environment texture).
+    texture coordinates (flatten_desc's "uv").  weight_rounding: the
+    linear filter's weights as the texture unit forms them (0, measured) or
+    as FP32 products (2); shared with the environment texture.
     material = -1 removes it."""
     if material < 0 or rgba is None:
         lib().vlrref_pt_set_texture(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0,
