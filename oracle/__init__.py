@@ -8,7 +8,9 @@
                              reference's integrators built on them:
                                ref_pt.inc   path_tracing.cu (camera, closest
                                             hit, NEE, MIS, the environment's
-                                            miss program and importance maps)
+                                            miss program and importance maps;
+                                            point emitters, a Matte albedo
+                                            texture and a normal map on demand)
                                ref_bpt.inc  lvc_bpt.cu (light vertex cache,
                                             connections, MIS recursion);
   oracle/_build/liboracle.so our sequential restatement of the LBVH build and
