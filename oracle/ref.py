@@ -241,6 +241,25 @@ def normal_map_set(group=-1, rgba=None, uv=None, nearest=False, directx=False, c
                                    ctypes.c_float(coeff), _p(tc), ctypes.c_uint32(len(tc)))
 
 
+def alpha_map_set(group=-1, rgba=None, uv=None, nearest=False, channel=3):
+    """Alpha map (channel `channel` of an Image2DTexture) on geometry group
+    `group` of the following pt_render calls, with the scene's per-vertex
+    texture coordinates: closest-hit rays keep an intersection with the
+    CUDA build's per-(path state, primitive) decision, shadow rays carry the
+    product of (1 - alpha).  Brute-force scenes only (under 4,096
+    triangles).  group = -1 removes it."""
+    if group < 0 or rgba is None:
+        lib().vlrref_pt_set_alpha_map(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0, 3,
+                                      None, ctypes.c_uint32(0))
+        return
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    tc = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    lib().vlrref_pt_set_alpha_map(ctypes.c_int32(group), _p(img), ctypes.c_uint32(w), ctypes.c_uint32(h),
+                                  ctypes.c_int(1 if nearest else 0), ctypes.c_int(channel), _p(tc),
+                                  ctypes.c_uint32(len(tc)))
+
+
 def env_unsampleable():
     """Texels with positive luminance that the importance map can never
     sample (zero CDF step): FP64 full-resolution map, the same map built by

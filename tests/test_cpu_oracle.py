@@ -458,3 +458,33 @@ def test_oracle_normal_map_of_the_vertex_normal_changes_nothing():
     assert films[0].sum() > 0
     assert np.array_equal(films[0], films[1])
     assert not np.array_equal(films[0], films[2])
+
+
+@needs_ref
+def test_oracle_alpha_map_limits():
+    """The oracle's alpha map: with a clear sheet (alpha 0) the film is bit
+    for bit that of the scene without the sheet; an opaque one (alpha 1)
+    takes all the light (the floor is lit only through the black sheet);
+    the LVC-BPT restatement refuses alpha maps."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = scenes.floor_desc(W, H, light_at=(0.0, 0.0), sheet=True)
+    flat = scenes.flatten_desc(desc)
+    bare_desc = scenes.floor_desc(W, H, light_at=(0.0, 0.0))
+    bare, _, _ = ref.pt_render(scenes.flatten_desc(bare_desc), bare_desc["camera"], W, H, 8, 4,
+                               rng_states=ref.seed_states(W * H))
+    films = []
+    for a in (0.0, 1.0):
+        rgba = np.zeros((2, 2, 4), np.float32)
+        rgba[..., 3] = a
+        ref.alpha_map_set(2, rgba, flat["uv"], channel=3)
+        try:
+            f, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 4, rng_states=ref.seed_states(W * H))
+            with pytest.raises(AssertionError):
+                ref.bpt_render(flat, desc["camera"], W, H, 1, 4, W * H)
+        finally:
+            ref.alpha_map_set()
+        films.append(f)
+    assert bare.sum() > 0
+    assert np.array_equal(films[0], bare)
+    assert films[1].sum() == 0.0

@@ -1099,8 +1099,8 @@ def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=
     (x, z), seen by a camera at height 0.9 looking straight down.
     floor_normal: the floor's vertex normal; normal_plug: the floor group's
     nodeNormal.  blocker_alpha: a black 6 x 6 sheet at height 1, between
-    the floor and the light and above the camera, with a constant alpha map
-    of this value (None: no sheet).  floor_mat / light_mat: functions
+    the floor and the light and above the camera, with an alpha map of this
+    constant value or (h, w) array of texels (None: no sheet).  floor_mat / light_mat: functions
     (ctx, make) -> material replacing the white Matte / the emitter, where
     make(type, **spectra) creates a material with linear Rec.709 spectra."""
     from vlr_b200 import vlr as VV
@@ -1134,8 +1134,9 @@ def _floor_scene(ctx, W, H, light_at, floor_normal=(0.0, 1.0, 0.0), normal_plug=
                                    (lx - .5, 2, lz + .5)], (0, -1, 0), (1, 0, 0), uvs,
                          light_mat(ctx, mat) if light_mat else mat("DiffuseEmitter", emittance=(10.0, 10.0, 10.0))))
     if blocker_alpha is not None:
-        rgba = np.zeros((2, 2, 4), np.float32)
-        rgba[..., 3] = blocker_alpha
+        ba = np.asarray(blocker_alpha, np.float32)
+        rgba = np.zeros(ba.shape + (4,) if ba.ndim == 2 else (2, 2, 4), np.float32)
+        rgba[..., 3] = ba
         img = ctx.createLinearImage2D(rgba, "Reflectance", lin)
         tex = ctx.createShaderNode("Image2DTexture")
         tex.set("image", img)
@@ -1191,6 +1192,46 @@ def test_alpha_map_scales_the_light_through_a_sheet(renderer):
     # triangles (the ray/triangle test is not watertight): about 1e-6 of the light
     assert opaque / bare < 1e-4, opaque / bare
     assert abs(half / bare - 0.5) < 0.02, half / bare
+
+
+@needs_ref
+def test_alpha_map_same_seed_as_the_oracle():
+    """A 4 x 4 random alpha map (bilinear) on the black sheet between the
+    floor and its light against the CPU restatement of path_tracing.cu with
+    the alpha node (shader_nodes.cu:437-455): fractional visibility of
+    shadow rays (light_transport_common.h:206-219) and the stochastic alpha
+    test of scattered rays (path_tracing.cu:15-25, with the CUDA build's
+    per-(path state, primitive) decision): same seeds, one sample per pixel
+    per launch, 4 frames: RNG state identical on at least 99% of pixels and,
+    on those, CIE Y within 1e-4 on 99% and the total within 1e-3."""
+    from vlr_b200 import vlr as VV, scenes
+    W = H = 48
+    alpha = np.random.default_rng(29).uniform(0.0, 1.0, (4, 4)).astype(np.float32)
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = _floor_scene(ctx, W, H, light_at=(0.0, 0.0), blocker_alpha=alpha)
+    ctx.setScene(scene)
+    ctx.setOptions(max_path_length=4, max_paths_in_flight=W * H)
+    ctx.render_samples(cam, True, 4)
+    g_states = ctx.read_pixel_rng_states()
+    gy = _y_of(ctx.read_film()).ravel()
+    ctx.close()
+    desc = scenes.floor_desc(W, H, light_at=(0.0, 0.0), sheet=True)
+    flat = scenes.flatten_desc(desc)
+    rgba = np.zeros((4, 4, 4), np.float32)
+    rgba[..., 3] = alpha
+    ref.alpha_map_set(2, rgba, flat["uv"], channel=3)
+    try:
+        cfilm, c_states, _ = ref.pt_render(flat, desc["camera"], W, H, 4, 4, rng_states=ref.seed_states(W * H))
+    finally:
+        ref.alpha_map_set()
+    cy = _y_of(cfilm).ravel()
+    assert cy.sum() > 0
+    same = g_states == c_states
+    assert same.mean() >= 0.99, same.mean()
+    rel = (np.abs(gy - cy) / np.maximum(np.abs(cy), 1e-3 * cy.mean()))[same]
+    assert np.mean(rel <= 1e-4) >= 0.99, np.mean(rel <= 1e-4)
+    assert abs(gy[same].sum() / cy[same].sum() - 1) < 1e-3, gy[same].sum() / cy[same].sum()
 
 
 def _normal_map_node(ctx, local_normal, bump_type, extra=()):

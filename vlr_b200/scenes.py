@@ -477,11 +477,12 @@ def build_instanced(ctx, desc):
     return scene, cam, keep
 
 
-def floor_desc(W, H, light_at=(1.2, -1.2)):
+def floor_desc(W, H, light_at=(1.2, -1.2), sheet=False):
     """Description of the lit-floor scene: a 4 x 4 white floor at y = 0 (u
     along +x, v along +z; tangent +x) and a 1 x 1 downward-facing light at
     height 2 over `light_at` (x, z), seen by a camera at height 0.9 looking
-    straight down (40-degree field of view)."""
+    straight down (40-degree field of view).  sheet: a black 6 x 6 sheet at
+    height 1 between them (its third group, for an alpha map)."""
     uvs = [(0, 0), (0, 1), (1, 1), (1, 0)]
 
     def quad(corners, n, t):
@@ -491,12 +492,15 @@ def floor_desc(W, H, light_at=(1.2, -1.2)):
     idx = np.array([0, 1, 2, 0, 2, 3], np.uint32)
     return {
         "materials": {"floor": ("Matte", {"albedo": ("Rec709(D65)", 0.8, 0.8, 0.8)}),
-                      "light": ("DiffuseEmitter", {"emittance": ("Rec709(D65)", 10.0, 10.0, 10.0)})},
+                      "light": ("DiffuseEmitter", {"emittance": ("Rec709(D65)", 10.0, 10.0, 10.0)}),
+                      "sheet": ("Matte", {"albedo": ("Rec709(D65)", 0.0, 0.0, 0.0)})},
         "meshes": [{"verts": quad([(-2, 0, -2), (-2, 0, 2), (2, 0, 2), (2, 0, -2)], (0, 1, 0), (1, 0, 0)),
                     "groups": [(idx, "floor")]},
                    {"verts": quad([(lx - .5, 2, lz - .5), (lx + .5, 2, lz - .5), (lx + .5, 2, lz + .5),
                                    (lx - .5, 2, lz + .5)], (0, -1, 0), (1, 0, 0)),
-                    "groups": [(idx, "light")]}],
+                    "groups": [(idx, "light")]}] +
+                  ([{"verts": quad([(-3, 1, -3), (3, 1, -3), (3, 1, 3), (-3, 1, 3)], (0, -1, 0), (1, 0, 0)),
+                     "groups": [(idx, "sheet")]}] if sheet else []),
         "camera": {"position": (0.0, 0.9, 0.0), "orientation": (np.sqrt(0.5), 0.0, 0.0, np.sqrt(0.5)),
                    "aspect": W / H, "sensitivity": 1.0, "fovy": 40 * np.pi / 180, "lens radius": 0.0,
                    "op distance": 1.0},
