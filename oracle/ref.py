@@ -260,6 +260,18 @@ def alpha_map_set(group=-1, rgba=None, uv=None, nearest=False, channel=3):
                                   ctypes.c_uint32(len(tc)))
 
 
+def multi_set(material=-1, subs=()):
+    """Multi material of the following pt_render calls: material index
+    `material` (in the flattened records) stands for the sum of the BSDFs of
+    the 1-4 sub-material indices `subs`, as the reference's MultiBSDF
+    samples, evaluates and blends them.  material = -1 removes it."""
+    if material < 0 or not len(subs):
+        lib().vlrref_pt_set_multi(ctypes.c_int32(-1), None, ctypes.c_uint32(0))
+        return
+    arr = np.array(subs, np.int32)
+    lib().vlrref_pt_set_multi(ctypes.c_int32(material), _p(arr), ctypes.c_uint32(len(arr)))
+
+
 def env_unsampleable():
     """Texels with positive luminance that the importance map can never
     sample (zero CDF step): FP64 full-resolution map, the same map built by

@@ -488,3 +488,32 @@ def test_oracle_alpha_map_limits():
     assert bare.sum() > 0
     assert np.array_equal(films[0], bare)
     assert films[1].sum() == 0.0
+
+
+@needs_ref
+def test_oracle_multi_material_of_two_mattes_is_their_sum():
+    """The oracle's Multi material (the reference's MultiBSDF,
+    materials.cu:2255-2532, restated over its BSDF classes): a Multi of grey
+    Mattes 0.3 and 0.4 samples the same cosine direction from the same
+    numbers as one Matte 0.7, with the summed value (Meng spectra of one
+    chromaticity scale with brightness) and the blended density of two equal
+    pdfs, so the film matches Matte 0.7's with the same seeds to float
+    round-off; the LVC-BPT restatement refuses Multi materials."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = scenes.floor_desc(W, H, light_at=(0.6, 0.0))
+    desc["materials"]["floor"] = ("Matte", {"albedo": ("Rec709(D65)", 0.7, 0.7, 0.7)})
+    desc["materials"]["sub0"] = ("Matte", {"albedo": ("Rec709(D65)", 0.3, 0.3, 0.3)})
+    desc["materials"]["sub1"] = ("Matte", {"albedo": ("Rec709(D65)", 0.4, 0.4, 0.4)})
+    flat = scenes.flatten_desc(desc)
+    names = list(desc["materials"])
+    single, _, _ = ref.pt_render(flat, desc["camera"], W, H, 16, 4, rng_states=ref.seed_states(W * H))
+    ref.multi_set(names.index("floor"), [names.index("sub0"), names.index("sub1")])
+    try:
+        multi, _, _ = ref.pt_render(flat, desc["camera"], W, H, 16, 4, rng_states=ref.seed_states(W * H))
+        with pytest.raises(AssertionError):
+            ref.bpt_render(flat, desc["camera"], W, H, 1, 4, W * H)
+    finally:
+        ref.multi_set()
+    assert single.sum() > 0
+    assert np.allclose(multi, single, rtol=1e-5, atol=1e-6 * single.max())

@@ -1614,6 +1614,61 @@ def test_multi_material_sums_its_bsdfs(renderer):
     assert np.allclose(a2[..., :3].mean(axis=(0, 1)), a1[..., :3].mean(axis=(0, 1)), rtol=0.01)
 
 
+@needs_ref
+def test_multi_material_per_pixel_against_the_oracle():
+    """A Multi of a Matte and a GGX metal (roughness 0.4) on the lit floor
+    against the CPU restatement of path_tracing.cu with the reference's
+    MultiBSDF (materials.cu:2255-2532: a component chosen by the BSDFs'
+    weights, the summed value, the weight-blended density).  The CUDA build
+    picks one component uniformly and weighs it by 2, another estimator of
+    the same sum, so the check is per pixel in expectation: 8 GPU batches of
+    4096 spp against 8 oracle batches of 1024 spp from distinct seeds, every
+    lit pixel within 4 combined standard errors on 99% of pixels (median
+    standard error at most 3% of the pixel), totals within 1%."""
+    from vlr_b200 import vlr as VV, scenes
+    W = H = 48
+    metal = {"eta": (0.2, 0.4, 1.4), "k": (3.5, 2.5, 1.9)}
+
+    def floor_mat(ctx, make):
+        a = make("Matte", albedo=(0.3, 0.3, 0.3))
+        b = make("MicrofacetReflection", **metal)
+        b.set("roughness", 0.4)
+        m = ctx.createSurfaceMaterial("Multi")
+        m.set("0", a)
+        m.set("1", b)
+        return m
+
+    g_b = []
+    ctx = VV.Context()
+    ctx.bindOutputBuffer(W, H)
+    scene, cam, keep = _floor_scene(ctx, W, H, light_at=(0.6, 0.0), floor_mat=floor_mat)
+    ctx.setScene(scene)
+    for k in range(8):
+        ctx.setOptions(max_path_length=4, rng_seed=3000 + k)
+        ctx.render_samples(cam, True, 4096)
+        g_b.append(_y_of(ctx.read_film()) / 4096)
+    ctx.close()
+    desc = scenes.floor_desc(W, H, light_at=(0.6, 0.0))
+    lin = "Rec709(D65)"
+    desc["materials"]["sub0"] = ("Matte", {"albedo": (lin, 0.3, 0.3, 0.3)})
+    desc["materials"]["sub1"] = ("MicrofacetReflection", {"eta": (lin,) + metal["eta"], "k": (lin,) + metal["k"],
+                                                          "roughness": 0.4})
+    flat = scenes.flatten_desc(desc)
+    names = list(desc["materials"])
+    ref.multi_set(names.index("floor"), [names.index("sub0"), names.index("sub1")])
+    c_b = []
+    try:
+        for k in range(8):
+            cfilm, _, _ = ref.pt_render(flat, desc["camera"], W, H, 1024, 4,
+                                        rng_states=ref.seed_states(W * H, 4000 + k))
+            c_b.append(_y_of(cfilm) / 1024)
+    finally:
+        ref.multi_set()
+    g_tot, c_tot = np.sum(g_b), np.sum(c_b)
+    assert abs(g_tot / c_tot - 1) < 0.01, g_tot / c_tot
+    _per_pixel_batches_agree(g_b, c_b)
+
+
 @pytest.mark.parametrize("renderer", ["path_tracing", "bpt"])
 def test_multi_material_emits_the_sum_of_its_emitters(renderer):
     """MultiEDF (materials.cu:2600-2823): a Multi of two diffuse emitters
