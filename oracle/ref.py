@@ -224,20 +224,23 @@ def texture_set(material=-1, rgba=None, uv=None, nearest=False, color_space=1, w
                                 ctypes.c_uint32(len(tc)), ctypes.c_int(weight_rounding))
 
 
-def normal_map_set(group=-1, rgba=None, uv=None, nearest=False, directx=False, coeff=1.0):
-    """Normal map (Image2DTexture read through its xyz plug, (n + 1) / 2 per
-    texel) on geometry group `group` of the following pt_render calls,
-    DirectX or OpenGL convention, the bump coefficient as the kernels receive
-    it, the scene's per-vertex texture coordinates.  group = -1 removes it."""
+def normal_map_set(group=-1, rgba=None, uv=None, nearest=False, directx=False, coeff=1.0, height=False, channel=0):
+    """Normal map on geometry group `group` of the following pt_render
+    calls: an Image2DTexture read through its xyz plug ((n + 1) / 2 per
+    texel, DirectX or OpenGL convention) or, with height=True, a height map
+    read through channel `channel` from the texture-gather footprint (repeat
+    addressing); the bump coefficient as the kernels receive it and the
+    scene's per-vertex texture coordinates.  group = -1 removes it."""
     if group < 0 or rgba is None:
-        lib().vlrref_pt_set_normal_map(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0, 0,
+        lib().vlrref_pt_set_normal_map(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0, 0, 0,
                                        ctypes.c_float(1.0), None, ctypes.c_uint32(0))
         return
     img = np.ascontiguousarray(rgba, np.float32)
     h, w = img.shape[:2]
     tc = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    kind = 2 if height else (1 if directx else 0)
     lib().vlrref_pt_set_normal_map(ctypes.c_int32(group), _p(img), ctypes.c_uint32(w), ctypes.c_uint32(h),
-                                   ctypes.c_int(1 if nearest else 0), ctypes.c_int(1 if directx else 0),
+                                   ctypes.c_int(1 if nearest else 0), ctypes.c_int(kind), ctypes.c_int(channel),
                                    ctypes.c_float(coeff), _p(tc), ctypes.c_uint32(len(tc)))
 
 

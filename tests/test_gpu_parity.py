@@ -1299,26 +1299,32 @@ def test_normal_map_tilts_the_shading_frame_like_vertex_normals(bump_type):
 
 
 @needs_ref
-@pytest.mark.parametrize("bump_type", ["Normal Map (OpenGL)", "Normal Map (DirectX)"])
+@pytest.mark.parametrize("bump_type", ["Normal Map (OpenGL)", "Normal Map (DirectX)", "Height Map"])
 def test_normal_map_same_seed_as_the_oracle(bump_type):
-    """A 4 x 4 random normal map (point-sampled, tilts up to ~37 degrees) on
-    the lit floor against the CPU restatement of path_tracing.cu with the
-    normal-map node and applyBumpMapping (shader_nodes.cu:349-391,
-    renderer_common.h:554-576; bump coefficient 17/16 as the kernels receive
-    the default): same seeds, one sample per pixel per launch, 4 frames:
-    RNG state identical on at least 99% of pixels and, on those, CIE Y
-    within 1e-4 on 99% and the total within 1e-3.  A wrong convention (the
-    DirectX y flip), rotation or texel lookup changes the floor's shading."""
+    """A 4 x 4 random normal map (point-sampled, tilts up to ~37 degrees) or
+    an 8 x 8 random height map (heights 0-20: slopes up to ~0.8, from the
+    texture-gather footprint, repeat addressing) on the lit floor against
+    the CPU restatement of path_tracing.cu with the normal-map node and
+    applyBumpMapping (shader_nodes.cu:349-391, renderer_common.h:554-576;
+    bump coefficient 17/16 as the kernels receive the default): same seeds,
+    one sample per pixel per launch, 4 frames: RNG state identical on at
+    least 99% of pixels and, on those, CIE Y within 1e-4 on 99% and the
+    total within 1e-3.  A wrong convention (the DirectX y flip, the gather
+    order), rotation or texel lookup changes the floor's shading."""
     from vlr_b200 import vlr as VV, scenes
     W = H = 48
     rng = np.random.default_rng(23)
-    n = np.concatenate([rng.uniform(-0.6, 0.6, (4, 4, 2)), np.zeros((4, 4, 1))], axis=2)
-    n[..., 2] = np.sqrt(1 - (n[..., :2] ** 2).sum(axis=2))
-    stored = n.copy()
-    if bump_type == "Normal Map (DirectX)":
-        stored[..., 1] = -stored[..., 1]
-    rgba = np.ones((4, 4, 4), np.float32)
-    rgba[..., :3] = (stored + 1) / 2
+    if bump_type == "Height Map":
+        rgba = np.ones((8, 8, 4), np.float32)
+        rgba[..., 0] = rng.uniform(0.0, 20.0, (8, 8))
+    else:
+        n = np.concatenate([rng.uniform(-0.6, 0.6, (4, 4, 2)), np.zeros((4, 4, 1))], axis=2)
+        n[..., 2] = np.sqrt(1 - (n[..., :2] ** 2).sum(axis=2))
+        stored = n.copy()
+        if bump_type == "Normal Map (DirectX)":
+            stored[..., 1] = -stored[..., 1]
+        rgba = np.ones((4, 4, 4), np.float32)
+        rgba[..., :3] = (stored + 1) / 2
     ctx = VV.Context()
     ctx.bindOutputBuffer(W, H)
     img = ctx.createLinearImage2D(rgba, "Reflectance", "Rec709(D65)")
@@ -1337,7 +1343,7 @@ def test_normal_map_same_seed_as_the_oracle(bump_type):
     desc = scenes.floor_desc(W, H, light_at=(1.2, -1.2))
     flat = scenes.flatten_desc(desc)
     ref.normal_map_set(0, rgba, flat["uv"], nearest=True, directx=bump_type == "Normal Map (DirectX)",
-                       coeff=17 / 16)
+                       coeff=17 / 16, height=bump_type == "Height Map", channel=0)
     try:
         cfilm, c_states, _ = ref.pt_render(flat, desc["camera"], W, H, 4, 4, rng_states=ref.seed_states(W * H))
     finally:
