@@ -203,25 +203,28 @@ def points_set(points=None, color_space=1, intensity=(1.0, 1.0, 1.0), scale=1.0)
                                ctypes.c_float(scale))
 
 
-def texture_set(material=-1, rgba=None, uv=None, nearest=False, color_space=1, weight_rounding=0):
+def texture_set(material=-1, rgba=None, uv=None, nearest=False, color_space=1, weight_rounding=0, scalars=False):
     """Image2DTexture on the albedo of Matte material `material` (index in
     the flattened material records) for the following pt_render calls: an
     (h, w, 4) float image (row 0 at v = 0) in color space `color_space`,
     nearest or linear filtering, repeat wrapping, and the scene's per-vertex
     texture coordinates (flatten_desc's "uv").  weight_rounding: the
     linear filter's weights as the texture unit forms them (0, measured) or
-    as FP32 products (2); shared with the environment texture.
-    material = -1 removes it."""
+    as FP32 products (2); shared with the environment texture.  scalars:
+    the texture feeds the float3 plug of a UE4 material (occlusion,
+    roughness, metallic) or a microfacet material (roughness, anisotropy,
+    rotation) instead of a Matte's albedo.  material = -1 removes it."""
     if material < 0 or rgba is None:
         lib().vlrref_pt_set_texture(ctypes.c_int32(-1), None, ctypes.c_uint32(0), ctypes.c_uint32(0), 0,
-                                    ctypes.c_int32(1), None, ctypes.c_uint32(0), ctypes.c_int(0))
+                                    ctypes.c_int32(1), None, ctypes.c_uint32(0), ctypes.c_int(0), ctypes.c_int(0))
         return
     img = np.ascontiguousarray(rgba, np.float32)
     h, w = img.shape[:2]
     tc = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
     lib().vlrref_pt_set_texture(ctypes.c_int32(material), _p(img), ctypes.c_uint32(w), ctypes.c_uint32(h),
                                 ctypes.c_int(1 if nearest else 0), ctypes.c_int32(color_space), _p(tc),
-                                ctypes.c_uint32(len(tc)), ctypes.c_int(weight_rounding))
+                                ctypes.c_uint32(len(tc)), ctypes.c_int(weight_rounding),
+                                ctypes.c_int(1 if scalars else 0))
 
 
 def normal_map_set(group=-1, rgba=None, uv=None, nearest=False, directx=False, coeff=1.0, height=False, channel=0):
