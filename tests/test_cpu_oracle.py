@@ -360,26 +360,28 @@ BULB = np.array([[0.0, 2.4, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0]], np.float32)
 def test_oracle_point_emitter_is_linear_in_its_intensity():
     """The oracle's point emitter (samplePoint, point.cu:38-80, with the
     reference's PointEDF, materials.cu:2194-2250): with the same seeds,
-    doubling the PointEmitter's scale doubles every film value exactly
-    (the light enters each path's contribution as one factor, and the
-    Russian roulette does not see it); without the point the box has no
-    light at all; the LVC-BPT restatement refuses point emitters."""
+    doubling the PointEmitter's scale doubles every film value exactly, in
+    the path tracer and in the LVC-BPT restatement (the light enters each
+    path's contribution as one factor, and neither Russian roulette nor the
+    MIS weights see it); without the point the box has no light at all."""
     from vlr_b200 import scenes
     W = H = 16
     desc = _point_lit_desc(W, H)
     flat = scenes.flatten_desc(desc)
-    films = []
+    films, bfilms = [], []
     try:
         for scale in (1.0, 2.0):
             ref.points_set(BULB, 1, (4.0, 4.0, 4.0), scale)
             f, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
             films.append(f)
-        with pytest.raises(AssertionError):
-            ref.bpt_render(flat, desc["camera"], W, H, 1, 6, W * H)
+            b, _, _, _ = ref.bpt_render(flat, desc["camera"], W, H, 8, 6, W * H)
+            bfilms.append(b)
     finally:
         ref.points_set(None)
     assert np.isfinite(films[0]).all() and films[0].sum() > 0
     assert np.array_equal(films[1], 2 * films[0])
+    assert bfilms[0].sum() > 0
+    assert np.array_equal(bfilms[1], 2 * bfilms[0])
     dark, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
     assert dark.sum() == 0.0
 
@@ -517,3 +519,20 @@ def test_oracle_multi_material_of_two_mattes_is_their_sum():
         ref.multi_set()
     assert single.sum() > 0
     assert np.allclose(multi, single, rtol=1e-5, atol=1e-6 * single.max())
+
+
+@needs_ref
+def test_oracle_directional_emitter_reaches_only_light_subpaths():
+    """The oracle's directional emitter (the reference's DirectionalEDF,
+    materials.cu:2100-2160: a delta direction, zero evaluation): the path
+    tracer restatement gets no light from it, the LVC-BPT restatement's
+    light subpaths leave it along its normal and light the box."""
+    from vlr_b200 import scenes
+    W = H = 16
+    desc = _point_lit_desc(W, H)
+    desc["materials"]["light"] = ("DirectionalEmitter", {"emittance": ("Rec709(D65)", 5.0, 5.0, 5.0)})
+    flat = scenes.flatten_desc(desc)
+    pt, _, _ = ref.pt_render(flat, desc["camera"], W, H, 8, 6, rng_states=ref.seed_states(W * H))
+    bpt, _, _, _ = ref.bpt_render(flat, desc["camera"], W, H, 8, 6, W * H)
+    assert pt.sum() == 0.0
+    assert np.isfinite(bpt).all() and bpt.sum() > 0

@@ -961,6 +961,57 @@ def test_directional_emitter_is_seen_by_light_subpaths_only():
     assert abs(sums[2] / sums[1] - 1) < 0.05, sums
 
 
+@needs_ref
+@pytest.mark.parametrize("emitter", ["point", "directional"])
+def test_delta_emitters_lvc_bpt_against_the_oracle(emitter):
+    """LVC-BPT with a point emitter (light subpaths from a delta position,
+    PointEDF's uniform sphere) or a directional emitter (light subpaths
+    along a delta direction, DirectionalEDF) in the diffuse box, against the
+    CPU restatement of lvc_bpt.cu with the same emitters (delta origins in
+    the MIS recursion, lvc_bpt.cu:330-332, 422-431, 736-739): 8 GPU batches
+    of 2048 frames against 8 oracle batches of 1024 frames, every lit pixel
+    within 4 combined standard errors on 99% of pixels (median standard
+    error at most 4% of the pixel), totals within 1% or 4 standard errors of
+    the batch totals.  The point itself, drawn by lens connections, is part
+    of the comparison."""
+    from vlr_b200 import vlr as VV, scenes
+    W = H = 32
+    g_b, c_b = [], []
+    for k in range(8):
+        ctx = VV.Context()
+        ctx.bindOutputBuffer(W, H)
+        scene, cam, keep = _point_lit_box(ctx, W, H, emitter)
+        ctx.setScene(scene)
+        ctx.setRenderer(VV.RENDERER_BPT)
+        ctx.setOptions(max_path_length=6, rng_seed=1000 + k)
+        ctx.render_samples(cam, True, 2048)
+        assert ctx.stats()["lightVertexOverflow"] == 0
+        g_b.append(_y_of(ctx.read_film()) / 2048)
+        ctx.close()
+    desc = scenes.cornell_box_desc(W, H)
+    for m in ("metal", "glass"):
+        desc["materials"][m] = ("Matte", {"albedo": ("Rec709(D65)", 0.5, 0.5, 0.5)})
+    if emitter == "directional":
+        desc["materials"]["light"] = ("DirectionalEmitter", {"emittance": ("Rec709(D65)", 5.0, 5.0, 5.0)})
+    else:
+        desc["materials"]["light"] = ("Matte", {"albedo": ("Rec709(D65)", 0.8, 0.8, 0.8)})
+        ref.points_set(np.array([[0.0, 2.4, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 0.0]], np.float32), 1, (4.0, 4.0, 4.0))
+    flat = scenes.flatten_desc(desc)
+    try:
+        for k in range(8):
+            state = {"eye": ref.seed_states(W * H, 2000 + k), "light": ref.seed_states(W * H, 3000 + k),
+                     "wl": np.array([100000 * k], np.uint64)}
+            cfilm, _, _, _ = ref.bpt_render(flat, desc["camera"], W, H, 1024, 6, W * H, state=state)
+            c_b.append(_y_of(cfilm) / 1024)
+    finally:
+        ref.points_set(None)
+    gt, ct = np.array([b.sum() for b in g_b]), np.array([b.sum() for b in c_b])
+    se = np.sqrt(gt.var(ddof=1) / len(gt) + ct.var(ddof=1) / len(ct))
+    assert ct.mean() > 0
+    assert abs(gt.mean() - ct.mean()) <= max(0.01 * ct.mean(), 4 * se), (gt.mean() / ct.mean(), se / ct.mean())
+    _per_pixel_batches_agree(g_b, c_b, max_median_se=0.04)
+
+
 def _poster_box(ctx, W, H, texels, nearest):
     """The diffuse Cornell box with its back wall split off as a "poster"
     whose albedo is an Image2DTexture of `texels` (an h x w x 3 linear-RGB

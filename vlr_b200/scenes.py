@@ -74,13 +74,15 @@ def uv_sphere(center, radius, n_lat, n_lon):
 
 
 MAT_TYPES = {"Matte": 0, "SpecularReflection": 1, "MicrofacetReflection": 2, "MicrofacetScattering": 3,
-             "LambertianScattering": 4, "UE4": 5, "SpecularScattering": 6, "DiffuseEmitter": 7}
+             "LambertianScattering": 4, "UE4": 5, "SpecularScattering": 6, "DiffuseEmitter": 7,
+             "DirectionalEmitter": 8}
 COLOR_SPACES = {"Rec709(D65) sRGB Gamma": 0, "Rec709(D65)": 1, "XYZ": 2, "xyY": 3}
 # spectrum parameter of each slot, per material type
 SPEC_SLOTS = {"Matte": ("albedo",), "SpecularReflection": ("coeff", "eta", "k"),
               "MicrofacetReflection": (None, "eta", "k"), "MicrofacetScattering": ("coeff", "eta ext", "eta int"),
               "LambertianScattering": ("coeff",), "UE4": ("base color",),
-              "SpecularScattering": ("coeff", "eta ext", "eta int"), "DiffuseEmitter": ("emittance",)}
+              "SpecularScattering": ("coeff", "eta ext", "eta int"), "DiffuseEmitter": ("emittance",),
+              "DirectionalEmitter": ("emittance",)}
 FLOAT_SLOTS = {"MicrofacetReflection": ("roughness", "anisotropy", "rotation"),
                "MicrofacetScattering": ("roughness", "anisotropy", "rotation"),
                "LambertianScattering": ("f0",), "UE4": ("roughness", "metallic")}
@@ -205,7 +207,7 @@ def flatten_desc(desc):
         for idx, mname in mesh["groups"]:
             g = len(gmat)
             gmat.append(names.index(mname))
-            is_emit = desc["materials"][mname][0] == "DiffuseEmitter"
+            is_emit = desc["materials"][mname][0] in ("DiffuseEmitter", "DirectionalEmitter")
             glight.append(n_light_inst if is_emit else -1)
             emitting = emitting or is_emit
             t = idx.reshape(-1, 3).astype(np.uint32) + base
