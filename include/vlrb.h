@@ -55,10 +55,13 @@ typedef struct VLRBBsdfBatch {
 VLRResult vlrbBsdfBatch(const VLRBBsdfBatch* batch, CUstream stream);
 
 /* All pointers are host pointers; copies in, runs, copies out, returns when
- * done.  kernelMs (may be NULL) receives the kernel's device time.  The
- * device buffers and stream it uses are kept per device between calls (grown
- * to the largest batch so far, released at process exit), and calls are
- * serialised; pinned host arrays copy at the link's full rate. */
+ * done.  The batch moves in chunks on three streams, so uploads, kernels and
+ * downloads of different chunks overlap; the outputs are those of one launch
+ * over the whole batch.  kernelMs (may be NULL) receives the kernels' device
+ * time summed over the chunks.  The device buffers and streams it uses are
+ * kept per device between calls (grown to the largest batch so far, released
+ * at process exit), and calls are serialised; pinned host arrays copy at the
+ * link's full rate and overlap, pageable ones are staged by the driver. */
 VLRResult vlrbBsdfBatchHost(const VLRBBsdfBatch* batch, float* kernelMs);
 
 /* vlrbBsdfBatchHost with options.  VLRB_BSDF_BATCH_CONTRACTED runs the copy
