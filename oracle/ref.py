@@ -147,6 +147,31 @@ def bpt_render(flat, camera, width, height, frames, max_path_length, num_light_p
     return film, state, seg.value, nlv.value
 
 
+def lt_render(flat, camera, width, height, frames, max_path_length, num_light_paths, light_states=None, film=None,
+              threads=0):
+    """Render `frames` light-tracing frames with the CPU restatement of the
+    reference's light_tracing.cu (oracle/ref_bpt.inc): per frame
+    num_light_paths light subpaths, each with its own hero wavelengths,
+    splatting a lens connection from every vertex.  light_states: one PCG32
+    state per light subpath (advanced in place).  Returns (film [H,W,16]
+    float64 sum, light_states, segments)."""
+    if light_states is None:
+        light_states = seed_states(num_light_paths, LIGHT_SEED)
+    if film is None:
+        film = np.zeros((height, width, 16), np.float64)
+    cam = _camera_array(camera)
+    seg = ctypes.c_uint64()
+    rc = lib().vlrref_lt_render(
+        _p(flat["pos"]), _p(flat["nrm"]), _p(flat["tan"]), ctypes.c_uint32(len(flat["pos"])),
+        _p(flat["tris"]), ctypes.c_uint32(len(flat["tris"])), _p(flat["groupMaterial"]),
+        _p(flat["groupLightInst"]), ctypes.c_uint32(len(flat["groupMaterial"])), _p(flat["mats"]),
+        ctypes.c_uint32(len(flat["mats"])), _p(cam), ctypes.c_uint32(width), ctypes.c_uint32(height),
+        ctypes.c_uint32(frames), ctypes.c_uint32(max_path_length), ctypes.c_uint32(num_light_paths),
+        ctypes.c_int(threads), _p(light_states), _p(film), ctypes.byref(seg))
+    assert rc == 0
+    return film, light_states, seg.value
+
+
 def pt_camera_rays(flat, camera, width, height, max_path_length, rng_states=None):
     """One frame of one sample per pixel (as pt_render) that also returns each
     pixel's camera ray and its brute-force closest hit: (film, rng_states,
