@@ -571,7 +571,7 @@ def glossy_guided_workload():
     return out
 
 
-def light_tracing_workload():
+def light_tracing_workload(cpu=True):
     """The light tracer (light subpaths with lens connections splatted to the
     film) on the Cornell box workload's scene, 512x512, one light subpath per
     pixel per frame, 64 frames in one launch of 2^24 light subpaths, max path
@@ -601,6 +601,19 @@ def light_tracing_workload():
            "lens_connections_per_s": (s1["shadowRays"] - s0["shadowRays"]) / (ms * 1e-3) / 1e9,
            "unit": "G path segments/s", "ms": ms}
     ctx.close()
+    if cpu:
+        # the CPU restatement of light_tracing.cu, all host threads, on a
+        # bounded sample of the same workload (4 frames)
+        from oracle import ref
+        if ref.available():
+            desc = scenes.cornell_box_desc(W, H)
+            frames = 4
+            _, _, seg = ref.lt_render(scenes.flatten_desc(desc), desc["camera"], W, H, frames, MAX_PATH_LENGTH, W * H)
+            secs = ref.last_render_seconds()
+            out["cpu_baseline"] = {"value": seg / secs / 1e9, "unit": "G path segments/s",
+                                   "cores": os.cpu_count() or 1, "kind": "port",
+                                   "sample": f"{frames} frames of {W * H} light subpaths: CPU restatement of "
+                                             "light_tracing.cu over the reference's BSDF/spectral code"}
     return out
 
 
@@ -646,7 +659,7 @@ WORKLOADS = {
                                                    paths_in_flight=a.paths_in_flight),
     "multi_scene_batch": lambda a: {"multi_scene_batch": batch_workload()},
     "glossy_guided": lambda a: {"glossy_guided": glossy_guided_workload()},
-    "light_tracing": lambda a: {"light_tracing": light_tracing_workload()},
+    "light_tracing": lambda a: {"light_tracing": light_tracing_workload(cpu=not a.no_cpu_baseline)},
     "denoise": lambda a: {"denoise": denoise_workload()},
     "time_to_rmse": lambda a: {"time_to_rmse": time_to_rmse()},
 }
@@ -924,7 +937,7 @@ def main():
         workloads = {}
         for fn in (lambda: {"bsdf_batch": bsdf_batch_workload(hbm_peak)}, terrain_workloads,
                    lambda: {"multi_scene_batch": batch_workload()},
-                   lambda: {"light_tracing": light_tracing_workload()},
+                   lambda: {"light_tracing": light_tracing_workload(cpu=not args.no_cpu_baseline)},
                    lambda: {"denoise": denoise_workload()}):
             try:
                 workloads.update(fn())
