@@ -653,8 +653,13 @@ void ptRenderLaunch(const SceneGPU &scene, const PathBuffers &pb, const Film &fi
         T.begin(kStageShade, stream, pMain + (guiding ? sizeof(GuideFrame) : 0));
         // the kMaps variants: normal maps, and float3 textures on scalar parameters
         const bool maps = scene.geomMaps != nullptr || scene.hasScalarTextures != 0;
-        if (guiding && maps) shadeKernel<true, true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
-        else if (guiding) shadeKernel<true, false><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
+        // the guided variant only where guiding acts: bounces that sample or
+        // record, and the one after the last recorded bounce, which closes
+        // its records; later bounces only add to the path's contribution,
+        // which the plain variant (fewer registers) does the same way
+        const bool guideShade = guiding && (b < gfp->recBounces || (gfp->record && b == gfp->recBounces));
+        if (guideShade && maps) shadeKernel<true, true><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
+        else if (guideShade) shadeKernel<true, false><<<grid, 256, 0, stream>>>(scene, pb, fp, *gfp);
         else if (maps) shadeKernel<false, true><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
         else shadeKernel<false, false><<<grid, 256, 0, stream>>>(scene, pb, fp, GuideFrame{});
         T.end(stream);
